@@ -1,0 +1,371 @@
+"""Benchmark: fused gate sweeps on a 30-qubit complex128 state (one B200).
+
+Workload (one "step"): the seeded 400-gate random mix (RotX/RotY/RotZ/U/
+PhaseShift, CX/CZ/Swap/ISwap/XX/YY/ZZ, CCNot/CSwap; seed 1234) applied to a
+2^30-amplitude complex128 state resident in HBM (16 GiB, far above the 126 MB
+L2, so no flush is needed between steps).
+
+Metric: effective gate-sweep bandwidth = gates x 2 x 16 B x 2^n / step time,
+the figure the reference's per-gate path is measured in (each reference gate
+is one full read+write sweep).  The roofline object reports the real HBM
+bandwidth of the fused sweep kernel: 2 x 16 B x 2^n per launch over its
+CUDA-event-timed launch duration, against the measured copy bandwidth.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU gate path (cpu::applyGate
+compiled from the reference sources into oracle/_ref) on the host cores,
+one gate of the same circuit per step.  With N > 1 (torchrun), every rank runs
+an independent replica (the single-state path does not shard), the step time
+is the max over ranks, and the value is the sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QUBITS = 30
+N_GATES = 400
+SEED = 1234
+AMP_BYTES = 16
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--qubits", type=int, default=N_QUBITS)
+    p.add_argument("--gates", type=int, default=N_GATES)
+    p.add_argument("--precision", default="complex128", choices=["complex128", "complex64"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def circuit(n, ngates):
+    from snuqs_b200 import circuits
+    return circuits.random_mix(n, ngates, seed=SEED)
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU path (oracle/_ref: the reference's cpu::applyGate)
+# ---------------------------------------------------------------------------
+def ref_cpu_gates(n, ops, max_seconds, min_gates=1, max_gates=None):
+    """Applies gates of `ops` in order with the reference CPU path until
+    max_seconds; returns (gates, seconds, threads)."""
+    import oracle
+
+    psi = np.zeros(1 << n, dtype=np.complex128)
+    oracle.ref().ref_initialize_basis_z(oracle._dptr(psi), n)
+    done, t0 = 0, time.perf_counter()
+    for op in ops:
+        if op[0] == "Unitary":
+            oracle.ref_apply_matrix(psi, n, op[3], op[1])
+        else:
+            oracle.ref_apply_gate(psi, n, op[0], op[1], op[2])
+        done += 1
+        el = time.perf_counter() - t0
+        if (el >= max_seconds and done >= min_gates) or (max_gates and done >= max_gates):
+            break
+    return done, time.perf_counter() - t0, oracle.ref().ref_max_threads()
+
+
+def host_ram_ok(n):
+    try:
+        import psutil
+
+        return psutil.virtual_memory().available > 2.5 * (1 << n) * AMP_BYTES
+    except Exception:
+        return False
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+
+    n, ops = args.qubits, circuit(args.qubits, args.gates)
+    if not host_ram_ok(n):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"host RAM below 2.5x the {n}-qubit state for the reference CPU path"}))
+        return
+    psi = np.zeros(1 << n, dtype=np.complex128)
+    oracle.ref().ref_initialize_basis_z(oracle._dptr(psi), n)
+    times = []
+    for s in range(args.warmup + args.steps):
+        op = ops[s % len(ops)]
+        t0 = time.perf_counter()
+        oracle.ref_apply_gate(psi, n, op[0], op[1], op[2])
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    value = 2 * AMP_BYTES * (1 << n) / t / 1e9
+    threads = oracle.ref().ref_max_threads()
+    sample = f"one gate of the {n}-qubit circuit per step, gates 0..{args.warmup + args.steps - 1}"
+    print(json.dumps({
+        "impl": "reference", "metric": metric_name(n, args.precision), "value": round(value, 3),
+        "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": f"synthetic: seeded random gate mix (seed {SEED})",
+        "config": config(n, args), "cpu_baseline": {
+            "value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+            "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
+def metric_name(n, precision):
+    return (f"{n}q {precision} random-mix effective gate-sweep GB/s "
+            f"(gates x 2 x amp bytes x 2^n / step time)")
+
+
+def config(n, args):
+    return {"workload": f"random_mix_{n}q_{args.precision}_{args.gates}g", "qubits": n,
+            "gates": args.gates, "precision": args.precision, "seed": SEED,
+            "state_bytes": (1 << n) * (16 if args.precision == "complex128" else 8),
+            "l2": "state far above the 126 MB L2; no flush between steps",
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------
+# Our engine
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    _run_ours(args, rank, world, local)
+
+
+def _run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+
+    from snuqs_b200 import _C, capi, circuits
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    n = args.qubits
+    amp = 16 if args.precision == "complex128" else 8
+    dtype = capi.SQ_C128 if args.precision == "complex128" else capi.SQ_C64
+    ops = circuit(n, args.gates)
+    mats = [circuits.op_matrix(op, capi.gate_matrix) for op in ops]
+    stream = torch.cuda.current_stream().cuda_stream
+
+    st = capi.State(n, dtype, stream=stream)
+    st.init_basis(0)
+
+    def step():
+        for op, m in zip(ops, mats):
+            st.apply_matrix(m, op[1])
+        st.flush()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    l0 = st.launches()
+    st.set_option(capi.SQ_OPT_TIMING, 1)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            step()
+        ev1.record()
+        torch.cuda.synchronize()
+    st.set_option(capi.SQ_OPT_TIMING, 0)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    sweep_ms, sweeps = st.sweep_timing()
+    launches = st.launches() - l0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.gates * 2 * amp * (1 << n) / (ms * 1e-3) / 1e9
+    sweeps_per_step = sweeps / args.steps
+    per_launch_ms = sweep_ms / max(1, sweeps)
+    alg_bytes = 2 * amp * (1 << n)
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    clocks = clk.summary()
+
+    out = {
+        "metric": metric_name(n, args.precision), "value": round(value, 2), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if dtype == capi.SQ_C128 else "f32",
+        "data": f"synthetic: seeded random gate mix (seed {SEED})", "config": config(n, args),
+        "gate_sweeps_per_s": round(world * args.gates / (ms * 1e-3), 2),
+        "fused_sweeps_per_step": sweeps_per_step,
+        "gates_per_sweep": round(args.gates / max(1e-9, sweeps_per_step), 2),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "kernel": "sq::sweep_kernel<double>" if dtype == capi.SQ_C128 else
+                     "sq::sweep_kernel<float>",
+                     "per_launch_ms": round(per_launch_ms, 4),
+                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+
+    if world == 1 and rank == 0 and not args.no_e2e:
+        out["e2e"] = e2e(n, ops, args, amp)
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(n, ops)
+    st.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def e2e(n, ops, args, amp):
+    """Same metric through the reference-facing `_C` drop-in, as
+    simulation.py drives it: initialize_basis_z, one functionals.apply per
+    gate, then the state copied to a pinned host StateVector (the result)."""
+    import torch
+
+    from snuqs_b200 import _C
+
+    G = _C.operation.gate_operations
+    prec = args.precision
+    try:
+        sv = _C.result_types.StateVector(_C.DeviceType.CUDA, n, prec)
+        if prec == "complex128":
+            host = _C.result_types.StateVector(n, True)
+        else:
+            return {"value": None, "unit": "GB/s", "note": "e2e measured for complex128 only"}
+    except Exception as e:  # pinned allocation can fail on small hosts
+        return {"value": None, "unit": "GB/s", "note": f"e2e skipped: {e}"}
+    gops = [G.Unitary(list(op[1]), op[3]) if op[0] == "Unitary" else
+            getattr(G, op[0])(list(op[1]), *op[2]) for op in ops]
+    h2d = sum(16 * (1 << (2 * len(g.targets))) for g in gops)
+    steps = max(1, min(args.steps, 3))
+
+    def one():
+        _C.functionals.initialize_basis_z(sv)
+        for g in gops:
+            _C.functionals.apply(sv, g, n, g.targets)
+        host.copy(sv)
+        return np.array(host, copy=False)[0]
+
+    one()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    t = (time.perf_counter() - t0) / steps
+    del sv, host
+    return {"value": round(args.gates * 2 * amp * (1 << n) / t / 1e9, 2), "unit": "GB/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": (1 << n) * amp,
+            "ms_per_step": round(t * 1e3, 2),
+            "path": "_C.functionals.apply per gate + StateVector.copy to pinned host",
+            "timing": "host wall clock around synchronous steps"}
+
+
+def cpu_baseline(n, ops):
+    if not host_ram_ok(n):
+        return {"value": None, "unit": "GB/s", "kind": "reference",
+                "sample": f"skipped: host RAM below 2.5x the {n}-qubit state"}
+    gates, secs, threads = ref_cpu_gates(n, ops, max_seconds=15.0, min_gates=2, max_gates=40)
+    return {"value": round(gates * 2 * AMP_BYTES * (1 << n) / secs / 1e9, 3), "unit": "GB/s",
+            "cores": threads, "kind": "reference",
+            "sample": f"first {gates} gates of the same {n}-qubit circuit, {secs:.1f} s, "
+                      f"OMP threads {threads}"}
+
+
+if __name__ == "__main__":
+    main()

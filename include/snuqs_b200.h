@@ -1,0 +1,180 @@
+/*
+ * snuqs_b200 -- C ABI of the B200 state-vector engine.
+ *
+ * Drop-in for SnuQS's per-gate state-update path:
+ *   functionals::apply   src/braket/snuqs/csrc/functionals/functionals.cc:15-28
+ *   cu::applyGate        src/braket/snuqs/csrc/operation/gate_operations_impl_cuda.cu:159-175
+ *   initialize_zero / initialize_basis_z   functionals.cc:30-50
+ *   StateVector(DeviceType::CUDA, n) / .cpu() / .copy()
+ *                        src/braket/snuqs/csrc/result_types/state_vector.cc:21-56
+ *   core.cuda.*          src/braket/snuqs/csrc/core/cuda/runtime.cu:4-25
+ *
+ * Conventions (the reference's):
+ *   - a state is 2^n amplitudes, interleaved re/im, complex128 (SQ_C128) or
+ *     complex64 (SQ_C64);
+ *   - qubit q is index bit n-1-q (big-endian, Braket order);
+ *   - a k-qubit matrix is row-major 2^k x 2^k complex128 (interleaved
+ *     re/im doubles, whatever the state's precision) and qubits[0] is the
+ *     most significant bit of its row/column index.
+ *
+ * Every entry point returns an sq_status; a nonzero status leaves a message
+ * for sq_last_error() (thread-local).  No entry point exits the process.
+ * Streams are cudaStream_t passed as void* (NULL = the legacy default stream).
+ * Gate application is queued per state and executed, fused, at the next
+ * flush; sq_flush, the copies, the reductions and sq_init_* flush first.
+ */
+#ifndef SNUQS_B200_H
+#define SNUQS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sq_state sq_state;
+
+typedef enum {
+  SQ_OK = 0,
+  SQ_ERR_INVALID = 1,     /* bad argument: qubit out of range, repeated qubit, null pointer */
+  SQ_ERR_CUDA = 2,        /* a CUDA runtime call failed (message has the CUDA error) */
+  SQ_ERR_OOM = 3,         /* device or pinned-host allocation failed */
+  SQ_ERR_UNSUPPORTED = 4, /* a size or option this build does not handle */
+  SQ_ERR_TIMEOUT = 5      /* a bounded device-side wait gave up */
+} sq_status;
+
+typedef enum { SQ_C128 = 0, SQ_C64 = 1 } sq_dtype;
+
+/* Gate ids: GateOperationType order of
+ * src/braket/snuqs/csrc/operation/operation.h:17-52, then the Braket gates the
+ * reference lists as removed (src/braket/snuqs/gate_operations.py:238). */
+typedef enum {
+  SQ_GATE_IDENTITY = 0, SQ_GATE_HADAMARD, SQ_GATE_PAULI_X, SQ_GATE_PAULI_Y,
+  SQ_GATE_PAULI_Z, SQ_GATE_CX, SQ_GATE_CY, SQ_GATE_CZ, SQ_GATE_S, SQ_GATE_SI,
+  SQ_GATE_T, SQ_GATE_TI, SQ_GATE_V, SQ_GATE_VI, SQ_GATE_PHASE_SHIFT,
+  SQ_GATE_CPHASE_SHIFT, SQ_GATE_CPHASE_SHIFT00, SQ_GATE_CPHASE_SHIFT01,
+  SQ_GATE_CPHASE_SHIFT10, SQ_GATE_ROT_X, SQ_GATE_ROT_Y, SQ_GATE_ROT_Z,
+  SQ_GATE_SWAP, SQ_GATE_ISWAP, SQ_GATE_PSWAP, SQ_GATE_XY, SQ_GATE_XX,
+  SQ_GATE_YY, SQ_GATE_ZZ, SQ_GATE_CCNOT, SQ_GATE_CSWAP, SQ_GATE_U,
+  SQ_GATE_GPHASE, SQ_GATE_SWAP_A2A, SQ_GATE_ECR, SQ_GATE_CV, SQ_GATE_PRX,
+  SQ_GATE_COUNT
+} sq_gate;
+
+typedef enum {
+  SQ_OPT_FUSION = 0,    /* 1 (default): fused tile sweeps; 0: one unfused kernel per gate */
+  SQ_OPT_TILE_BITS = 1, /* log2 amplitudes per shared-memory tile (4..12; default 12) */
+  SQ_OPT_REORDER = 2,   /* 1 (default): the planner may absorb later gates that commute */
+  SQ_OPT_TIMING = 3     /* 1: record a CUDA event pair around every fused-sweep launch */
+} sq_option;
+
+/* ---- library / device ------------------------------------------------ */
+const char *sq_version(void);
+const char *sq_last_error(void);
+/* core.cuda.device_count / get_device / set_device / device_synchronize /
+ * mem_info: src/braket/snuqs/csrc/core/cuda/runtime.cu:4-25 */
+int sq_device_count(int *count);
+int sq_get_device(int *device);
+int sq_set_device(int device);
+int sq_device_synchronize(void);
+int sq_mem_info(size_t *free_bytes, size_t *total_bytes);
+
+/* Stream / Event / pinned host memory, so callers need no CUDA headers:
+ * Stream (src/braket/snuqs/csrc/stream/stream.cc:6-34), Event
+ * (src/braket/snuqs/csrc/event/event.cc:5-26), BufferPinned host memory. */
+int sq_stream_create(void **stream, int nonblocking);
+int sq_stream_destroy(void *stream);
+int sq_stream_synchronize(void *stream);
+int sq_stream_wait_event(void *stream, void *event);
+int sq_event_create(void **event);
+int sq_event_destroy(void *event);
+int sq_event_record(void *event, void *stream);
+int sq_event_synchronize(void *event);
+/* Milliseconds between two recorded events. */
+int sq_event_elapsed(void *start, void *stop, float *ms);
+int sq_host_alloc(void **ptr, size_t bytes);
+int sq_host_free(void *ptr);
+
+/* ---- gate matrices ------------------------------------------------------
+ * Matrix of a named gate (the reference constructors,
+ * src/braket/snuqs/csrc/operation/gate_operations.cc:9-734; ECR/CV/PRx from
+ * their Braket definitions).  out receives 4^k complex128 (interleaved);
+ * *k receives the gate's qubit count. */
+int sq_gate_matrix(int gate, const double *angles, uint32_t nangles,
+                   double *out, uint32_t *k);
+int sq_gate_qubits(int gate);
+
+/* ---- state handle -------------------------------------------------------
+ * StateVector(DeviceType::CUDA, n): state_vector.cc:21-25 + buffer_cuda.cc:13-17. */
+int sq_state_create(uint32_t num_qubits, int dtype, sq_state **out);
+/* Wraps caller-owned device memory of 2^n amplitudes (not freed by destroy). */
+int sq_state_wrap(void *device_ptr, uint32_t num_qubits, int dtype,
+                  sq_state **out);
+int sq_state_destroy(sq_state *s);
+void *sq_state_data(const sq_state *s);
+uint32_t sq_state_num_qubits(const sq_state *s);
+int sq_state_dtype(const sq_state *s);
+int sq_set_option(sq_state *s, int option, int64_t value);
+
+/* initialize_zero / initialize_basis_z (functionals.cc:30-50); init_basis
+ * writes |index>, so index 0 is the reference's |0...0>. Pending gates are
+ * discarded. */
+int sq_init_zero(sq_state *s, void *stream);
+int sq_init_basis(sq_state *s, uint64_t index, void *stream);
+
+/* functionals::apply (functionals.cc:15-28): queue one k-qubit gate given by
+ * its matrix (k = 0 is a global phase: a 1x1 matrix).  k <= 10. */
+int sq_apply_matrix(sq_state *s, const double *matrix, const uint32_t *qubits,
+                    uint32_t k, void *stream);
+/* As sq_apply_matrix with extra control qubits: the matrix acts on `qubits`
+ * when every control qubit c[i] has value cv[i] (cv NULL = all ones).  This
+ * is the ctrl/negctrl modifier the reference stores but never applies
+ * (src/braket/snuqs/openqasm/program_context.py:744-780). */
+int sq_apply_controlled_matrix(sq_state *s, const double *matrix,
+                               const uint32_t *qubits, uint32_t k,
+                               const uint32_t *controls,
+                               const uint8_t *control_values, uint32_t nc,
+                               void *stream);
+/* Queue a named gate (sq_gate id) with its angles. */
+int sq_apply_gate(sq_state *s, int gate, const uint32_t *qubits, uint32_t k,
+                  const double *angles, uint32_t nangles, void *stream);
+/* Execute every queued gate on `stream` (fused sweeps). */
+int sq_flush(sq_state *s, void *stream);
+int sq_pending(const sq_state *s, uint32_t *count);
+/* Kernels launched by all flushes of this state so far. */
+int sq_launch_count(const sq_state *s, uint64_t *count);
+/* With SQ_OPT_TIMING on: total device time (ms) and number of the fused-sweep
+ * launches recorded since the last call (synchronises on the recorded
+ * events, then clears them). */
+int sq_sweep_timing(sq_state *s, double *total_ms, uint64_t *launches);
+
+/* cu::applyGate (gate_operations_impl_cuda.cu:159-175), unqueued: apply
+ * one gate to a raw complex128 device buffer of nelems = 2^nqubits
+ * amplitudes, with a device-resident row-major matrix, on `stream`.
+ * targets are size_t-sized qubit indices as in the reference. */
+int sq_apply_gate_buffer(void *buffer, const void *gate_device,
+                         const uint64_t *targets, uint32_t ntargets,
+                         uint32_t nqubits, uint64_t nelems, void *stream);
+
+/* ---- copies (StateVector.cpu()/.cuda()/.copy(): state_vector.cc:35-56) --
+ * Asynchronous on `stream`; synchronise the stream before reading dst. */
+int sq_copy_to_host(sq_state *s, void *dst, void *stream);
+int sq_copy_from_host(sq_state *s, const void *src, void *stream);
+int sq_copy_state(sq_state *dst, sq_state *src, void *stream);
+
+/* ---- results ----------------------------------------------------------- */
+/* |psi_i|^2 into a caller-provided DEVICE array of 2^n doubles
+ * (simulation.py:208-215 computes this on the host). */
+int sq_probabilities(sq_state *s, double *out_device, void *stream);
+/* sum_t w_t <psi|P_t|psi> for n_terms Pauli strings, paulis[t*n + q] in
+ * {'I','X','Y','Z'} acting on qubit q (observables.py:136-243 semantics).
+ * Synchronous: returns the FP64 value in *out. */
+int sq_expect_pauli(sq_state *s, const char *paulis, const double *weights,
+                    uint32_t n_terms, double *out, void *stream);
+/* Squared norm in FP64 (synchronous). */
+int sq_norm2(sq_state *s, double *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SNUQS_B200_H */

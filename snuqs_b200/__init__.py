@@ -1,0 +1,27 @@
+"""snuqs_b200: a B200-native state-vector engine behind SnuQS's plugin surface.
+
+* ``snuqs_b200._C`` -- the reference's pybind11 module surface
+  (``braket.snuqs._C``: operation, operation.gate_operations, functionals,
+  result_types, stream, event, core, core.cuda, DeviceType).
+* ``snuqs_b200.capi`` -- ctypes binding of the C ABI (include/snuqs_b200.h).
+* ``snuqs_b200.simulation`` / ``transpile`` / ``gate_operations`` -- the
+  reference's Python driver layer for the no-offload CUDA path.
+
+The native libraries are built in-tree by ``python -m snuqs_b200.build``.
+Importing the package without them raises: the engine has no CPU fallback.
+"""
+from __future__ import annotations
+
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+try:
+    from . import _C  # noqa: F401
+except ImportError as e:  # pragma: no cover - exercised only on a broken install
+    raise ImportError(
+        "snuqs_b200 native extension not built (run `python -m snuqs_b200.build`): " + str(e)
+    ) from e
+
+__version__ = "0.1.0"
+LIB_PATH = os.path.join(_HERE, "libsnuqs_b200.so")

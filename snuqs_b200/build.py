@@ -1,0 +1,92 @@
+"""Build recipe for the snuqs_b200 native code (in-tree, sm_100a).
+
+Produces, next to this file:
+
+* ``libsnuqs_b200.so`` -- the engine: CUDA kernels + planner + the C ABI of
+  ``include/snuqs_b200.h``;
+* ``_C.<abi>.so``       -- the pybind11 module with the reference's ``_C``
+  surface, linked against ``libsnuqs_b200.so`` (rpath ``$ORIGIN``).
+
+nvcc cross-compiles for ``sm_100a`` without a GPU.  Run as
+``python -m snuqs_b200.build`` or through ``__graft_entry__.build()``.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import sysconfig
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+BUILD = os.path.join(HERE, "_build")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ENGINE_CU = ["engine.cu"]
+ENGINE_CC = ["gates.cc", "planner.cc"]
+LIB = os.path.join(HERE, "libsnuqs_b200.so")
+
+
+def _ext_suffix() -> str:
+    return sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+
+
+PYEXT = os.path.join(HERE, "_C" + _ext_suffix())
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {cmd[0]} ... {cmd[-1]}")
+
+
+def _stale(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def _headers() -> list[str]:
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    return hs + [os.path.join(INCLUDE, "snuqs_b200.h")]
+
+
+def build(force: bool = False, verbose: bool = False) -> None:
+    os.makedirs(BUILD, exist_ok=True)
+    common = ["-O3", "-std=c++17", "-I", CSRC, "-I", INCLUDE]
+    objs = []
+    hdrs = _headers()
+    for f in ENGINE_CU:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(BUILD, f + ".o")
+        if force or _stale(obj, [src] + hdrs):
+            _run([NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
+                  "-Xptxas", "-warn-spills", "-c", src, "-o", obj])
+        objs.append(obj)
+    for f in ENGINE_CC:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(BUILD, f + ".o")
+        if force or _stale(obj, [src] + hdrs):
+            _run(["g++", *common, "-fPIC", "-Wall", "-c", src, "-o", obj])
+        objs.append(obj)
+    if force or _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static",
+              "-Xlinker", "--no-undefined"])
+    import pybind11
+
+    pysrc = os.path.join(CSRC, "pymodule.cc")
+    if force or _stale(PYEXT, [pysrc, LIB] + hdrs):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden",
+              "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
+              "-I", INCLUDE, pysrc, "-o", PYEXT, "-L", HERE, "-lsnuqs_b200",
+              "-Wl,-rpath,$ORIGIN"])
+    if verbose:
+        print("built", LIB, PYEXT)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

@@ -1,0 +1,226 @@
+"""ctypes binding of the C ABI (include/snuqs_b200.h).
+
+This is the binding a maintainer would add on the reference side to call the
+engine without pybind11; the tests use it to drive the
+C ABI directly.  Every call checks its status and raises SqError with the
+library's message.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsnuqs_b200.so")
+
+SQ_OK, SQ_ERR_INVALID, SQ_ERR_CUDA, SQ_ERR_OOM, SQ_ERR_UNSUPPORTED, SQ_ERR_TIMEOUT = range(6)
+SQ_C128, SQ_C64 = 0, 1
+SQ_OPT_FUSION, SQ_OPT_TILE_BITS, SQ_OPT_REORDER, SQ_OPT_TIMING = 0, 1, 2, 3
+
+GATE_NAMES = [
+    "Identity", "Hadamard", "PauliX", "PauliY", "PauliZ", "CX", "CY", "CZ", "S", "Si", "T",
+    "Ti", "V", "Vi", "PhaseShift", "CPhaseShift", "CPhaseShift00", "CPhaseShift01",
+    "CPhaseShift10", "RotX", "RotY", "RotZ", "Swap", "ISwap", "PSwap", "XY", "XX", "YY", "ZZ",
+    "CCNot", "CSwap", "U", "GPhase", "SwapA2A", "ECR", "CV", "PRx",
+]
+GATE_ID = {n: i for i, n in enumerate(GATE_NAMES)}
+
+# Every entry point the header declares: name -> (restype, argtypes).
+_P = ctypes.c_void_p
+_U32, _U64, _I, _D = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_double
+_PU32, _PU64, _PD = ctypes.POINTER(_U32), ctypes.POINTER(_U64), ctypes.POINTER(_D)
+SIGNATURES = {
+    "sq_version": (ctypes.c_char_p, []),
+    "sq_last_error": (ctypes.c_char_p, []),
+    "sq_device_count": (_I, [ctypes.POINTER(_I)]),
+    "sq_get_device": (_I, [ctypes.POINTER(_I)]),
+    "sq_set_device": (_I, [_I]),
+    "sq_device_synchronize": (_I, []),
+    "sq_mem_info": (_I, [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
+    "sq_stream_create": (_I, [ctypes.POINTER(_P), _I]),
+    "sq_stream_destroy": (_I, [_P]),
+    "sq_stream_synchronize": (_I, [_P]),
+    "sq_stream_wait_event": (_I, [_P, _P]),
+    "sq_event_create": (_I, [ctypes.POINTER(_P)]),
+    "sq_event_destroy": (_I, [_P]),
+    "sq_event_record": (_I, [_P, _P]),
+    "sq_event_synchronize": (_I, [_P]),
+    "sq_event_elapsed": (_I, [_P, _P, ctypes.POINTER(ctypes.c_float)]),
+    "sq_host_alloc": (_I, [ctypes.POINTER(_P), ctypes.c_size_t]),
+    "sq_host_free": (_I, [_P]),
+    "sq_gate_matrix": (_I, [_I, _PD, _U32, _PD, _PU32]),
+    "sq_gate_qubits": (_I, [_I]),
+    "sq_state_create": (_I, [_U32, _I, ctypes.POINTER(_P)]),
+    "sq_state_wrap": (_I, [_P, _U32, _I, ctypes.POINTER(_P)]),
+    "sq_state_destroy": (_I, [_P]),
+    "sq_state_data": (_P, [_P]),
+    "sq_state_num_qubits": (_U32, [_P]),
+    "sq_state_dtype": (_I, [_P]),
+    "sq_set_option": (_I, [_P, _I, ctypes.c_int64]),
+    "sq_init_zero": (_I, [_P, _P]),
+    "sq_init_basis": (_I, [_P, _U64, _P]),
+    "sq_apply_matrix": (_I, [_P, _PD, _PU32, _U32, _P]),
+    "sq_apply_controlled_matrix": (_I, [_P, _PD, _PU32, _U32, _PU32,
+                                        ctypes.POINTER(ctypes.c_uint8), _U32, _P]),
+    "sq_apply_gate": (_I, [_P, _I, _PU32, _U32, _PD, _U32, _P]),
+    "sq_flush": (_I, [_P, _P]),
+    "sq_pending": (_I, [_P, _PU32]),
+    "sq_launch_count": (_I, [_P, _PU64]),
+    "sq_sweep_timing": (_I, [_P, _PD, _PU64]),
+    "sq_apply_gate_buffer": (_I, [_P, _P, _PU64, _U32, _U32, _U64, _P]),
+    "sq_copy_to_host": (_I, [_P, _P, _P]),
+    "sq_copy_from_host": (_I, [_P, _P, _P]),
+    "sq_copy_state": (_I, [_P, _P, _P]),
+    "sq_probabilities": (_I, [_P, _P, _P]),
+    "sq_expect_pauli": (_I, [_P, ctypes.c_char_p, _PD, _U32, _PD, _P]),
+    "sq_norm2": (_I, [_P, _PD, _P]),
+}
+
+
+class SqError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"sq status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libsnuqs_b200.so.  Raises if it has not been built: there is no
+    fallback implementation."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; build it with python -m snuqs_b200.build")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != SQ_OK:
+        raise SqError(status, lib().sq_last_error().decode())
+
+
+def _u32(xs: Sequence[int]):
+    return (_U32 * max(1, len(xs)))(*xs)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_PD)
+
+
+def gate_matrix(name: str, angles: Sequence[float] = ()) -> np.ndarray:
+    a = np.zeros(3, dtype=np.float64)
+    a[: len(angles)] = angles
+    out = np.zeros(64, dtype=np.complex128)
+    k = _U32(0)
+    check(lib().sq_gate_matrix(GATE_ID[name], _dp(a), len(angles), _dp(out), ctypes.byref(k)))
+    d = 1 << k.value
+    return out[: d * d].reshape(d, d).copy()
+
+
+class State:
+    """Owning wrapper of an sq_state* (complex128 or complex64)."""
+
+    def __init__(self, num_qubits: int, dtype: int = SQ_C128, stream=None):
+        self.n = num_qubits
+        self.dtype = dtype
+        self.stream = stream
+        h = _P()
+        check(lib().sq_state_create(num_qubits, dtype, ctypes.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            check(lib().sq_state_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def np_dtype(self):
+        return np.complex64 if self.dtype == SQ_C64 else np.complex128
+
+    def set_option(self, opt: int, value: int) -> None:
+        check(lib().sq_set_option(self.h, opt, value))
+
+    def init_basis(self, index: int = 0) -> None:
+        check(lib().sq_init_basis(self.h, index, self.stream))
+
+    def apply_matrix(self, m: np.ndarray, qubits: Sequence[int], controls: Sequence[int] = (),
+                     control_values: Sequence[int] | None = None) -> None:
+        mm = np.ascontiguousarray(m, dtype=np.complex128)
+        if controls:
+            cv = (ctypes.c_uint8 * len(controls))(*(control_values or [1] * len(controls)))
+            check(lib().sq_apply_controlled_matrix(self.h, _dp(mm), _u32(qubits), len(qubits),
+                                                   _u32(controls), cv, len(controls), self.stream))
+        else:
+            check(lib().sq_apply_matrix(self.h, _dp(mm), _u32(qubits), len(qubits), self.stream))
+
+    def apply_gate(self, name: str, qubits: Sequence[int], angles: Sequence[float] = ()) -> None:
+        a = np.ascontiguousarray(np.array(list(angles) + [0.0], dtype=np.float64))
+        check(lib().sq_apply_gate(self.h, GATE_ID[name], _u32(qubits), len(qubits), _dp(a),
+                                  len(angles), self.stream))
+
+    def apply_ops(self, ops) -> None:
+        for op in ops:
+            if op[0] == "Unitary":
+                self.apply_matrix(op[3], op[1])
+            else:
+                self.apply_gate(op[0], op[1], op[2])
+
+    def flush(self) -> None:
+        check(lib().sq_flush(self.h, self.stream))
+
+    def launches(self) -> int:
+        c = _U64(0)
+        check(lib().sq_launch_count(self.h, ctypes.byref(c)))
+        return c.value
+
+    def sweep_timing(self):
+        """(total ms, launches) of the fused sweeps recorded with SQ_OPT_TIMING."""
+        ms, c = _D(0), _U64(0)
+        check(lib().sq_sweep_timing(self.h, ctypes.byref(ms), ctypes.byref(c)))
+        return ms.value, c.value
+
+    def to_host(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(1 << self.n, dtype=self.np_dtype)
+        check(lib().sq_copy_to_host(self.h, out.ctypes.data_as(_P), self.stream))
+        check(lib().sq_stream_synchronize(self.stream))
+        return out
+
+    def from_host(self, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=self.np_dtype)
+        check(lib().sq_copy_from_host(self.h, a.ctypes.data_as(_P), self.stream))
+        check(lib().sq_stream_synchronize(self.stream))
+
+    def expectation(self, terms) -> float:
+        """terms: list of (weight, pauli string of length n)."""
+        flat = "".join(p for _, p in terms).encode()
+        w = np.ascontiguousarray([float(x) for x, _ in terms] or [0.0], dtype=np.float64)
+        out = _D(0)
+        check(lib().sq_expect_pauli(self.h, flat, _dp(w), len(terms), ctypes.byref(out),
+                                    self.stream))
+        return out.value
+
+    def norm2(self) -> float:
+        out = _D(0)
+        check(lib().sq_norm2(self.h, ctypes.byref(out), self.stream))
+        return out.value
+
+    def data_ptr(self) -> int:
+        return lib().sq_state_data(self.h)

@@ -1,0 +1,67 @@
+// Host-side gate representation, gate-matrix factory and fusion planner.
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sq_plan.h"
+
+namespace sq {
+
+using cplx = std::complex<double>;
+
+// Matrix of gate `gate` (sq_gate id) into m (4^k entries, row-major).
+// Returns k, or -1 for an unknown gate / wrong angle count.
+int gate_matrix(int gate, const double *angles, uint32_t nangles, std::vector<cplx> &m);
+int gate_qubits(int gate);
+int gate_num_angles(int gate);
+
+// One queued gate after qubit -> index-bit translation.
+//   kind kOpDense: m is 4^k row-major, tbits[0] is the MSB of its index.
+//   kind kOpDiag:  m is the 2^k diagonal.
+// Controls (cmask/cval, index bits) apply to dense ops; diagonal ops fold
+// their controls into the diagonal.
+struct HostOp {
+  uint8_t kind = kOpDense;
+  std::vector<int> tbits;
+  uint64_t cmask = 0, cval = 0;
+  std::vector<cplx> m;
+  uint64_t target_mask() const;
+  uint64_t touched_mask() const;  // targets + controls
+  uint64_t nondiag_mask() const;  // bits acted on non-diagonally
+};
+
+// Structure analysis of a dense matrix on `tbits` with controls: peels off
+// exact control qubits, detects exactly diagonal matrices and drops exact
+// identities.  Entries are compared exactly (== 0, == 1), so the result
+// applies the same products as the full matrix minus exact zeros.
+// Returns false when the op is an exact identity (nothing to apply).
+bool analyse_op(const std::vector<cplx> &m, const std::vector<int> &tbits, uint64_t cmask,
+                uint64_t cval, HostOp &out);
+
+// A planned launch: a fused sweep, or one unfused gate.
+struct PlannedSweep {
+  SweepHeader h;
+  std::vector<SweepPhase> ph;
+  std::vector<SweepOp> op;
+  std::vector<cplx> coef;
+  uint32_t ngates = 0;  // queued ops it carries
+};
+
+struct PlannedLaunch {
+  bool is_sweep = true;
+  PlannedSweep sweep;
+  HostOp gate;  // unfused gate (dense, any k; cmask/cval are its controls)
+};
+
+struct PlanOptions {
+  uint32_t tile_bits = kMaxTileBits;
+  bool reorder = true;
+};
+
+// Packs ops (in circuit order) into fused sweeps for an n-qubit state.
+std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t n,
+                                       const PlanOptions &opt);
+
+}  // namespace sq

@@ -1,0 +1,266 @@
+// Fusion planner: packs queued gates into fused tile sweeps.
+//
+// The reference applies every gate as its own full-state kernel
+// (src/braket/snuqs/simulation.py:280-284 -> gate_operations_impl_cuda.cu).
+// Here a sweep carries as many gates as fit its tile: a gate fits when its
+// non-diagonal targets lie in the sweep's tile bit set S (|S| = m, the l
+// lowest index bits always included); controls and diagonal gates fit
+// anywhere.  With reordering on, a gate that does not fit is skipped and later
+// gates that commute with every skipped gate may still join (gates commute
+// when neither acts non-diagonally on a bit the other touches).  Inside a
+// sweep, gates are cut into phases of at most 4 distinct target bits (the
+// register bits).
+#include <algorithm>
+#include <cassert>
+#include <cstring>
+#include <stdexcept>
+
+#include "host_ops.h"
+
+namespace sq {
+
+namespace {
+
+int popc64(uint64_t x) { return __builtin_popcountll(x); }
+
+struct SweepBuilder {
+  uint32_t n, m, l;
+  uint64_t S;  // tile bits (global index bits)
+  std::vector<const HostOp *> ops;
+  std::vector<uint64_t> phase_regs;  // register bits (global) of each phase
+  std::vector<uint32_t> phase_first; // first op index of each phase
+  uint32_t ncoef = 0;
+
+  SweepBuilder(uint32_t n_, uint32_t m_, uint32_t l_) : n(n_), m(m_), l(l_) {
+    S = (l >= 64) ? ~uint64_t(0) : ((uint64_t(1) << l) - 1);
+  }
+
+  static uint32_t coef_count(const HostOp &op) {
+    return op.kind == kOpDiag ? (1u << op.tbits.size()) : (1u << (2 * op.tbits.size()));
+  }
+
+  // Would `op` fit (tile, register, budget)?  If so, add it.
+  bool try_add(const HostOp &op) {
+    if (ops.size() >= size_t(kMaxOps)) return false;
+    if (ncoef + coef_count(op) > uint32_t(kMaxCoef)) return false;
+    if (op.kind == kOpDiag) {
+      if (op.tbits.size() > size_t(kMaxDiagK)) return false;
+      if (phase_regs.empty()) {
+        phase_regs.push_back(0);
+        phase_first.push_back(uint32_t(ops.size()));
+      }
+      ops.push_back(&op);
+      ncoef += coef_count(op);
+      return true;
+    }
+    if (op.tbits.size() > size_t(kRegBits)) return false;
+    const uint64_t T = op.target_mask();
+    if (uint32_t(popc64(S | T)) > m) return false;
+    const bool new_phase = phase_regs.empty() || popc64(phase_regs.back() | T) > kRegBits;
+    if (new_phase && phase_regs.size() >= size_t(kMaxPhases)) return false;
+    S |= T;
+    if (new_phase) {
+      phase_regs.push_back(T);
+      phase_first.push_back(uint32_t(ops.size()));
+    } else {
+      phase_regs.back() |= T;
+    }
+    ops.push_back(&op);
+    ncoef += coef_count(op);
+    return true;
+  }
+
+  PlannedSweep finish() const;
+};
+
+// Position of global bit b within the ascending bit list of mask.
+int rank_in(uint64_t mask, int b) { return popc64(mask & ((uint64_t(1) << b) - 1)); }
+
+PlannedSweep SweepBuilder::finish() const {
+  PlannedSweep ps;
+  // Pad the tile to exactly m bits with the lowest unused bits.
+  uint64_t tile = S;
+  for (uint32_t b = 0; b < n && uint32_t(popc64(tile)) < m; ++b) tile |= uint64_t(1) << b;
+  SweepHeader &h = ps.h;
+  std::memset(&h, 0, sizeof(h));
+  h.n = n;
+  h.m = m;
+  h.l = l;
+  h.num_tiles = uint64_t(1) << (n - m);
+  {
+    int i = 0;
+    for (uint32_t b = l; b < n; ++b)
+      if ((tile >> b) & 1) h.hi[i++] = uint8_t(b);
+  }
+  // Phases: register bits as tile positions, padded from the top of the tile
+  // so lanes keep the low positions (coalesced global access, no bank
+  // conflicts).
+  const int np = int(phase_regs.size());
+  for (int p = 0; p < np; ++p) {
+    uint32_t regpos = 0;  // bitmask of tile positions
+    for (int b = 0; b < 64; ++b)
+      if ((phase_regs[p] >> b) & 1) regpos |= 1u << rank_in(tile, b);
+    for (int pos = int(m) - 1; pos >= 0 && __builtin_popcount(regpos) < kRegBits; --pos)
+      regpos |= 1u << pos;
+    SweepPhase ph{};
+    int r = 0;
+    for (uint32_t pos = 0; pos < m; ++pos)
+      if ((regpos >> pos) & 1) ph.reg[r++] = uint8_t(pos);
+    ph.op_begin = uint16_t(phase_first[p]);
+    ph.op_end = uint16_t(p + 1 < np ? phase_first[p + 1] : ops.size());
+    ps.ph.push_back(ph);
+  }
+  h.nphases = uint32_t(np);
+  const uint32_t lowpos = (1u << std::min<uint32_t>(l, 5)) - 1;
+  auto regmask = [&](const SweepPhase &ph) {
+    uint32_t x = 0;
+    for (int b = 0; b < kRegBits; ++b) x |= 1u << ph.reg[b];
+    return x;
+  };
+  if ((regmask(ps.ph.front()) & lowpos) == 0) h.flags |= kDirectLoad;
+  if ((regmask(ps.ph.back()) & lowpos) == 0) h.flags |= kDirectStore;
+
+  // Ops.
+  for (int p = 0; p < np; ++p) {
+    const SweepPhase &ph = ps.ph[p];
+    auto regof = [&](int gbit) -> int {  // register position of a global bit, or -1
+      if (!((tile >> gbit) & 1)) return -1;
+      const int pos = rank_in(tile, gbit);
+      for (int r = 0; r < kRegBits; ++r)
+        if (ph.reg[r] == pos) return r;
+      return -1;
+    };
+    for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
+      const HostOp &op = *ops[oi];
+      SweepOp so;
+      std::memset(&so, 0, sizeof(so));
+      so.kind = op.kind;
+      so.k = uint8_t(op.tbits.size());
+      so.coef = uint32_t(ps.coef.size());
+      const int k = int(op.tbits.size());
+      if (op.kind == kOpDiag) {
+        for (int t = 0; t < k; ++t) {
+          const int b = op.tbits[t];
+          const int r = regof(b);
+          if (r >= 0) {
+            so.dsrc[t] = kSrcReg;
+            so.dpos[t] = uint8_t(r);
+          } else if ((tile >> b) & 1) {
+            so.dsrc[t] = kSrcLocal;
+            so.dpos[t] = uint8_t(rank_in(tile, b));
+          } else {
+            so.dsrc[t] = kSrcGlobal;
+            so.dpos[t] = uint8_t(b);
+          }
+        }
+        ps.coef.insert(ps.coef.end(), op.m.begin(), op.m.end());
+      } else {
+        // Target j (matrix bit k-1-j) sits at register position rp[j]; the
+        // kernel's canonical order has matrix bit i <-> i-th set bit of vmask.
+        int rp[kRegBits];
+        uint32_t vmask = 0;
+        for (int j = 0; j < k; ++j) {
+          rp[j] = regof(op.tbits[j]);
+          assert(rp[j] >= 0);
+          vmask |= 1u << rp[j];
+        }
+        so.vmask = uint8_t(vmask);
+        int newbit[kRegBits];  // old matrix bit (k-1-j) -> canonical bit
+        for (int j = 0; j < k; ++j) newbit[k - 1 - j] = __builtin_popcount(vmask & ((1u << rp[j]) - 1));
+        const int d = 1 << k;
+        std::vector<cplx> cm(size_t(d) * d);
+        auto remap = [&](int x) {
+          int y = 0;
+          for (int b = 0; b < k; ++b)
+            if ((x >> b) & 1) y |= 1 << newbit[b];
+          return y;
+        };
+        for (int r = 0; r < d; ++r)
+          for (int c = 0; c < d; ++c) cm[size_t(remap(r)) * d + remap(c)] = op.m[size_t(r) * d + c];
+        ps.coef.insert(ps.coef.end(), cm.begin(), cm.end());
+        for (int b = 0; b < 64; ++b) {
+          if (!((op.cmask >> b) & 1)) continue;
+          const uint64_t v = (op.cval >> b) & 1;
+          const int r = regof(b);
+          if (r >= 0) {
+            so.rmask |= uint8_t(1u << r);
+            if (v) so.rval |= uint8_t(1u << r);
+          } else if ((tile >> b) & 1) {
+            const int pos = rank_in(tile, b);
+            so.lmask |= 1u << pos;
+            if (v) so.lval |= 1u << pos;
+          } else {
+            so.gmask |= uint64_t(1) << b;
+            if (v) so.gval |= uint64_t(1) << b;
+          }
+        }
+      }
+      ps.op.push_back(so);
+    }
+  }
+  h.ncoef = uint32_t(ps.coef.size());
+  ps.ngates = uint32_t(ops.size());
+  return ps;
+}
+
+}  // namespace
+
+std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t n,
+                                       const PlanOptions &opt) {
+  std::vector<PlannedLaunch> out;
+  if (n < uint32_t(kRegBits)) throw std::invalid_argument("fused sweeps need n >= 4");
+  // A tile must hold the low bits plus one full register set.
+  const uint32_t want = std::max<uint32_t>(opt.tile_bits, kLowBits + kRegBits);
+  const uint32_t m = std::min<uint32_t>(std::min<uint32_t>(want, kMaxTileBits), n);
+  const uint32_t l = std::min<uint32_t>(kLowBits, m);
+  const size_t kWindow = 256;  // lookahead when reordering
+
+  std::vector<const HostOp *> rem;
+  for (const auto &o : ops) rem.push_back(&o);
+  size_t head = 0;  // rem[head..] still to place
+  while (head < rem.size()) {
+    const HostOp &first = *rem[head];
+    const bool first_fusable =
+        !(first.kind == kOpDense && first.tbits.size() > size_t(kRegBits)) &&
+        !(first.kind == kOpDiag && first.tbits.size() > size_t(kMaxDiagK));
+    if (!first_fusable) {
+      PlannedLaunch pl;
+      pl.is_sweep = false;
+      pl.gate = first;
+      out.push_back(std::move(pl));
+      ++head;
+      continue;
+    }
+    SweepBuilder sb(n, m, l);
+    std::vector<const HostOp *> skipped;
+    uint64_t blockT = 0, blockAll = 0;  // non-diagonal / all bits of skipped gates
+    size_t i = head;
+    for (; i < rem.size(); ++i) {
+      const HostOp &op = *rem[i];
+      const uint64_t T = op.nondiag_mask(), A = op.touched_mask();
+      const bool commutes = (T & blockAll) == 0 && (A & blockT) == 0;
+      if (commutes && sb.try_add(op)) continue;
+      if (!opt.reorder) break;
+      skipped.push_back(&op);
+      blockT |= T;
+      blockAll |= A;
+      if (skipped.size() >= kWindow || popc64(blockT) >= int(n)) {
+        ++i;
+        break;
+      }
+    }
+    if (sb.ops.empty()) throw std::logic_error("planner: first gate does not fit an empty sweep");
+    PlannedLaunch pl;
+    pl.is_sweep = true;
+    pl.sweep = sb.finish();
+    out.push_back(std::move(pl));
+    // Remaining = skipped (in order) + everything after i.
+    std::vector<const HostOp *> next(skipped.begin(), skipped.end());
+    next.insert(next.end(), rem.begin() + i, rem.end());
+    rem.swap(next);
+    head = 0;
+  }
+  return out;
+}
+
+}  // namespace sq

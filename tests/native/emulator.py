@@ -1,0 +1,42 @@
+"""ctypes wrapper for the test-only plan emulator (tests/native)."""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from tests.native.build import build  # noqa: E402
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(build())
+        _lib.emu_run.restype = ctypes.c_int
+    return _lib
+
+
+def run(state, n, gates, tile_bits=12, reorder=True):
+    """gates: list of (matrix, qubits, controls, control_values). Returns
+    (state, sweeps, unfused)."""
+    psi = np.array(state, dtype=np.complex128)
+    k, qoff, qs, nc, coff, cs, cv, moff, mats = [], [], [], [], [], [], [], [], []
+    mo = 0
+    for m, q, c, v in gates:
+        k.append(len(q)); qoff.append(len(qs)); qs.extend(q)
+        nc.append(len(c)); coff.append(len(cs)); cs.extend(c); cv.extend(v)
+        moff.append(mo); mats.append(np.asarray(m, dtype=np.complex128).ravel()); mo += mats[-1].size
+    arr = lambda x, t: np.ascontiguousarray(np.array(x if x else [0], dtype=t))
+    K, QO, QS, NC, CO, CS, CV = (arr(x, np.int32) for x in (k, qoff, qs, nc, coff, cs, cv))
+    MO = arr(moff, np.int64)
+    M = np.ascontiguousarray(np.concatenate(mats) if mats else np.zeros(1, np.complex128))
+    unf = ctypes.c_int(0)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    r = lib().emu_run(P(psi), n, len(gates), P(K), P(QO), P(QS), P(NC), P(CO), P(CS), P(CV),
+                      P(MO), P(M), tile_bits, int(reorder), ctypes.byref(unf))
+    if r < 0:
+        raise RuntimeError("emulator failed")
+    return psi, r, unf.value

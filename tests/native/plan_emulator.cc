@@ -1,0 +1,186 @@
+// TEST ONLY: executes the engine's fusion plans on the host, thread by
+// thread, with the same index arithmetic as sweep_kernel / gate_kernel
+// (snuqs_b200/csrc/sweep_kernels.cuh), so the planner and the gate analysis
+// can be checked against the oracle on a machine without a GPU.  It is built
+// into tests/native/libplan_emulator.so by tests/native/build.py and is never
+// linked into the product.
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "host_ops.h"
+
+using namespace sq;
+
+namespace {
+
+uint64_t insert_zero(uint64_t x, uint32_t p) {
+  const uint64_t lo = x & ((uint64_t(1) << p) - 1);
+  return ((x >> p) << (p + 1)) | lo;
+}
+
+void emulate_sweep(cplx *psi, const PlannedSweep &ps) {
+  const SweepHeader &h = ps.h;
+  const uint32_t m = h.m, l = h.l, nthr = 1u << (m - kRegBits);
+  std::vector<uint64_t> hitab(size_t(1) << (m - l));
+  for (uint32_t c = 0; c < hitab.size(); ++c) {
+    uint64_t a = 0;
+    for (uint32_t i = 0; i < m - l; ++i)
+      if ((c >> i) & 1) a |= uint64_t(1) << h.hi[i];
+    hitab[c] = a;
+  }
+  auto addr = [&](uint64_t gbase, uint32_t j) {
+    return gbase | hitab[j >> l] | (j & ((1u << l) - 1));
+  };
+  std::vector<cplx> tile(size_t(1) << m);
+  for (uint64_t t = 0; t < h.num_tiles; ++t) {
+    uint64_t gbase = t << l;
+    for (uint32_t i = 0; i < m - l; ++i) gbase = insert_zero(gbase, h.hi[i]);
+    for (uint32_t j = 0; j < (1u << m); ++j) tile[j] = psi[addr(gbase, j)];
+    for (uint32_t p = 0; p < h.nphases; ++p) {
+      const SweepPhase &ph = ps.ph[p];
+      for (uint32_t tid = 0; tid < nthr; ++tid) {
+        uint32_t jb = tid;
+        for (int b = 0; b < kRegBits; ++b) jb = uint32_t(insert_zero(jb, ph.reg[b]));
+        cplx v[kRegAmps];
+        uint32_t jj[kRegAmps];
+        for (int ri = 0; ri < kRegAmps; ++ri) {
+          uint32_t j = jb;
+          for (int b = 0; b < kRegBits; ++b)
+            if ((ri >> b) & 1) j |= 1u << ph.reg[b];
+          jj[ri] = j;
+          v[ri] = tile[j];
+        }
+        for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+          const SweepOp &op = ps.op[o];
+          const cplx *c = ps.coef.data() + op.coef;
+          if (op.kind == kOpDiag) {
+            for (int ri = 0; ri < kRegAmps; ++ri) {
+              uint32_t idx = 0;
+              for (int tt = 0; tt < op.k; ++tt) {
+                int bit;
+                if (op.dsrc[tt] == kSrcGlobal) bit = (gbase >> op.dpos[tt]) & 1;
+                else if (op.dsrc[tt] == kSrcLocal) bit = (jb >> op.dpos[tt]) & 1;
+                else bit = (ri >> op.dpos[tt]) & 1;
+                if (bit) idx |= 1u << (op.k - 1 - tt);
+              }
+              v[ri] *= c[idx];
+            }
+          } else {
+            const bool tok = ((gbase & op.gmask) == op.gval) && ((jb & op.lmask) == op.lval);
+            const int V = op.vmask, K = __builtin_popcount(V), D = 1 << K;
+            for (int g = 0; g < kRegAmps; ++g) {
+              if (g & V) continue;
+              if (!(tok && ((g & op.rmask) == op.rval))) continue;
+              auto dep = [&](int x) {
+                int r = 0, b = 0;
+                for (int pp = 0; pp < 4; ++pp)
+                  if (V & (1 << pp)) {
+                    if (x & (1 << b)) r |= 1 << pp;
+                    ++b;
+                  }
+                return r;
+              };
+              cplx a[16], out[16];
+              for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
+              for (int r = 0; r < D; ++r) {
+                cplx s = c[r * D] * a[0];
+                for (int x = 1; x < D; ++x) s += c[r * D + x] * a[x];
+                out[r] = s;
+              }
+              for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
+            }
+          }
+        }
+        for (int ri = 0; ri < kRegAmps; ++ri) tile[jj[ri]] = v[ri];
+      }
+    }
+    for (uint32_t j = 0; j < (1u << m); ++j) psi[addr(gbase, j)] = tile[j];
+  }
+}
+
+void emulate_gate(cplx *psi, uint32_t n, const HostOp &op0) {
+  HostOp op = op0;
+  if (op.kind == kOpDiag) {  // as the engine does: expand to dense
+    const size_t D = op.m.size();
+    std::vector<cplx> d(D * D, cplx(0, 0));
+    for (size_t i = 0; i < D; ++i) d[i * D + i] = op.m[i];
+    op.m = d;
+  }
+  const int k = int(op.tbits.size()), D = 1 << k;
+  std::vector<int> sorted(op.tbits);
+  std::sort(sorted.begin(), sorted.end());
+  std::vector<uint64_t> off(D);
+  for (int x = 0; x < D; ++x) {
+    uint64_t o = 0;
+    for (int j = 0; j < k; ++j)
+      if ((x >> (k - 1 - j)) & 1) o |= uint64_t(1) << op.tbits[j];
+    off[x] = o;
+  }
+  std::vector<cplx> a(D);
+  for (uint64_t g = 0; g < ((uint64_t(1) << n) >> k); ++g) {
+    uint64_t base = g;
+    for (int j = 0; j < k; ++j) base = insert_zero(base, sorted[j]);
+    if ((base & op.cmask) != op.cval) continue;
+    for (int x = 0; x < D; ++x) a[x] = psi[base | off[x]];
+    for (int r = 0; r < D; ++r) {
+      cplx s = op.m[size_t(r) * D] * a[0];
+      for (int x = 1; x < D; ++x) s += op.m[size_t(r) * D + x] * a[x];
+      psi[base | off[r]] = s;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// ops: nops gates; gate i has k[i] targets at qubits[qoff[i]..], nc[i]
+// controls at controls[coff[i]..] with values cvals[coff[i]..], and its
+// 4^k matrix at mats[moff[i]..] (complex128).  Returns the number of fused
+// sweeps (>= 0) or -1 on error.
+int emu_run(double *state, int n, int nops, const int *k, const int *qoff, const int *qubits,
+            const int *nc, const int *coff, const int *controls, const int *cvals,
+            const long *moff, const double *mats, int tile_bits, int reorder,
+            int *unfused_out) {
+  try {
+    std::vector<HostOp> ops;
+    for (int i = 0; i < nops; ++i) {
+      std::vector<int> tb;
+      for (int j = 0; j < k[i]; ++j) tb.push_back(n - 1 - qubits[qoff[i] + j]);
+      uint64_t cm = 0, cv = 0;
+      for (int j = 0; j < nc[i]; ++j) {
+        const uint64_t bit = uint64_t(1) << (n - 1 - controls[coff[i] + j]);
+        cm |= bit;
+        if (cvals[coff[i] + j]) cv |= bit;
+      }
+      const size_t d = size_t(1) << k[i];
+      std::vector<cplx> mm(d * d);
+      std::memcpy(mm.data(), mats + 2 * moff[i], d * d * sizeof(cplx));
+      HostOp h;
+      if (analyse_op(mm, tb, cm, cv, h)) ops.push_back(h);
+    }
+    PlanOptions opt;
+    opt.tile_bits = uint32_t(tile_bits);
+    opt.reorder = reorder != 0;
+    auto plan = plan_sweeps(ops, uint32_t(n), opt);
+    int sweeps = 0, unfused = 0;
+    cplx *psi = reinterpret_cast<cplx *>(state);
+    for (const auto &pl : plan) {
+      if (pl.is_sweep) {
+        emulate_sweep(psi, pl.sweep);
+        ++sweeps;
+      } else {
+        emulate_gate(psi, uint32_t(n), pl.gate);
+        ++unfused;
+      }
+    }
+    if (unfused_out) *unfused_out = unfused;
+    return sweeps;
+  } catch (const std::exception &) {
+    return -1;
+  }
+}
+
+}  // extern "C"

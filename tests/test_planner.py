@@ -1,0 +1,79 @@
+"""Host logic of the fused path, no GPU: the fusion planner and the gate
+structure analysis, executed by the test-only plan emulator
+(tests/native/plan_emulator.cc) with the kernels' index arithmetic, against
+the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from snuqs_b200 import circuits
+from tests.native import emulator
+
+
+def gates_of(ops):
+    return [(circuits.op_matrix(op, oracle.gate_matrix), op[1], [], []) for op in ops]
+
+
+@pytest.mark.parametrize("n", [4, 5, 7, 9, 11, 12, 13, 15])
+@pytest.mark.parametrize("reorder", [True, False])
+def test_plans_match_oracle_all_gates(n, reorder):
+    for seed in range(2):
+        ops = circuits.random_all_gates(n, 120, seed=seed)
+        ref = oracle.run_ops(ops, n)
+        for tb in (12, 9):
+            psi, sweeps, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops), tb, reorder)
+            assert np.abs(psi - ref).max() <= 1e-12, (n, seed, tb)
+
+
+def test_plans_match_oracle_golden(golden_circuits):
+    for key, (n, ops, ref) in golden_circuits.items():
+        psi, _, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops))
+        assert np.abs(psi - ref).max() <= 1e-12, key
+
+
+def test_fusion_packs_many_gates_per_sweep():
+    ops = circuits.random_mix(20, 400, seed=1234)
+    ref = oracle.run_ops(ops, 20)
+    psi, sweeps, unfused = emulator.run(oracle.basis_state(20), 20, gates_of(ops))
+    assert np.abs(psi - ref).max() <= 1e-12
+    assert unfused == 0
+    assert sweeps <= 40  # >= 10 gates per sweep
+
+
+def test_controls_and_large_unitaries():
+    rng = np.random.default_rng(9)
+    n = 11
+    gates = []
+    for i in range(40):
+        k = int(rng.integers(1, 6))  # up to 5 targets: k = 5 takes the unfused path
+        qs = [int(x) for x in rng.choice(n, size=k + 2, replace=False)]
+        u = circuits.haar_unitary(1 << k, rng)
+        nc = int(rng.integers(0, 3))
+        ctrl, vals = qs[k:k + nc], [int(v) for v in rng.integers(0, 2, size=nc)]
+        gates.append((u, qs[:k], ctrl, vals))
+    psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    ref = psi0.copy()
+    for u, q, c, v in gates:
+        # controlled(u) as a dense matrix over controls + targets
+        kk = len(c) + len(q)
+        D = 1 << kk
+        full = np.eye(D, dtype=np.complex128)
+        cidx = int("".join(map(str, v)), 2) if c else 0
+        blk = cidx << len(q)
+        full[blk:blk + (1 << len(q)), blk:blk + (1 << len(q))] = u
+        oracle.apply_matrix(ref, n, full, list(c) + list(q))
+    psi, sweeps, unfused = emulator.run(psi0, n, gates)
+    assert np.abs(psi - ref).max() <= 1e-12
+    assert unfused > 0
+
+
+def test_diagonal_and_identity_gates_fold():
+    n = 10
+    ops = [("Hadamard", (q,), ()) for q in range(n)]
+    ops += [("RotZ", (q,), (0.1 * q,)) for q in range(n)]
+    ops += [("ZZ", (q, (q + 3) % n), (0.3,)) for q in range(n)]
+    ops += [("Identity", (2,), ()), ("GPhase", (), (0.25,)), ("CPhaseShift10", (1, 7), (1.0,))]
+    ref = oracle.run_ops(ops, n)
+    psi, sweeps, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops))
+    assert np.abs(psi - ref).max() <= 1e-12
+    assert sweeps == 1
