@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--tile-bits", type=int, default=0, help="override the engine's tile size")
     return p.parse_args()
 
 
@@ -245,6 +246,8 @@ def _run_ours(args, rank, world, local):
 
     st = capi.State(n, dtype, stream=stream)
     st.init_basis(0)
+    if args.tile_bits:
+        st.set_option(capi.SQ_OPT_TILE_BITS, args.tile_bits)
 
     def step():
         for op, m in zip(ops, mats):

@@ -26,6 +26,13 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ENGINE_CU = ["engine.cu"]
 ENGINE_CC = ["gates.cc", "planner.cc"]
+# Fused-sweep kernel instantiations: (precision, tile bits, CTAs per SM).
+# Tile sizes must match kTileBitsC128 / kTileBitsC64 in csrc/sq_plan.h; the
+# CTA counts keep registers <= 65536 / (CTAs x threads).
+SWEEP_INSTANCES = [
+    ("double", 4, 1), ("double", 7, 1), ("double", 10, 6), ("double", 11, 3), ("double", 12, 1),
+    ("float", 4, 1), ("float", 7, 1), ("float", 10, 8), ("float", 12, 2),
+]
 LIB = os.path.join(HERE, "libsnuqs_b200.so")
 
 
@@ -67,6 +74,24 @@ def build(force: bool = False, verbose: bool = False) -> None:
             _run([NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
                   "-Xptxas", "-warn-spills", "-c", src, "-o", obj])
         objs.append(obj)
+    jobs = []
+    inst_src = os.path.join(CSRC, "sweep_inst.cu")
+    for real, m, minb in SWEEP_INSTANCES:
+        obj = os.path.join(BUILD, f"sweep_{real}_{m}.o")
+        if force or _stale(obj, [inst_src] + hdrs):
+            cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
+                   f"-DSQ_REAL={real}", f"-DSQ_M={m}", f"-DSQ_MINB={minb}",
+                   "-Xptxas", "-warn-spills", "-c", inst_src, "-o", obj]
+            jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                               stderr=subprocess.STDOUT, text=True)))
+        objs.append(obj)
+    for cmd, proc in jobs:
+        out, _ = proc.communicate()
+        if proc.returncode != 0:
+            sys.stderr.write(" ".join(cmd) + "\n" + out)
+            raise RuntimeError("build step failed: " + cmd[-1])
+        if verbose and out.strip():
+            print(out.strip())
     for f in ENGINE_CC:
         src = os.path.join(CSRC, f)
         obj = os.path.join(BUILD, f + ".o")

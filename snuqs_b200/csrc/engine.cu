@@ -17,6 +17,7 @@
 #include "host_ops.h"
 #include "reduce_kernels.cuh"
 #include "sweep_kernels.cuh"
+#include "sweep_registry.h"
 
 using sq::cplx;
 
@@ -66,7 +67,7 @@ struct sq_state {
   bool owns = true;
   int device = 0;
   int fusion = 1;
-  uint32_t tile_bits = sq::kMaxTileBits;
+  uint32_t tile_bits = 0;  // 0: the precision's default
   int reorder = 1;
   std::vector<PendingOp> pending;
   double *scratch = nullptr;  // reduction partials + result
@@ -91,6 +92,54 @@ struct DeviceInfo {
 static std::mutex g_dev_mu;
 static std::map<int, DeviceInfo> g_devs;
 
+// Compiled sweep kernel for (precision, tile bits m); nullptr if none.
+template <typename Real>
+static const void *sweep_fn(uint32_t m) {
+  if constexpr (sizeof(Real) == 8) {
+    switch (m) {
+      case 4: return SQ_SWEEP_PTR_NAME(double, 4)();
+      case 7: return SQ_SWEEP_PTR_NAME(double, 7)();
+      case 10: return SQ_SWEEP_PTR_NAME(double, 10)();
+      case 11: return SQ_SWEEP_PTR_NAME(double, 11)();
+      case 12: return SQ_SWEEP_PTR_NAME(double, 12)();
+    }
+  } else {
+    switch (m) {
+      case 4: return SQ_SWEEP_PTR_NAME(float, 4)();
+      case 7: return SQ_SWEEP_PTR_NAME(float, 7)();
+      case 10: return SQ_SWEEP_PTR_NAME(float, 10)();
+      case 12: return SQ_SWEEP_PTR_NAME(float, 12)();
+    }
+  }
+  return nullptr;
+}
+
+// Largest compiled tile size <= min(n, requested).
+static uint32_t pick_tile_bits(int dtype, uint32_t n, uint32_t requested) {
+  const uint32_t cap = std::min(n, requested);
+  uint32_t best = 0;
+  if (dtype == SQ_C64) {
+    for (int m : sq::kTileBitsC64)
+      if (uint32_t(m) <= cap) best = uint32_t(m);
+  } else {
+    for (int m : sq::kTileBitsC128)
+      if (uint32_t(m) <= cap) best = uint32_t(m);
+  }
+  return best;
+}
+
+template <typename Real>
+static int set_sweep_attributes() {
+  for (uint32_t m = 4; m <= uint32_t(sq::kMaxTileBits); ++m) {
+    const void *fn = sweep_fn<Real>(m);
+    if (!fn) continue;
+    const int max_smem = 2 * (1 << m) * int(2 * sizeof(Real)) + sq::kMaxCoef * int(2 * sizeof(Real)) +
+                         (1 << m) * 8;
+    SQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  }
+  return SQ_OK;
+}
+
 static int device_info(int dev, DeviceInfo &out) {
   std::lock_guard<std::mutex> lk(g_dev_mu);
   auto it = g_devs.find(dev);
@@ -101,11 +150,8 @@ static int device_info(int dev, DeviceInfo &out) {
   DeviceInfo di;
   SQ_CUDA(cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, dev));
   // Kernel attributes are per device; set them while we hold the lock.
-  const int max_smem = (1 << sq::kMaxTileBits) * 16 + sq::kMaxCoef * 16 + 1024 * 8;
-  SQ_CUDA(cudaFuncSetAttribute(sq::sweep_kernel<double>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-  SQ_CUDA(cudaFuncSetAttribute(sq::sweep_kernel<float>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  SQ_TRY(set_sweep_attributes<double>());
+  SQ_TRY(set_sweep_attributes<float>());
   SQ_CUDA(cudaFuncSetAttribute(sq::gate_kernel_large<double>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, 1024 * 16));
   SQ_CUDA(cudaFuncSetAttribute(sq::gate_kernel_large<float>,
@@ -137,11 +183,13 @@ static int launch_sweep(sq_state *s, const sq::PlannedSweep &ps, cudaStream_t st
   }
   const uint32_t m = ps.h.m, l = ps.h.l;
   const int threads = 1 << (m - sq::kRegBits);
-  const size_t smem = (size_t(1) << m) * sizeof(C2) + size_t((ps.h.ncoef + 1) & ~1u) * sizeof(C2) +
+  const size_t smem = 2 * (size_t(1) << m) * sizeof(C2) +
+                      size_t((ps.h.ncoef + 1) & ~1u) * sizeof(C2) +
                       (size_t(1) << (m - l)) * sizeof(uint64_t);
   int per_sm = 0;
-  SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sq::sweep_kernel<Real>, threads,
-                                                        smem));
+  const void *fn = sweep_fn<Real>(m);
+  if (!fn) return fail(SQ_ERR_INVALID, "internal: no sweep kernel for %u tile bits", m);
+  SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
   if (per_sm < 1) per_sm = 1;
   const uint64_t grid = std::min<uint64_t>(ps.h.num_tiles, uint64_t(per_sm) * di.sms);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -150,8 +198,9 @@ static int launch_sweep(sq_state *s, const sq::PlannedSweep &ps, cudaStream_t st
     SQ_CUDA(cudaEventCreate(&e1));
     SQ_CUDA(cudaEventRecord(e0, st));
   }
-  sq::sweep_kernel<Real><<<unsigned(grid), threads, smem, st>>>(reinterpret_cast<C2 *>(s->data),
-                                                                *P);
+  C2 *psi = reinterpret_cast<C2 *>(s->data);
+  void *args[] = {&psi, P.get()};
+  SQ_CUDA(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(threads), args, smem, st));
   SQ_CUDA(cudaGetLastError());
   if (s->timing) {
     SQ_CUDA(cudaEventRecord(e1, st));
@@ -266,6 +315,7 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
   SQ_TRY(device_info(s->device, di));
   const uint32_t n = s->n;
   const bool fused = s->fusion && n >= uint32_t(sq::kRegBits);
+  const bool c64 = s->dtype == SQ_C64;
   std::vector<sq::HostOp> ops;
   ops.reserve(s->pending.size());
   for (const PendingOp &p : s->pending) {
@@ -291,7 +341,6 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
     }
   }
   s->pending.clear();
-  const bool c64 = s->dtype == SQ_C64;
   if (!fused) {
     for (const auto &op : ops) {
       SQ_TRY(c64 ? launch_gate<float>(s->data, n, op, nullptr, st, di.sms)
@@ -303,8 +352,10 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
   std::vector<sq::PlannedLaunch> plan;
   try {
     sq::PlanOptions opt;
-    opt.tile_bits = s->tile_bits;
+    opt.tile_bits = pick_tile_bits(s->dtype, n, s->tile_bits);
+    if (opt.tile_bits < uint32_t(sq::kRegBits)) return fail(SQ_ERR_INVALID, "internal: no tile size");
     opt.reorder = s->reorder != 0;
+    opt.max_dense_k = c64 ? 4 : 3;
     plan = sq::plan_sweeps(ops, n, opt);
   } catch (const std::exception &e) {
     return fail(SQ_ERR_INVALID, "planner: %s", e.what());
@@ -440,6 +491,7 @@ int sq_state_create(uint32_t num_qubits, int dtype, sq_state **out) {
   auto s = std::make_unique<sq_state>();
   s->n = num_qubits;
   s->dtype = dtype;
+  s->tile_bits = dtype == SQ_C64 ? sq::kDefaultTileBitsC64 : sq::kDefaultTileBitsC128;
   SQ_CUDA(cudaGetDevice(&s->device));
   const size_t bytes = (size_t(1) << num_qubits) * amp_bytes(dtype);
   SQ_CUDA(cudaMalloc(&s->data, bytes));
@@ -457,6 +509,7 @@ int sq_state_wrap(void *device_ptr, uint32_t num_qubits, int dtype, sq_state **o
   s->dtype = dtype;
   s->data = device_ptr;
   s->owns = false;
+  s->tile_bits = dtype == SQ_C64 ? sq::kDefaultTileBitsC64 : sq::kDefaultTileBitsC128;
   SQ_CUDA(cudaGetDevice(&s->device));
   *out = s.release();
   return SQ_OK;

@@ -58,6 +58,10 @@ struct PlannedLaunch {
 struct PlanOptions {
   uint32_t tile_bits = kMaxTileBits;
   bool reorder = true;
+  // Widest dense gate a sweep may carry in registers: 3 for complex128 (a
+  // 4-qubit dense matrix needs a second copy of all 16 amplitudes), 4 for
+  // complex64.  Wider dense gates run unfused.
+  uint32_t max_dense_k = 3;
 };
 
 // Packs ops (in circuit order) into fused sweeps for an n-qubit state.

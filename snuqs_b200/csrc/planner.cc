@@ -24,7 +24,7 @@ namespace {
 int popc64(uint64_t x) { return __builtin_popcountll(x); }
 
 struct SweepBuilder {
-  uint32_t n, m, l;
+  uint32_t n, m, l, max_dense_k = 3;
   uint64_t S;  // tile bits (global index bits)
   std::vector<const HostOp *> ops;
   std::vector<uint64_t> phase_regs;  // register bits (global) of each phase
@@ -53,7 +53,7 @@ struct SweepBuilder {
       ncoef += coef_count(op);
       return true;
     }
-    if (op.tbits.size() > size_t(kRegBits)) return false;
+    if (op.tbits.size() > size_t(max_dense_k)) return false;
     const uint64_t T = op.target_mask();
     if (uint32_t(popc64(S | T)) > m) return false;
     const bool new_phase = phase_regs.empty() || popc64(phase_regs.back() | T) > kRegBits;
@@ -75,6 +75,70 @@ struct SweepBuilder {
 
 // Position of global bit b within the ascending bit list of mask.
 int rank_in(uint64_t mask, int b) { return popc64(mask & ((uint64_t(1) << b) - 1)); }
+
+// Picks the cheapest sweep-op kind for a dense k-qubit matrix in canonical
+// order and appends its coefficients.
+void encode_dense(SweepOp &so, const std::vector<cplx> &cm, int k, std::vector<cplx> &coef) {
+  const int d = 1 << k;
+  auto M = [&](int r, int c) { return cm[size_t(r) * d + c]; };
+  const cplx zero(0, 0), one(1, 0);
+  if (k == 1 && M(0, 0) == zero && M(1, 1) == zero) {
+    so.kind = kSwAnti1;
+    if (M(0, 1) == one && M(1, 0) == one) so.aux |= kAuxPure;
+    coef.push_back(M(0, 1));
+    coef.push_back(M(1, 0));
+    return;
+  }
+  if (k == 2) {
+    bool swap2 = M(0, 0) == one && M(3, 3) == one && M(1, 2) != zero && M(2, 1) != zero;
+    for (int r = 0; r < 4 && swap2; ++r)
+      for (int c = 0; c < 4; ++c) {
+        const bool keep = (r == c && (r == 0 || r == 3)) || (r == 1 && c == 2) || (r == 2 && c == 1);
+        if (!keep && M(r, c) != zero) swap2 = false;
+      }
+    if (swap2) {
+      so.kind = kSwSwap2;
+      if (M(1, 2) == one && M(2, 1) == one) so.aux |= kAuxPure;
+      coef.push_back(M(1, 2));
+      coef.push_back(M(2, 1));
+      return;
+    }
+  }
+  if (k <= 2) {
+    // c_r a_r + f s_r a_(r^x): real diagonal, one partner column per row, all
+    // partner entries real or all imaginary.
+    int x = 0;
+    bool ok = true;
+    for (int r = 0; r < d && ok; ++r) {
+      if (M(r, r).imag() != 0) ok = false;
+      for (int c = 0; c < d && ok; ++c)
+        if (c != r && M(r, c) != zero) {
+          if (x == 0) x = r ^ c;
+          else if ((r ^ c) != x) ok = false;
+        }
+    }
+    if (ok && x != 0) {
+      bool all_re = true, all_im = true;
+      for (int r = 0; r < d; ++r) {
+        const cplx v = M(r, r ^ x);
+        if (v.imag() != 0) all_re = false;
+        if (v.real() != 0) all_im = false;
+      }
+      if (all_re || all_im) {
+        so.kind = kSwXRot;
+        so.aux |= uint8_t(x);
+        if (!all_re) so.aux |= kAuxImag;
+        for (int r = 0; r < d; ++r) {
+          const cplx v = M(r, r ^ x);
+          coef.push_back(cplx(M(r, r).real(), all_re ? v.real() : v.imag()));
+        }
+        return;
+      }
+    }
+  }
+  so.kind = kSwDense;
+  coef.insert(coef.end(), cm.begin(), cm.end());
+}
 
 PlannedSweep SweepBuilder::finish() const {
   PlannedSweep ps;
@@ -130,30 +194,75 @@ PlannedSweep SweepBuilder::finish() const {
         if (ph.reg[r] == pos) return r;
       return -1;
     };
+    // Route a condition bit (global bit b must equal v) to the register,
+    // tile-local or global masks.
+    auto add_cond = [&](SweepOp &so, int b, uint64_t v) {
+      const int r = regof(b);
+      if (r >= 0) {
+        so.rmask |= uint8_t(1u << r);
+        if (v) so.rval |= uint8_t(1u << r);
+      } else if ((tile >> b) & 1) {
+        const int pos = rank_in(tile, b);
+        so.lmask |= 1u << pos;
+        if (v) so.lval |= 1u << pos;
+      } else {
+        so.gmask |= uint64_t(1) << b;
+        if (v) so.gval |= uint64_t(1) << b;
+      }
+    };
     for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
       const HostOp &op = *ops[oi];
       SweepOp so;
       std::memset(&so, 0, sizeof(so));
-      so.kind = op.kind;
       so.k = uint8_t(op.tbits.size());
       so.coef = uint32_t(ps.coef.size());
       const int k = int(op.tbits.size());
       if (op.kind == kOpDiag) {
-        for (int t = 0; t < k; ++t) {
-          const int b = op.tbits[t];
-          const int r = regof(b);
-          if (r >= 0) {
-            so.dsrc[t] = kSrcReg;
-            so.dpos[t] = uint8_t(r);
-          } else if ((tile >> b) & 1) {
-            so.dsrc[t] = kSrcLocal;
-            so.dpos[t] = uint8_t(rank_in(tile, b));
-          } else {
-            so.dsrc[t] = kSrcGlobal;
-            so.dpos[t] = uint8_t(b);
+        int nonone = 0, e = -1;
+        for (size_t x = 0; x < op.m.size(); ++x)
+          if (op.m[x] != cplx(1, 0)) ++nonone, e = int(x);
+        if (nonone == 1) {
+          so.kind = kSwPhase;
+          for (int t = 0; t < k; ++t) add_cond(so, op.tbits[t], (e >> (k - 1 - t)) & 1);
+          if (op.m[e] == cplx(-1, 0)) so.aux |= kAuxPure;
+          ps.coef.push_back(op.m[e]);
+        } else {
+          so.kind = kSwDiag;
+          // Register targets -> canonical low index bits; the rest -> high
+          // bits, most significant first.
+          uint32_t vmask = 0;
+          for (int t = 0; t < k; ++t) {
+            const int r = regof(op.tbits[t]);
+            if (r >= 0) vmask |= 1u << r;
           }
+          const int nreg = __builtin_popcount(vmask);
+          int newbit[kMaxDiagK];
+          int nd = 0;
+          for (int t = 0; t < k; ++t) {
+            const int b = op.tbits[t];
+            const int r = regof(b);
+            if (r >= 0) {
+              newbit[t] = __builtin_popcount(vmask & ((1u << r) - 1));
+            } else {
+              so.dsrc[nd] = ((tile >> b) & 1) ? kSrcLocal : kSrcGlobal;
+              so.dpos[nd] = uint8_t(((tile >> b) & 1) ? rank_in(tile, b) : b);
+              newbit[t] = -1 - nd;  // placeholder: fixed below
+              ++nd;
+            }
+          }
+          for (int t = 0; t < k; ++t)
+            if (newbit[t] < 0) newbit[t] = nreg + (nd - 1 - (-1 - newbit[t]));
+          so.ndt = uint8_t(nd);
+          so.vmask = uint8_t(vmask);
+          std::vector<cplx> cd(op.m.size());
+          for (size_t x = 0; x < op.m.size(); ++x) {
+            size_t y = 0;
+            for (int t = 0; t < k; ++t)
+              if ((x >> (k - 1 - t)) & 1) y |= size_t(1) << newbit[t];
+            cd[y] = op.m[x];
+          }
+          ps.coef.insert(ps.coef.end(), cd.begin(), cd.end());
         }
-        ps.coef.insert(ps.coef.end(), op.m.begin(), op.m.end());
       } else {
         // Target j (matrix bit k-1-j) sits at register position rp[j]; the
         // kernel's canonical order has matrix bit i <-> i-th set bit of vmask.
@@ -177,24 +286,11 @@ PlannedSweep SweepBuilder::finish() const {
         };
         for (int r = 0; r < d; ++r)
           for (int c = 0; c < d; ++c) cm[size_t(remap(r)) * d + remap(c)] = op.m[size_t(r) * d + c];
-        ps.coef.insert(ps.coef.end(), cm.begin(), cm.end());
-        for (int b = 0; b < 64; ++b) {
-          if (!((op.cmask >> b) & 1)) continue;
-          const uint64_t v = (op.cval >> b) & 1;
-          const int r = regof(b);
-          if (r >= 0) {
-            so.rmask |= uint8_t(1u << r);
-            if (v) so.rval |= uint8_t(1u << r);
-          } else if ((tile >> b) & 1) {
-            const int pos = rank_in(tile, b);
-            so.lmask |= 1u << pos;
-            if (v) so.lval |= 1u << pos;
-          } else {
-            so.gmask |= uint64_t(1) << b;
-            if (v) so.gval |= uint64_t(1) << b;
-          }
-        }
+        for (int b = 0; b < 64; ++b)
+          if ((op.cmask >> b) & 1) add_cond(so, b, (op.cval >> b) & 1);
+        encode_dense(so, cm, k, ps.coef);
       }
+      so.code = uint8_t(sq_op_code(so.kind, so.vmask, so.aux));
       ps.op.push_back(so);
     }
   }
@@ -209,10 +305,12 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
                                        const PlanOptions &opt) {
   std::vector<PlannedLaunch> out;
   if (n < uint32_t(kRegBits)) throw std::invalid_argument("fused sweeps need n >= 4");
-  // A tile must hold the low bits plus one full register set.
-  const uint32_t want = std::max<uint32_t>(opt.tile_bits, kLowBits + kRegBits);
-  const uint32_t m = std::min<uint32_t>(std::min<uint32_t>(want, kMaxTileBits), n);
-  const uint32_t l = std::min<uint32_t>(kLowBits, m);
+  // The tile size is the compiled kernel's (opt.tile_bits <= n); the low
+  // contiguous bits leave at least one full register set free.
+  const uint32_t m = std::min<uint32_t>(opt.tile_bits, n);
+  if (m < uint32_t(kRegBits) || m > uint32_t(kMaxTileBits))
+    throw std::invalid_argument("tile bits out of range");
+  const uint32_t l = uint32_t(sweep_low_bits(int(m)));
   const size_t kWindow = 256;  // lookahead when reordering
 
   std::vector<const HostOp *> rem;
@@ -221,7 +319,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
   while (head < rem.size()) {
     const HostOp &first = *rem[head];
     const bool first_fusable =
-        !(first.kind == kOpDense && first.tbits.size() > size_t(kRegBits)) &&
+        !(first.kind == kOpDense && first.tbits.size() > size_t(std::min<uint32_t>(opt.max_dense_k, kRegBits))) &&
         !(first.kind == kOpDiag && first.tbits.size() > size_t(kMaxDiagK));
     if (!first_fusable) {
       PlannedLaunch pl;
@@ -232,6 +330,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       continue;
     }
     SweepBuilder sb(n, m, l);
+    sb.max_dense_k = std::min<uint32_t>(opt.max_dense_k, kRegBits);
     std::vector<const HostOp *> skipped;
     uint64_t blockT = 0, blockAll = 0;  // non-diagonal / all bits of skipped gates
     size_t i = head;

@@ -23,25 +23,80 @@ constexpr int kMaxOps = 64;
 constexpr int kMaxCoef = 1024;              // complex coefficients per sweep
 constexpr int kMaxDiagK = 8;                // targets of one diagonal op
 
+// HostOp kinds (structure analysis) ...
 enum OpKind : uint8_t { kOpDense = 1, kOpDiag = 2 };
+// ... and the specialised sweep-op kinds the planner encodes them as.  The
+// coefficient layout of each kind:
+//   kSwDense  4^k complex, canonical row-major (matrix bit b <-> b-th set bit
+//             of vmask)
+//   kSwDiag   2^k complex; index = (non-register target bits) << popc(vmask)
+//             | (register target bits in canonical order)
+//   kSwAnti1  p0, p1:            out0 = p0 a1, out1 = p1 a0
+//   kSwXRot   2^k (c_r, s_r) pairs stored as (re, im):
+//             out_r = c_r a_r + f s_r a_(r^x), f = i when aux & kAuxImag
+//   kSwSwap2  p12, p21:          out1 = p12 a2, out2 = p21 a1
+//   kSwPhase  p:                 a *= p where the op's condition holds
+enum SweepKind : uint8_t {
+  kSwDense = 1, kSwDiag = 2, kSwAnti1 = 3, kSwXRot = 4, kSwSwap2 = 5, kSwPhase = 6
+};
+enum SweepAux : uint8_t {
+  kAuxXMask = 3,  // XRot: partner XOR mask over the op's canonical local bits
+  kAuxImag = 4,   // XRot: f = i
+  kAuxPure = 8,   // Anti1/Swap2: unit phases (pure permutation); Phase: p = -1
+};
 enum DiagSrc : uint8_t { kSrcGlobal = 0, kSrcLocal = 1, kSrcReg = 2 };
+
+#ifdef __CUDACC__
+#define SQ_HD __host__ __device__
+#else
+#define SQ_HD
+#endif
+
+// Contiguous low index bits of a 2^m tile: 5 (chunks of 32 amplitudes, one
+// per warp) for m >= 9; smaller tiles keep 4 free bits for the registers.
+SQ_HD constexpr int sweep_low_bits(int m) { return m >= kLowBits + kRegBits ? kLowBits : m - kRegBits; }
+
+// Tile sizes with a compiled sweep kernel, per precision (ascending).
+constexpr int kTileBitsC128[] = {4, 7, 10, 11, 12};
+constexpr int kTileBitsC64[] = {4, 7, 10, 12};
+constexpr int kDefaultTileBitsC128 = 11;
+constexpr int kDefaultTileBitsC64 = 12;
+
+// Flat dispatch code of a sweep op: one switch in the kernel selects the
+// fully specialised routine (kind, register positions, partner mask, flags).
+SQ_HD constexpr int sq_log2_4(int v) { return v == 1 ? 0 : v == 2 ? 1 : v == 4 ? 2 : 3; }
+SQ_HD constexpr int sq_pair_index(int v) {  // two-bit masks of 4 positions
+  return v == 3 ? 0 : v == 5 ? 1 : v == 6 ? 2 : v == 9 ? 3 : v == 10 ? 4 : 5;
+}
+SQ_HD constexpr int sq_op_code(int kind, int v, int aux) {
+  return kind == kSwPhase ? 1 + ((aux & kAuxPure) ? 1 : 0)
+         : kind == kSwDiag ? 16 + v
+         : kind == kSwAnti1 ? 32 + sq_log2_4(v) + ((aux & kAuxPure) ? 4 : 0)
+         : kind == kSwSwap2 ? 40 + sq_pair_index(v) + ((aux & kAuxPure) ? 6 : 0)
+         : kind == kSwXRot
+             ? 52 + 2 * ((v & (v - 1)) == 0 ? sq_log2_4(v) : 4 + 3 * sq_pair_index(v) + (aux & 3) - 1) +
+                   ((aux & kAuxImag) ? 1 : 0)
+             : 96 + v;  // kSwDense
+}
 enum SweepFlags : uint32_t { kDirectLoad = 1u, kDirectStore = 2u };
 
 struct SweepOp {
-  uint8_t kind;    // kOpDense / kOpDiag
+  uint8_t kind;    // SweepKind
   uint8_t k;       // number of targets
-  uint8_t vmask;   // dense: register positions of the targets (bit p = register bit p)
-  uint8_t rmask;   // dense: register positions that are controls
+  uint8_t vmask;   // register positions of the targets (bit p = register bit p)
+  uint8_t rmask;   // register positions that are controls / phase conditions
   uint8_t rval;    //        and their required values
-  uint8_t pad0[3];
+  uint8_t aux;     // SweepAux flags
+  uint8_t ndt;     // kSwDiag: number of non-register targets (dsrc/dpos)
+  uint8_t code;    // sq_op_code(kind, vmask, aux)
   uint32_t coef;   // offset of the op's coefficients (complex units)
-  uint32_t lmask;  // dense: in-tile, non-register control bits (tile-local index)
+  uint32_t lmask;  // in-tile, non-register control bits (tile-local index)
   uint32_t lval;
   uint32_t pad1;
-  uint64_t gmask;  // dense: control bits outside the tile (global index)
+  uint64_t gmask;  // control bits outside the tile (global index)
   uint64_t gval;
-  // diag: target t (t = 0 is the most significant bit of the coefficient
-  // index) comes from a global bit, a tile-local bit or a register bit.
+  // kSwDiag: the non-register targets, most significant first: each from a
+  // global bit or a tile-local bit; `ndt` of them.
   uint8_t dsrc[kMaxDiagK];
   uint8_t dpos[kMaxDiagK];
 };

@@ -58,24 +58,57 @@ __device__ __forceinline__ constexpr int ct_dep(int x) {
   return r;
 }
 
-// Dense op on register positions V (canonical order: coefficient-index bit b
-// <-> the b-th set bit of V).  Row r of the output is accumulated left to
-// right over the columns, as the reference does.
-template <typename Real, int V>
-__device__ __forceinline__ void dense_op(Real (&re)[kRegAmps], Real (&im)[kRegAmps],
-                                         const typename Vec2<Real>::T *__restrict__ c,
-                                         int rmask, int rval, bool tok) {
-  constexpr int K = ct_popc<V>();
-  constexpr int D = 1 << K;
+// Compile-time extract of the bits of x at the set bits of mask V.
+template <int V>
+__device__ __forceinline__ constexpr int ct_ext(int x) {
+  int r = 0, b = 0;
+  for (int p = 0; p < 4; ++p)
+    if (V & (1 << p)) {
+      if (x & (1 << p)) r |= 1 << b;
+      ++b;
+    }
+  return r;
+}
+
+// Runs f(g) for every register group g (register index with the bits of V
+// clear).  Without register controls the loop is branch-free; with them each
+// group is predicated on its control bits.
+template <int V, class F>
+__device__ __forceinline__ void for_groups(int rmask, int rval, F &&f) {
+  if (rmask == 0) {
 #pragma unroll
-  for (int g = 0; g < kRegAmps; ++g) {
-    if (g & V) continue;
-    if (!(tok && ((g & rmask) == rval))) continue;
+    for (int g = 0; g < kRegAmps; ++g)
+      if (!(g & V)) f(g);
+  } else {
+#pragma unroll
+    for (int g = 0; g < kRegAmps; ++g)
+      if (!(g & V) && ((g & rmask) == rval)) f(g);
+  }
+}
+
+template <typename Real>
+struct Amps {
+  Real re[kRegAmps], im[kRegAmps];
+};
+
+// out = p * a (complex)
+template <typename Real>
+__device__ __forceinline__ void cmul(Real pr, Real pi, Real ar, Real ai, Real &o_r, Real &o_i) {
+  o_r = pr * ar - pi * ai;
+  o_i = pr * ai + pi * ar;
+}
+
+// kSwDense on register positions V: row r accumulated left to right.
+template <typename Real, int V>
+__device__ __forceinline__ void op_dense(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+                                         int rmask, int rval) {
+  constexpr int D = 1 << ct_popc<V>();
+  for_groups<V>(rmask, rval, [&](int g) {
     Real ar[D], ai[D];
 #pragma unroll
     for (int x = 0; x < D; ++x) {
-      ar[x] = re[g | ct_dep<V>(x)];
-      ai[x] = im[g | ct_dep<V>(x)];
+      ar[x] = A.re[g | ct_dep<V>(x)];
+      ai[x] = A.im[g | ct_dep<V>(x)];
     }
 #pragma unroll
     for (int r = 0; r < D; ++r) {
@@ -90,59 +123,186 @@ __device__ __forceinline__ void dense_op(Real (&re)[kRegAmps], Real (&im)[kRegAm
         si = fma(m.x, ai[x], si);
         si = fma(m.y, ar[x], si);
       }
-      re[g | ct_dep<V>(r)] = sr;
-      im[g | ct_dep<V>(r)] = si;
+      A.re[g | ct_dep<V>(r)] = sr;
+      A.im[g | ct_dep<V>(r)] = si;
     }
+  });
+}
+
+// kSwAnti1 on register bit V: out0 = p0 a1, out1 = p1 a0 (a swap when pure).
+template <typename Real, int V, bool PURE>
+__device__ __forceinline__ void op_anti1(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+                                         int rmask, int rval) {
+  if constexpr (PURE) {
+    for_groups<V>(rmask, rval, [&](int g) {
+      const Real tr = A.re[g], ti = A.im[g];
+      A.re[g] = A.re[g | V];
+      A.im[g] = A.im[g | V];
+      A.re[g | V] = tr;
+      A.im[g | V] = ti;
+    });
+  } else {
+    const auto p0 = c[0], p1 = c[1];
+    for_groups<V>(rmask, rval, [&](int g) {
+      const Real a0r = A.re[g], a0i = A.im[g], a1r = A.re[g | V], a1i = A.im[g | V];
+      cmul(p0.x, p0.y, a1r, a1i, A.re[g], A.im[g]);
+      cmul(p1.x, p1.y, a0r, a0i, A.re[g | V], A.im[g | V]);
+    });
   }
 }
 
-template <typename Real>
-__device__ __forceinline__ void dense_dispatch(int v, Real (&re)[kRegAmps], Real (&im)[kRegAmps],
-                                               const typename Vec2<Real>::T *c, int rmask,
-                                               int rval, bool tok) {
-  switch (v) {
-#define SQ_CASE(V) \
-  case V: dense_op<Real, V>(re, im, c, rmask, rval, tok); break;
-    SQ_CASE(1) SQ_CASE(2) SQ_CASE(3) SQ_CASE(4) SQ_CASE(5) SQ_CASE(6) SQ_CASE(7)
-    SQ_CASE(8) SQ_CASE(9) SQ_CASE(10) SQ_CASE(11) SQ_CASE(12) SQ_CASE(13)
-    SQ_CASE(14) SQ_CASE(15)
-#undef SQ_CASE
-    default: break;
+// kSwXRot on register positions V with partner mask X (canonical local bits):
+// out_r = c_r a_r + f s_r a_(r^X).
+template <typename Real, int V, int X, bool IMAG>
+__device__ __forceinline__ void op_xrot(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+                                        int rmask, int rval) {
+  constexpr int D = 1 << ct_popc<V>();
+  Real cr[D], sr[D];
+#pragma unroll
+  for (int r = 0; r < D; ++r) {
+    const auto v = c[r];
+    cr[r] = v.x;
+    sr[r] = v.y;
+  }
+  for_groups<V>(rmask, rval, [&](int g) {
+    Real ar[D], ai[D];
+#pragma unroll
+    for (int x = 0; x < D; ++x) {
+      ar[x] = A.re[g | ct_dep<V>(x)];
+      ai[x] = A.im[g | ct_dep<V>(x)];
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+      const int q = r ^ X;
+      Real o_r, o_i;
+      if constexpr (IMAG) {  // f = i: s (i a_q) = s (-a_q.im, a_q.re)
+        o_r = fma(-sr[r], ai[q], cr[r] * ar[r]);
+        o_i = fma(sr[r], ar[q], cr[r] * ai[r]);
+      } else {
+        o_r = fma(sr[r], ar[q], cr[r] * ar[r]);
+        o_i = fma(sr[r], ai[q], cr[r] * ai[r]);
+      }
+      A.re[g | ct_dep<V>(r)] = o_r;
+      A.im[g | ct_dep<V>(r)] = o_i;
+    }
+  });
+}
+
+// kSwSwap2 on register positions V (two bits): out1 = p12 a2, out2 = p21 a1.
+template <typename Real, int V, bool PURE>
+__device__ __forceinline__ void op_swap2(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+                                         int rmask, int rval) {
+  constexpr int B1 = ct_dep<V>(1), B2 = ct_dep<V>(2);
+  if constexpr (PURE) {
+    for_groups<V>(rmask, rval, [&](int g) {
+      const Real tr = A.re[g | B1], ti = A.im[g | B1];
+      A.re[g | B1] = A.re[g | B2];
+      A.im[g | B1] = A.im[g | B2];
+      A.re[g | B2] = tr;
+      A.im[g | B2] = ti;
+    });
+  } else {
+    const auto p12 = c[0], p21 = c[1];
+    for_groups<V>(rmask, rval, [&](int g) {
+      const Real a1r = A.re[g | B1], a1i = A.im[g | B1], a2r = A.re[g | B2], a2i = A.im[g | B2];
+      cmul(p12.x, p12.y, a2r, a2i, A.re[g | B1], A.im[g | B1]);
+      cmul(p21.x, p21.y, a1r, a1i, A.re[g | B2], A.im[g | B2]);
+    });
   }
 }
 
-// Diagonal op: coefficient index = bits of the amplitude's global index at
-// the op's targets.  Global and tile-local sources are constant per thread
-// in a phase; register sources vary with the register slot.
-template <typename Real>
-__device__ __forceinline__ void diag_op(Real (&re)[kRegAmps], Real (&im)[kRegAmps],
-                                        const typename Vec2<Real>::T *__restrict__ c,
-                                        const SweepOp &op, uint64_t gbase, uint32_t jb) {
-  uint32_t base = 0, w0 = 0, w1 = 0, w2 = 0, w3 = 0;
-  const int k = op.k;
-  for (int t = 0; t < k; ++t) {
-    const uint32_t wt = 1u << (k - 1 - t);
-    const int src = op.dsrc[t], pos = op.dpos[t];
-    if (src == kSrcGlobal) {
-      if ((gbase >> pos) & 1) base |= wt;
-    } else if (src == kSrcLocal) {
-      if ((jb >> pos) & 1) base |= wt;
-    } else {
-      w0 |= pos == 0 ? wt : 0;
-      w1 |= pos == 1 ? wt : 0;
-      w2 |= pos == 2 ? wt : 0;
-      w3 |= pos == 3 ? wt : 0;
-    }
-  }
+// kSwDiag: coefficient index = thread part << popc(V) | register part.
+template <typename Real, int V>
+__device__ __forceinline__ void op_diag(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+                                        uint32_t base) {
+  const auto *cb = c + (base << ct_popc<V>());
 #pragma unroll
   for (int ri = 0; ri < kRegAmps; ++ri) {
-    const uint32_t idx = base | ((ri & 1) ? w0 : 0) | ((ri & 2) ? w1 : 0) |
-                         ((ri & 4) ? w2 : 0) | ((ri & 8) ? w3 : 0);
-    const auto d = c[idx];
-    const Real r = re[ri], i = im[ri];
-    re[ri] = d.x * r - d.y * i;
-    im[ri] = d.x * i + d.y * r;
+    const auto d = cb[ct_ext<V>(ri)];
+    const Real r = A.re[ri], i = A.im[ri];
+    cmul(d.x, d.y, r, i, A.re[ri], A.im[ri]);
   }
+}
+
+// kSwPhase: a *= p on the register slots whose bits match (rmask, rval).
+template <typename Real, bool NEG>
+__device__ __forceinline__ void op_phase(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+                                         int rmask, int rval) {
+  if constexpr (NEG) {
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri)
+      if ((ri & rmask) == rval) {
+        A.re[ri] = -A.re[ri];
+        A.im[ri] = -A.im[ri];
+      }
+  } else {
+    const auto p = c[0];
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri)
+      if ((ri & rmask) == rval) {
+        const Real r = A.re[ri], i = A.im[ri];
+        cmul(p.x, p.y, r, i, A.re[ri], A.im[ri]);
+      }
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ uint32_t diag_base(const SweepOp &op, uint64_t gbase, uint32_t jb) {
+  uint32_t base = 0;
+  for (int t = 0; t < op.ndt; ++t) {
+    const uint32_t bit = op.dsrc[t] == kSrcGlobal ? uint32_t(gbase >> op.dpos[t]) & 1u
+                                                  : (jb >> op.dpos[t]) & 1u;
+    base = (base << 1) | bit;
+  }
+  return base;
+}
+
+template <typename Real>
+__device__ __forceinline__ void apply_op(Amps<Real> &A, const typename Vec2<Real>::T *coef,
+                                         const SweepOp &op, uint64_t gbase, uint32_t jb) {
+  // Controls outside the registers are constant for this thread.
+  if ((gbase & op.gmask) != op.gval || (jb & op.lmask) != op.lval) return;
+  const auto *c = coef + op.coef;
+  const int rm = op.rmask, rv = op.rval;
+#define SQ_CODE(kind, v, aux) case sq_op_code(kind, v, aux):
+  switch (op.code) {
+    SQ_CODE(kSwPhase, 0, 0) op_phase<Real, false>(A, c, rm, rv); break;
+    SQ_CODE(kSwPhase, 0, kAuxPure) op_phase<Real, true>(A, c, rm, rv); break;
+#define SQ_DIAG(V) SQ_CODE(kSwDiag, V, 0) op_diag<Real, V>(A, c, diag_base<Real>(op, gbase, jb)); break;
+    SQ_DIAG(0) SQ_DIAG(1) SQ_DIAG(2) SQ_DIAG(3) SQ_DIAG(4) SQ_DIAG(5) SQ_DIAG(6) SQ_DIAG(7)
+    SQ_DIAG(8) SQ_DIAG(9) SQ_DIAG(10) SQ_DIAG(11) SQ_DIAG(12) SQ_DIAG(13) SQ_DIAG(14) SQ_DIAG(15)
+#undef SQ_DIAG
+#define SQ_ANTI(V)                                                               \
+  SQ_CODE(kSwAnti1, V, 0) op_anti1<Real, V, false>(A, c, rm, rv); break;         \
+  SQ_CODE(kSwAnti1, V, kAuxPure) op_anti1<Real, V, true>(A, c, rm, rv); break;
+    SQ_ANTI(1) SQ_ANTI(2) SQ_ANTI(4) SQ_ANTI(8)
+#undef SQ_ANTI
+#define SQ_SWAP(V)                                                               \
+  SQ_CODE(kSwSwap2, V, 0) op_swap2<Real, V, false>(A, c, rm, rv); break;         \
+  SQ_CODE(kSwSwap2, V, kAuxPure) op_swap2<Real, V, true>(A, c, rm, rv); break;
+    SQ_SWAP(3) SQ_SWAP(5) SQ_SWAP(6) SQ_SWAP(9) SQ_SWAP(10) SQ_SWAP(12)
+#undef SQ_SWAP
+#define SQ_XROT(V, X)                                                              \
+  SQ_CODE(kSwXRot, V, X) op_xrot<Real, V, X, false>(A, c, rm, rv); break;          \
+  SQ_CODE(kSwXRot, V, X | kAuxImag) op_xrot<Real, V, X, true>(A, c, rm, rv); break;
+    SQ_XROT(1, 1) SQ_XROT(2, 1) SQ_XROT(4, 1) SQ_XROT(8, 1)
+    SQ_XROT(3, 1) SQ_XROT(3, 2) SQ_XROT(3, 3) SQ_XROT(5, 1) SQ_XROT(5, 2) SQ_XROT(5, 3)
+    SQ_XROT(6, 1) SQ_XROT(6, 2) SQ_XROT(6, 3) SQ_XROT(9, 1) SQ_XROT(9, 2) SQ_XROT(9, 3)
+    SQ_XROT(10, 1) SQ_XROT(10, 2) SQ_XROT(10, 3) SQ_XROT(12, 1) SQ_XROT(12, 2) SQ_XROT(12, 3)
+#undef SQ_XROT
+#define SQ_DENSE(V) SQ_CODE(kSwDense, V, 0) op_dense<Real, V>(A, c, rm, rv); break;
+    SQ_DENSE(1) SQ_DENSE(2) SQ_DENSE(3) SQ_DENSE(4) SQ_DENSE(5) SQ_DENSE(6) SQ_DENSE(7)
+    SQ_DENSE(8) SQ_DENSE(9) SQ_DENSE(10) SQ_DENSE(11) SQ_DENSE(12) SQ_DENSE(13) SQ_DENSE(14)
+#undef SQ_DENSE
+    // A 4-qubit dense matrix needs a second copy of all 16 amplitudes; only
+    // the complex64 registers have room (the planner keeps complex128
+    // 4-qubit dense gates out of sweeps).
+    SQ_CODE(kSwDense, 15, 0)
+      if constexpr (sizeof(Real) == 4) op_dense<Real, 15>(A, c, rm, rv);
+      break;
+    default: break;
+  }
+#undef SQ_CODE
 }
 
 // Tile base: the tile index with zeros inserted at every tile bit position.
@@ -152,99 +312,149 @@ __device__ __forceinline__ uint64_t tile_base(uint64_t tile, const SweepHeader &
   return x;
 }
 
-// Fused sweep.  blockDim.x = 2^(m-4).  Dynamic shared memory: tile
-// (2^m amplitudes) | coefficients | high-bit address table (2^(m-l) u64).
-template <typename Real>
-__global__ void __launch_bounds__(256, 2)
+// Asynchronous global -> shared copy of one amplitude (Ampere-style
+// cp.async: no register staging, so a CTA can have its next tile in flight
+// while it computes on the current one).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
+// Fused sweep over 2^M-amplitude tiles; 2^(M-4) threads, 16 amplitudes each,
+// at least MINB CTAs per SM.
+// Persistent CTAs walk the tiles with a stride of gridDim.x and keep two tile
+// buffers: while the phases of tile t run on one buffer, tile t + gridDim.x
+// streams into the other.
+// Dynamic shared memory: 2 tiles (2 x 2^M amplitudes) | coefficients |
+// high-bit address table (2^(M-L) u64).  The swizzle is XOR-linear, so the
+// slot of (a ^ b) is slot(a) ^ slot(b): a thread derives all 16 slots of a
+// phase from five precomputed values.
+template <typename Real, int M, int MINB>
+__global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
     sweep_kernel(typename Vec2<Real>::T *__restrict__ psi,
                  const __grid_constant__ SweepParams<Real> P) {
   using C2 = typename Vec2<Real>::T;
+  constexpr int NT = 1 << (M - kRegBits);
+  constexpr int L = sweep_low_bits(M);
+  constexpr uint32_t TS = 1u << M;
+  constexpr uint32_t PER = TS / NT;  // amplitudes each thread copies per tile
+  constexpr uint32_t LOWMASK = (1u << L) - 1u;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SweepHeader &h = P.h;
-  const uint32_t m = h.m, l = h.l;
-  const uint32_t tsize = 1u << m;
-  C2 *tile = reinterpret_cast<C2 *>(smem_raw);
-  C2 *coef = tile + tsize;
+  C2 *bufs = reinterpret_cast<C2 *>(smem_raw);
+  C2 *coef = bufs + 2 * TS;
   uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + ((h.ncoef + 1) & ~1u));
-  const uint32_t tid = threadIdx.x, nthr = blockDim.x;
-  const uint32_t lowmask = (1u << l) - 1u;
+  const uint32_t tid = threadIdx.x;
 
-  for (uint32_t i = tid; i < h.ncoef; i += nthr) {
+  for (uint32_t i = tid; i < h.ncoef; i += NT) {
     C2 v;
     v.x = P.coef[2 * i];
     v.y = P.coef[2 * i + 1];
     coef[i] = v;
   }
-  for (uint32_t c = tid; c < (1u << (m - l)); c += nthr) {
+  for (uint32_t c = tid; c < (1u << (M - L)); c += NT) {
     uint64_t a = 0;
-    for (uint32_t i = 0; i < m - l; ++i)
+#pragma unroll
+    for (int i = 0; i < M - L; ++i)
       if ((c >> i) & 1) a |= uint64_t(1) << h.hi[i];
     hitab[c] = a;
   }
   __syncthreads();
 
-  const uint32_t last = h.nphases - 1;
-  for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
-    const uint64_t gbase = tile_base(t, h);
-    if (!(h.flags & kDirectLoad)) {
-#pragma unroll 4
-      for (uint32_t j = tid; j < tsize; j += nthr)
-        tile[swz<Real>(j)] = psi[gbase | hitab[j >> l] | (j & lowmask)];
-      __syncthreads();
+  // Element j = it * NT + tid of a tile; for M >= 9 the lanes of a warp cover
+  // 32 contiguous amplitudes of one chunk.
+  const uint32_t s_tid = swz<Real>(tid);
+  auto prefetch = [&](uint64_t t, C2 *dst) {
+    const uint64_t gb = tile_base(t, h);
+#pragma unroll
+    for (uint32_t it = 0; it < PER; ++it) {
+      const uint32_t j = it * NT + tid;
+      cp_async<sizeof(C2)>(dst + (s_tid ^ swz<Real>(it * NT)), psi + (gb | hitab[j >> L] | (j & LOWMASK)));
     }
+  };
+
+  const uint32_t last = h.nphases - 1;
+  uint32_t cur = 0;
+  if (blockIdx.x < h.num_tiles) prefetch(blockIdx.x, bufs);
+  cp_async_commit();
+  for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
+    C2 *tile = bufs + cur * TS;
+    const uint64_t tn = t + gridDim.x;
+    if (tn < h.num_tiles) prefetch(tn, bufs + (cur ^ 1) * TS);
+    cp_async_commit();
+    cp_async_wait_prev();  // this thread's copies of tile t have landed
+    __syncthreads();       // ... and everyone else's
+    const uint64_t gbase = tile_base(t, h);
     for (uint32_t p = 0; p <= last; ++p) {
       const SweepPhase &ph = P.ph[p];
       // Thread bits fill the non-register tile positions, ascending.
       uint32_t jb = tid;
 #pragma unroll
       for (int b = 0; b < kRegBits; ++b) jb = uint32_t(insert_zero(jb, ph.reg[b]));
-      const uint32_t r0 = 1u << ph.reg[0], r1 = 1u << ph.reg[1];
-      const uint32_t r2 = 1u << ph.reg[2], r3 = 1u << ph.reg[3];
-      Real re[kRegAmps], im[kRegAmps];
-      const bool gload = (p == 0) && (h.flags & kDirectLoad);
-#pragma unroll
-      for (int ri = 0; ri < kRegAmps; ++ri) {
-        const uint32_t j = jb | ((ri & 1) ? r0 : 0) | ((ri & 2) ? r1 : 0) |
-                           ((ri & 4) ? r2 : 0) | ((ri & 8) ? r3 : 0);
-        C2 v;
-        if (gload)
-          v = psi[gbase | hitab[j >> l] | (j & lowmask)];
-        else
-          v = tile[swz<Real>(j)];
-        re[ri] = v.x;
-        im[ri] = v.y;
-      }
-      for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
-        const SweepOp &op = P.op[o];
-        if (op.kind == kOpDiag) {
-          diag_op<Real>(re, im, coef + op.coef, op, gbase, jb);
-        } else {
-          const bool tok = ((gbase & op.gmask) == op.gval) && ((jb & op.lmask) == op.lval);
-          dense_dispatch<Real>(op.vmask, re, im, coef + op.coef, op.rmask, op.rval, tok);
-        }
-      }
       const bool gstore = (p == last) && (h.flags & kDirectStore);
+      // Shared-memory slots: sb ^ (selected w_b).  Register-bit values are
+      // disjoint bits.
+      const uint32_t sb = swz<Real>(jb);
+      const uint32_t w0 = swz<Real>(1u << ph.reg[0]), w1 = swz<Real>(1u << ph.reg[1]);
+      const uint32_t w2 = swz<Real>(1u << ph.reg[2]), w3 = swz<Real>(1u << ph.reg[3]);
+      Amps<Real> A;
 #pragma unroll
       for (int ri = 0; ri < kRegAmps; ++ri) {
-        const uint32_t j = jb | ((ri & 1) ? r0 : 0) | ((ri & 2) ? r1 : 0) |
-                           ((ri & 4) ? r2 : 0) | ((ri & 8) ? r3 : 0);
-        C2 v;
-        v.x = re[ri];
-        v.y = im[ri];
-        if (gstore)
-          psi[gbase | hitab[j >> l] | (j & lowmask)] = v;
-        else
-          tile[swz<Real>(j)] = v;
+        const C2 v = tile[sb ^ ((ri & 1) ? w0 : 0) ^ ((ri & 2) ? w1 : 0) ^ ((ri & 4) ? w2 : 0) ^
+                          ((ri & 8) ? w3 : 0)];
+        A.re[ri] = v.x;
+        A.im[ri] = v.y;
       }
-      __syncthreads();
+      for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) apply_op<Real>(A, coef, P.op[o], gbase, jb);
+      if (gstore) {
+        // Global index of register slot ri = tbase | selected register-bit
+        // weights (disjoint bits).
+        auto gw = [&](uint32_t pos) -> uint64_t {
+          return pos < uint32_t(L) ? (uint64_t(1) << pos) : (uint64_t(1) << h.hi[pos - L]);
+        };
+        const uint64_t tbase = gbase | hitab[jb >> L] | (jb & LOWMASK);
+        const uint64_t g0 = gw(ph.reg[0]), g1 = gw(ph.reg[1]), g2 = gw(ph.reg[2]), g3 = gw(ph.reg[3]);
+#pragma unroll
+        for (int ri = 0; ri < kRegAmps; ++ri) {
+          C2 v;
+          v.x = A.re[ri];
+          v.y = A.im[ri];
+          psi[tbase + ((ri & 1) ? g0 : 0) + ((ri & 2) ? g1 : 0) + ((ri & 4) ? g2 : 0) +
+              ((ri & 8) ? g3 : 0)] = v;
+        }
+      } else {
+#pragma unroll
+        for (int ri = 0; ri < kRegAmps; ++ri) {
+          C2 v;
+          v.x = A.re[ri];
+          v.y = A.im[ri];
+          tile[sb ^ ((ri & 1) ? w0 : 0) ^ ((ri & 2) ? w1 : 0) ^ ((ri & 4) ? w2 : 0) ^
+               ((ri & 8) ? w3 : 0)] = v;
+        }
+        __syncthreads();
+      }
     }
     if (!(h.flags & kDirectStore)) {
-#pragma unroll 4
-      for (uint32_t j = tid; j < tsize; j += nthr)
-        psi[gbase | hitab[j >> l] | (j & lowmask)] = tile[swz<Real>(j)];
-      __syncthreads();
+#pragma unroll
+      for (uint32_t it = 0; it < PER; ++it) {
+        const uint32_t j = it * NT + tid;
+        psi[gbase | hitab[j >> L] | (j & LOWMASK)] = tile[s_tid ^ swz<Real>(it * NT)];
+      }
     }
+    // Everyone is done with `tile` before the next iteration prefetches into it.
+    __syncthreads();
+    cur ^= 1;
   }
+  cp_async_wait_prev();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------

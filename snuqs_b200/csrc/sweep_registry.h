@@ -1,0 +1,18 @@
+// Host-side lookup of the compiled fused-sweep kernels (one object file per
+// instantiation, see sweep_inst.cu).
+#pragma once
+
+#define SQ_SWEEP_CAT(a, b, c) a##_##b##_##c
+#define SQ_SWEEP_PTR_NAME(real, m) SQ_SWEEP_CAT(sq_sweep_kernel_ptr, real, m)
+
+#define SQ_DECLARE_SWEEP(real, m) const void *SQ_SWEEP_PTR_NAME(real, m)();
+SQ_DECLARE_SWEEP(double, 4)
+SQ_DECLARE_SWEEP(double, 7)
+SQ_DECLARE_SWEEP(double, 10)
+SQ_DECLARE_SWEEP(double, 11)
+SQ_DECLARE_SWEEP(double, 12)
+SQ_DECLARE_SWEEP(float, 4)
+SQ_DECLARE_SWEEP(float, 7)
+SQ_DECLARE_SWEEP(float, 10)
+SQ_DECLARE_SWEEP(float, 12)
+#undef SQ_DECLARE_SWEEP

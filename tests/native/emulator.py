@@ -40,3 +40,25 @@ def run(state, n, gates, tile_bits=12, reorder=True):
     if r < 0:
         raise RuntimeError("emulator failed")
     return psi, r, unf.value
+
+
+def plan_stats(n, gates, tile_bits=12, reorder=True):
+    """{sweeps, phases, ops, kinds{...}, unfused} of the engine's plan."""
+    k, qoff, qs, nc, coff, cs, cv, moff, mats = [], [], [], [], [], [], [], [], []
+    mo = 0
+    for m, q, c, v in gates:
+        k.append(len(q)); qoff.append(len(qs)); qs.extend(q)
+        nc.append(len(c)); coff.append(len(cs)); cs.extend(c); cv.extend(v)
+        moff.append(mo); mats.append(np.asarray(m, dtype=np.complex128).ravel()); mo += mats[-1].size
+    arr = lambda x, t: np.ascontiguousarray(np.array(x if x else [0], dtype=t))
+    K, QO, QS, NC, CO, CS, CV = (arr(x, np.int32) for x in (k, qoff, qs, nc, coff, cs, cv))
+    MO = arr(moff, np.int64)
+    M = np.ascontiguousarray(np.concatenate(mats))
+    out = np.zeros(10, dtype=np.int64)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    if lib().emu_plan_stats(n, len(gates), P(K), P(QO), P(QS), P(NC), P(CO), P(CS), P(CV),
+                            P(MO), P(M), tile_bits, int(reorder), P(out)) != 0:
+        raise RuntimeError("planner failed")
+    names = ["dense", "diag", "anti1", "xrot", "swap2", "phase"]
+    return {"sweeps": int(out[0]), "phases": int(out[1]), "ops": int(out[2]),
+            "kinds": {names[i]: int(out[3 + i]) for i in range(6)}, "unfused": int(out[9])}

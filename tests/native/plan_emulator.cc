@@ -55,42 +55,84 @@ void emulate_sweep(cplx *psi, const PlannedSweep &ps) {
         for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
           const SweepOp &op = ps.op[o];
           const cplx *c = ps.coef.data() + op.coef;
-          if (op.kind == kOpDiag) {
-            for (int ri = 0; ri < kRegAmps; ++ri) {
-              uint32_t idx = 0;
-              for (int tt = 0; tt < op.k; ++tt) {
-                int bit;
-                if (op.dsrc[tt] == kSrcGlobal) bit = (gbase >> op.dpos[tt]) & 1;
-                else if (op.dsrc[tt] == kSrcLocal) bit = (jb >> op.dpos[tt]) & 1;
-                else bit = (ri >> op.dpos[tt]) & 1;
-                if (bit) idx |= 1u << (op.k - 1 - tt);
+          if ((gbase & op.gmask) != op.gval || (jb & op.lmask) != op.lval) continue;
+          const int V = op.vmask;
+          auto dep = [&](int x) {
+            int r = 0, b = 0;
+            for (int pp = 0; pp < 4; ++pp)
+              if (V & (1 << pp)) {
+                if (x & (1 << b)) r |= 1 << pp;
+                ++b;
               }
-              v[ri] *= c[idx];
-            }
-          } else {
-            const bool tok = ((gbase & op.gmask) == op.gval) && ((jb & op.lmask) == op.lval);
-            const int V = op.vmask, K = __builtin_popcount(V), D = 1 << K;
-            for (int g = 0; g < kRegAmps; ++g) {
-              if (g & V) continue;
-              if (!(tok && ((g & op.rmask) == op.rval))) continue;
-              auto dep = [&](int x) {
-                int r = 0, b = 0;
-                for (int pp = 0; pp < 4; ++pp)
-                  if (V & (1 << pp)) {
-                    if (x & (1 << b)) r |= 1 << pp;
-                    ++b;
-                  }
-                return r;
-              };
-              cplx a[16], out[16];
-              for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
-              for (int r = 0; r < D; ++r) {
-                cplx s = c[r * D] * a[0];
-                for (int x = 1; x < D; ++x) s += c[r * D + x] * a[x];
-                out[r] = s;
+            return r;
+          };
+          auto ext = [&](int x) {
+            int r = 0, b = 0;
+            for (int pp = 0; pp < 4; ++pp)
+              if (V & (1 << pp)) {
+                if (x & (1 << pp)) r |= 1 << b;
+                ++b;
               }
-              for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
-            }
+            return r;
+          };
+          auto groups = [&](auto f) {
+            for (int g = 0; g < kRegAmps; ++g)
+              if (!(g & V) && ((g & op.rmask) == op.rval)) f(g);
+          };
+          const bool pure = op.aux & kAuxPure;
+          switch (op.kind) {
+            case kSwPhase:
+              for (int ri = 0; ri < kRegAmps; ++ri)
+                if ((ri & op.rmask) == op.rval) v[ri] = pure ? -v[ri] : c[0] * v[ri];
+              break;
+            case kSwDiag: {
+              uint32_t base = 0;
+              for (int t = 0; t < op.ndt; ++t) {
+                const uint32_t bit = op.dsrc[t] == kSrcGlobal ? uint32_t(gbase >> op.dpos[t]) & 1u
+                                                              : (jb >> op.dpos[t]) & 1u;
+                base = (base << 1) | bit;
+              }
+              const int nreg = __builtin_popcount(V);
+              for (int ri = 0; ri < kRegAmps; ++ri) v[ri] = c[(base << nreg) | ext(ri)] * v[ri];
+            } break;
+            case kSwAnti1:
+              groups([&](int g) {
+                const cplx a0 = v[g], a1 = v[g | V];
+                v[g] = pure ? a1 : c[0] * a1;
+                v[g | V] = pure ? a0 : c[1] * a0;
+              });
+              break;
+            case kSwSwap2: {
+              const int B1 = dep(1), B2 = dep(2);
+              groups([&](int g) {
+                const cplx a1 = v[g | B1], a2 = v[g | B2];
+                v[g | B1] = pure ? a2 : c[0] * a2;
+                v[g | B2] = pure ? a1 : c[1] * a1;
+              });
+            } break;
+            case kSwXRot: {
+              const int X = op.aux & kAuxXMask, D = 1 << __builtin_popcount(V);
+              const cplx f = (op.aux & kAuxImag) ? cplx(0, 1) : cplx(1, 0);
+              groups([&](int g) {
+                cplx a[16], out[16];
+                for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
+                for (int r = 0; r < D; ++r) out[r] = c[r].real() * a[r] + f * c[r].imag() * a[r ^ X];
+                for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
+              });
+            } break;
+            default: {
+              const int K = __builtin_popcount(V), D = 1 << K;
+              groups([&](int g) {
+                cplx a[16], out[16];
+                for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
+                for (int r = 0; r < D; ++r) {
+                  cplx s = c[r * D] * a[0];
+                  for (int x = 1; x < D; ++x) s += c[r * D + x] * a[x];
+                  out[r] = s;
+                }
+                for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
+              });
+            } break;
           }
         }
         for (int ri = 0; ri < kRegAmps; ++ri) tile[jj[ri]] = v[ri];
@@ -184,3 +226,49 @@ int emu_run(double *state, int n, int nops, const int *k, const int *qoff, const
 }
 
 }  // extern "C"
+
+extern "C" {
+// Plan statistics for a gate list (same arguments as emu_run): writes
+// [sweeps, phases, ops, ops by kind 1..6, unfused] into out[0..9].
+int emu_plan_stats(int n, int nops, const int *k, const int *qoff, const int *qubits,
+                   const int *nc, const int *coff, const int *controls, const int *cvals,
+                   const long *moff, const double *mats, int tile_bits, int reorder,
+                   long *out) {
+  try {
+    std::vector<HostOp> ops;
+    for (int i = 0; i < nops; ++i) {
+      std::vector<int> tb;
+      for (int j = 0; j < k[i]; ++j) tb.push_back(n - 1 - qubits[qoff[i] + j]);
+      uint64_t cm = 0, cv = 0;
+      for (int j = 0; j < nc[i]; ++j) {
+        const uint64_t bit = uint64_t(1) << (n - 1 - controls[coff[i] + j]);
+        cm |= bit;
+        if (cvals[coff[i] + j]) cv |= bit;
+      }
+      const size_t d = size_t(1) << k[i];
+      std::vector<cplx> mm(d * d);
+      std::memcpy(mm.data(), mats + 2 * moff[i], d * d * sizeof(cplx));
+      HostOp h;
+      if (analyse_op(mm, tb, cm, cv, h)) ops.push_back(h);
+    }
+    PlanOptions opt;
+    opt.tile_bits = uint32_t(tile_bits);
+    opt.reorder = reorder != 0;
+    auto plan = plan_sweeps(ops, uint32_t(n), opt);
+    for (int i = 0; i < 10; ++i) out[i] = 0;
+    for (const auto &pl : plan) {
+      if (!pl.is_sweep) {
+        out[9]++;
+        continue;
+      }
+      out[0]++;
+      out[1] += pl.sweep.h.nphases;
+      out[2] += long(pl.sweep.op.size());
+      for (const auto &o : pl.sweep.op) out[2 + o.kind]++;
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return -1;
+  }
+}
+}
