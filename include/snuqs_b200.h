@@ -174,6 +174,24 @@ int sq_expect_pauli(sq_state *s, const char *paulis, const double *weights,
 /* Squared norm in FP64 (synchronous). */
 int sq_norm2(sq_state *s, double *out, void *stream);
 
+/* No counterpart in the reference.  sq_expect_pauli for callers that cannot
+ * allocate device memory: code recording a CUDA graph (a cudaMalloc would
+ * break the capture), applications whose memory pool owns the whole device,
+ * callers holding only a raw device pointer to a state.  `state` is a device
+ * array of 2^num_qubits amplitudes of `dtype`; the FP64 result is written
+ * to out_device (one double in device memory), asynchronously on `stream`.
+ * Nothing is allocated: the reduction's partial sums live in one fixed
+ * 16 KiB device array (2048 doubles) inside the library, which each device
+ * holds from the moment the library's device code is loaded on it until the
+ * process exits.  The first call on each device looks that array up (make
+ * it once, before any stream capture).  Every call on a device shares the
+ * array, so calls that overlap on the GPU (different streams, no ordering)
+ * race; order them.  Limits: n_terms <= 1024 and at most 256 distinct
+ * (X/Y mask, Y parity) groups; larger requests return SQ_ERR_UNSUPPORTED. */
+int sq_expect_pauli_noalloc(const void *state, uint32_t num_qubits, int dtype,
+                            const char *paulis, const double *weights,
+                            uint32_t n_terms, double *out_device, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,7 +24,7 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-ENGINE_CU = ["engine.cu"]
+ENGINE_CU = ["engine.cu", "noalloc.cu"]
 ENGINE_CC = ["gates.cc", "planner.cc"]
 # Fused-sweep kernel instantiations: (precision, tile bits, CTAs per SM).
 # Tile sizes must match kTileBitsC128 / kTileBitsC64 in csrc/sq_plan.h; the
@@ -76,9 +76,11 @@ def build(force: bool = False, verbose: bool = False) -> None:
         objs.append(obj)
     jobs = []
     inst_src = os.path.join(CSRC, "sweep_inst.cu")
+    inst_deps = [inst_src] + [os.path.join(CSRC, f) for f in
+                              ("sweep_kernels.cuh", "sq_plan.h", "sweep_registry.h")]
     for real, m, minb in SWEEP_INSTANCES:
         obj = os.path.join(BUILD, f"sweep_{real}_{m}.o")
-        if force or _stale(obj, [inst_src] + hdrs):
+        if force or _stale(obj, inst_deps):
             cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
                    f"-DSQ_REAL={real}", f"-DSQ_M={m}", f"-DSQ_MINB={minb}",
                    "-Xptxas", "-warn-spills", "-c", inst_src, "-o", obj]

@@ -77,6 +77,7 @@ SIGNATURES = {
     "sq_probabilities": (_I, [_P, _P, _P]),
     "sq_expect_pauli": (_I, [_P, ctypes.c_char_p, _PD, _U32, _PD, _P]),
     "sq_norm2": (_I, [_P, _PD, _P]),
+    "sq_expect_pauli_noalloc": (_I, [_P, _U32, _I, ctypes.c_char_p, _PD, _U32, _P, _P]),
 }
 
 

@@ -36,6 +36,9 @@ static int fail(int code, const char *fmt, ...) {
   return code;
 }
 
+// For the library's other translation units: record an error, return `code`.
+int sq_detail_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+
 #define SQ_CUDA(call)                                                                  \
   do {                                                                                 \
     cudaError_t e_ = (call);                                                           \

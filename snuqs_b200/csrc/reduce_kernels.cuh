@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kReduceThreads)
 }
 
 // out[0] = sum of partial[0..n) in a fixed order (deterministic).
-__global__ void __launch_bounds__(kReduceThreads)
+static __global__ void __launch_bounds__(kReduceThreads)
     finalize_sum_kernel(const double *__restrict__ partial, uint32_t n, double *__restrict__ out) {
   double v = 0.0;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
