@@ -111,6 +111,12 @@ def ref_gate_matrix(name: str, angles: Sequence[float] = ()) -> np.ndarray:
     return out
 
 
+def ref_initialize_basis_z(state: np.ndarray, nq: int) -> None:
+    """In place: the reference cpu::initializeBasis_Z on a host state."""
+    assert state.dtype == np.complex128 and state.size == (1 << nq)
+    ref().ref_initialize_basis_z(_dptr(state), nq)
+
+
 def basis_state(nq: int, index: int = 0) -> np.ndarray:
     s = np.zeros(1 << nq, dtype=np.complex128)
     s[index] = 1.0
