@@ -308,6 +308,11 @@ def _run_ours(args, rank, world, local):
             out["e2e"] = e2e(n, ops, args, amp)
         except Exception as e:  # report, do not lose the device-timed line
             out["e2e"] = {"value": None, "unit": "GB/s", "note": f"e2e failed: {e}"}
+    if world == 1 and rank == 0 and not args.no_adjoint:
+        try:
+            out["adjoint"] = adjoint_metric(args.precision)
+        except Exception as e:
+            out["adjoint"] = {"note": f"adjoint failed: {e}"}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(n, ops)
@@ -320,6 +325,61 @@ def _run_ours(args, rank, world, local):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def qaoa_workload(n=26, p=8, seed=SEED):
+    """QAOA MaxCut: seeded random 3-regular graph on n vertices, p layers of
+    ZZ(gamma_l) on every edge and RotX(beta_l) on every qubit (2p parameters)."""
+    from snuqs_b200 import circuits
+
+    edges = circuits.random_regular_graph(n, 3, seed=seed)
+    ops = [("Hadamard", (q,), ()) for q in range(n)]
+    for l in range(p):
+        ops += [("ZZ", (i, j), (0.0,), (l,)) for i, j in edges]
+        ops += [("RotX", (q,), (0.0,), (p + l,)) for q in range(n)]
+    theta = np.random.default_rng(seed).uniform(0, np.pi, 2 * p)
+    return ops, circuits.maxcut_hamiltonian(n, edges), theta
+
+
+def adjoint_metric(precision: str):
+    """Adjoint gradient (one forward + one fused reverse pass) against the
+    parameter-shift rule on the same engine, QAOA MaxCut 26 qubits p = 8."""
+    import torch
+
+    from snuqs_b200 import adjoint, capi
+
+    n, p = 26, 8
+    dtype = capi.SQ_C128 if precision == "complex128" else capi.SQ_C64
+    ops, terms, theta = qaoa_workload(n, p)
+    ws = adjoint.Workspace(n, dtype)
+    for _ in range(2):
+        adjoint.adjoint_gradient(ws, ops, theta, terms, 2 * p)
+    reps = 5
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        e, g = adjoint.adjoint_gradient(ws, ops, theta, terms, 2 * p)
+    t_adj = (time.perf_counter() - t0) / reps
+    # Parameter shift: time a sample of shifted evaluations, extrapolate to
+    # the 2 x 520 evaluations one gradient needs.
+    st = ws.psi
+    adjoint.parameter_shift_gradient(st, ops, theta, terms, 2 * p, max_evals=4)
+    torch.cuda.synchronize()
+    sample = 40
+    t0 = time.perf_counter()
+    _, done = adjoint.parameter_shift_gradient(st, ops, theta, terms, 2 * p, max_evals=sample)
+    t_eval = (time.perf_counter() - t0) / done
+    evals = adjoint.count_shift_evaluations(ops)
+    ws.close()
+    return {"workload": f"qaoa_maxcut_{n}q_p{p}_{precision}", "params": 2 * p,
+            "gate_occurrences": evals // 2, "energy": e,
+            "adjoint_ms": round(t_adj * 1e3, 3), "adjoint_grads_per_s": round(1.0 / t_adj, 3),
+            "param_shift_evals_per_grad": evals,
+            "param_shift_ms_per_eval": round(t_eval * 1e3, 3),
+            "param_shift_grads_per_s": round(1.0 / (t_eval * evals), 4),
+            "speedup_vs_param_shift": round(t_eval * evals / t_adj, 1),
+            "timing": "host wall clock around synchronous calls; parameter shift extrapolated "
+                      f"from {done} evaluations"}
 
 
 def e2e(n, ops, args, amp):

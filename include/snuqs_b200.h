@@ -103,6 +103,11 @@ int sq_host_free(void *ptr);
 int sq_gate_matrix(int gate, const double *angles, uint32_t nangles,
                    double *out, uint32_t *k);
 int sq_gate_qubits(int gate);
+/* Analytic derivative d/d angles[param] of the named gate's matrix (same
+ * layout as sq_gate_matrix).  No counterpart in the reference (it has no
+ * gradients); used by the adjoint gradient. */
+int sq_gate_matrix_derivative(int gate, const double *angles, uint32_t nangles,
+                              uint32_t param, double *out, uint32_t *k);
 
 /* ---- state handle -------------------------------------------------------
  * StateVector(DeviceType::CUDA, n): state_vector.cc:21-25 + buffer_cuda.cc:13-17. */
@@ -173,6 +178,38 @@ int sq_expect_pauli(sq_state *s, const char *paulis, const double *weights,
                     uint32_t n_terms, double *out, void *stream);
 /* Squared norm in FP64 (synchronous). */
 int sq_norm2(sq_state *s, double *out, void *stream);
+
+/* ---- adjoint gradient ---------------------------------------------------
+ * No counterpart in the reference (its plugin forbids the adjoint-gradient
+ * result type: src/braket/snuqs/simulator.py:649).
+ *
+ * One gate of a parametrised circuit.  gate is an sq_gate id, or -1 for a
+ * fixed matrix (`matrix`, 4^k complex128).  Angle j of the gate takes the
+ * value angles[j]; when param[j] >= 0 it depends on parameter param[j] with
+ * d angles[j] / d theta[param[j]] = scale[j] (1 for the angle itself). */
+typedef struct {
+  int32_t gate;
+  uint32_t k;
+  uint32_t qubits[3];
+  uint32_t nangles;
+  double angles[3];
+  int32_t param[3];
+  double scale[3];
+  const double *matrix;
+} sq_circuit_op;
+
+/* Energy E = <psi|H|psi> of psi = U(theta)|0...0> for H = sum_t w_t P_t, and
+ * dE/dtheta for n_params parameters, by one forward pass and one reverse
+ * (adjoint) pass: the reverse pass un-computes the gates on psi and on
+ * lambda = H psi together in fused two-state sweeps and accumulates
+ * 2 Re <lambda| dU U^dagger |psi> per parametrised angle; no intermediate
+ * state is stored.  `psi` and `lam` are two caller-owned work states of the
+ * same size and precision (their contents are overwritten).  energy and grad
+ * (n_params doubles) are host pointers; the call is synchronous. */
+int sq_adjoint_gradient(sq_state *psi, sq_state *lam, const sq_circuit_op *ops,
+                        uint32_t nops, const char *paulis, const double *weights,
+                        uint32_t n_terms, uint32_t n_params, double *energy,
+                        double *grad, void *stream);
 
 /* No counterpart in the reference.  sq_expect_pauli for callers that cannot
  * allocate device memory: code recording a CUDA graph (a cudaMalloc would

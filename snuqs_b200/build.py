@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ENGINE_CU = ["engine.cu", "noalloc.cu"]
-ENGINE_CC = ["gates.cc", "planner.cc"]
+ENGINE_CC = ["gates.cc", "planner.cc", "adjoint_plan.cc"]
 # Fused-sweep kernel instantiations: (precision, tile bits, CTAs per SM).
 # Tile sizes must match kTileBitsC128 / kTileBitsC64 in csrc/sq_plan.h; the
 # CTA counts keep registers <= 65536 / (CTAs x threads).
@@ -33,6 +33,9 @@ SWEEP_INSTANCES = [
     ("double", 4, 1), ("double", 7, 1), ("double", 10, 6), ("double", 11, 3), ("double", 12, 1),
     ("float", 4, 1), ("float", 7, 1), ("float", 10, 8), ("float", 12, 2),
 ]
+# Two-state adjoint kernels: (precision, tile bits); must match kAdjTileBits*.
+ADJOINT_INSTANCES = [("double", 4), ("double", 7), ("double", 10),
+                     ("float", 4), ("float", 7), ("float", 11)]
 LIB = os.path.join(HERE, "libsnuqs_b200.so")
 
 
@@ -84,6 +87,18 @@ def build(force: bool = False, verbose: bool = False) -> None:
             cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
                    f"-DSQ_REAL={real}", f"-DSQ_M={m}", f"-DSQ_MINB={minb}",
                    "-Xptxas", "-warn-spills", "-c", inst_src, "-o", obj]
+            jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                               stderr=subprocess.STDOUT, text=True)))
+        objs.append(obj)
+    adj_src = os.path.join(CSRC, "adjoint_inst.cu")
+    adj_deps = inst_deps + [adj_src, os.path.join(CSRC, "adjoint_kernels.cuh"),
+                            os.path.join(CSRC, "reduce_kernels.cuh")]
+    for real, m in ADJOINT_INSTANCES:
+        obj = os.path.join(BUILD, f"adjoint_{real}_{m}.o")
+        if force or _stale(obj, adj_deps):
+            cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
+                   f"-DSQ_REAL={real}", f"-DSQ_M={m}",
+                   "-Xptxas", "-warn-spills", "-c", adj_src, "-o", obj]
             jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
                                                stderr=subprocess.STDOUT, text=True)))
         objs.append(obj)

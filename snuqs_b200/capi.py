@@ -53,6 +53,7 @@ SIGNATURES = {
     "sq_host_free": (_I, [_P]),
     "sq_gate_matrix": (_I, [_I, _PD, _U32, _PD, _PU32]),
     "sq_gate_qubits": (_I, [_I]),
+    "sq_gate_matrix_derivative": (_I, [_I, _PD, _U32, _U32, _PD, _PU32]),
     "sq_state_create": (_I, [_U32, _I, ctypes.POINTER(_P)]),
     "sq_state_wrap": (_I, [_P, _U32, _I, ctypes.POINTER(_P)]),
     "sq_state_destroy": (_I, [_P]),
@@ -78,7 +79,49 @@ SIGNATURES = {
     "sq_expect_pauli": (_I, [_P, ctypes.c_char_p, _PD, _U32, _PD, _P]),
     "sq_norm2": (_I, [_P, _PD, _P]),
     "sq_expect_pauli_noalloc": (_I, [_P, _U32, _I, ctypes.c_char_p, _PD, _U32, _P, _P]),
+    "sq_adjoint_gradient": (_I, [_P, _P, _P, _U32, ctypes.c_char_p, _PD, _U32, _U32, _PD, _PD, _P]),
 }
+
+
+class SqCircuitOp(ctypes.Structure):
+    """sq_circuit_op (include/snuqs_b200.h)."""
+    _fields_ = [("gate", ctypes.c_int32), ("k", ctypes.c_uint32), ("qubits", ctypes.c_uint32 * 3),
+                ("nangles", ctypes.c_uint32), ("angles", ctypes.c_double * 3),
+                ("param", ctypes.c_int32 * 3), ("scale", ctypes.c_double * 3),
+                ("matrix", ctypes.POINTER(ctypes.c_double))]
+
+
+def circuit_ops(ops):
+    """Array of SqCircuitOp from ops (name, qubits, angles[, params[, scales]]) or
+    ("Unitary", qubits, (), matrix).  params[j] is the parameter index fed by
+    angle j (-1 = constant).  Returns (array, keepalive)."""
+    arr = (SqCircuitOp * max(1, len(ops)))()
+    keep = []
+    for i, op in enumerate(ops):
+        o = arr[i]
+        o.k = len(op[1])
+        for j, q in enumerate(op[1]):
+            o.qubits[j] = q
+        for j in range(3):
+            o.param[j] = -1
+            o.scale[j] = 1.0
+        if op[0] == "Unitary":
+            m = np.ascontiguousarray(op[3], dtype=np.complex128)
+            keep.append(m)
+            o.gate = -1
+            o.matrix = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            continue
+        o.gate = GATE_ID[op[0]]
+        o.nangles = len(op[2])
+        for j, a in enumerate(op[2]):
+            o.angles[j] = a
+        if len(op) > 3:
+            for j, p in enumerate(op[3]):
+                o.param[j] = p
+        if len(op) > 4:
+            for j, sc in enumerate(op[4]):
+                o.scale[j] = sc
+    return arr, keep
 
 
 class SqError(RuntimeError):
@@ -125,6 +168,17 @@ def gate_matrix(name: str, angles: Sequence[float] = ()) -> np.ndarray:
     out = np.zeros(64, dtype=np.complex128)
     k = _U32(0)
     check(lib().sq_gate_matrix(GATE_ID[name], _dp(a), len(angles), _dp(out), ctypes.byref(k)))
+    d = 1 << k.value
+    return out[: d * d].reshape(d, d).copy()
+
+
+def gate_matrix_derivative(name: str, angles: Sequence[float], param: int) -> np.ndarray:
+    a = np.zeros(3, dtype=np.float64)
+    a[: len(angles)] = angles
+    out = np.zeros(64, dtype=np.complex128)
+    k = _U32(0)
+    check(lib().sq_gate_matrix_derivative(GATE_ID[name], _dp(a), len(angles), param, _dp(out),
+                                          ctypes.byref(k)))
     d = 1 << k.value
     return out[: d * d].reshape(d, d).copy()
 

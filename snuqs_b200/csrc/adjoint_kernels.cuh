@@ -1,0 +1,307 @@
+// Adjoint-gradient kernels (sm_100a).
+//
+// adjoint_sweep_kernel: the two-state analogue of sweep_kernel.  Each thread
+//   holds 8 amplitudes of phi and the same 8 amplitudes of lambda (3 register
+//   bits per phase); every un-compute gate U^dagger is applied to both, and
+//   every inner-product op accumulates <lambda| K |phi> over the tile into a
+//   per-warp slot in shared memory.  phi and lambda are each read and written
+//   once per sweep, however many gates and parameters the sweep carries.
+// pauli_apply_kernel: lambda = H psi for a Pauli-string sum, with
+//   E = Re <psi|lambda> accumulated in FP64 in the same pass.
+// inner_reduce_kernel: fixed-order sum of the per-warp partials of each slot.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "reduce_kernels.cuh"
+#include "sweep_kernels.cuh"
+
+namespace sq {
+
+constexpr int kAdjRegBits = 3;
+constexpr int kAdjAmps = 1 << kAdjRegBits;
+
+struct PauliApplyGroup {
+  uint64_t x;        // flip mask
+  uint32_t t0, t1;   // term range
+};
+
+struct PauliApplyParams {
+  uint32_t n, ngroups;
+  PauliApplyGroup g[kMaxGroups];
+  uint64_t zy[kMaxTerms];
+  double wr[kMaxTerms], wi[kMaxTerms];  // w_t * (-i)^ny_t
+};
+
+// out[i] = sum_t w_t (-i)^ny_t (-1)^popc(i & zy_t) psi[i ^ x_t];
+// partial[block] = this block's share of Re <psi|out> (FP64).
+template <typename Real>
+__global__ void __launch_bounds__(kReduceThreads)
+    pauli_apply_kernel(const typename Vec2<Real>::T *__restrict__ psi,
+                       typename Vec2<Real>::T *__restrict__ out,
+                       const __grid_constant__ PauliApplyParams P, double *__restrict__ partial) {
+  using C2 = typename Vec2<Real>::T;
+  const uint64_t N = uint64_t(1) << P.n;
+  double e = 0.0;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    double ar = 0.0, ai = 0.0;
+    for (uint32_t gi = 0; gi < P.ngroups; ++gi) {
+      const PauliApplyGroup &G = P.g[gi];
+      double cr = 0.0, ci = 0.0;
+      for (uint32_t t = G.t0; t < G.t1; ++t) {
+        const double s = (__popcll(i & P.zy[t]) & 1) ? -1.0 : 1.0;
+        cr = fma(s, P.wr[t], cr);
+        ci = fma(s, P.wi[t], ci);
+      }
+      const C2 b = psi[i ^ G.x];
+      ar += cr * double(b.x) - ci * double(b.y);
+      ai += cr * double(b.y) + ci * double(b.x);
+    }
+    C2 o;
+    o.x = Real(ar);
+    o.y = Real(ai);
+    out[i] = o;
+    const C2 a = psi[i];
+    e += double(a.x) * ar + double(a.y) * ai;  // Re(conj(a) * acc)
+  }
+  const double s = block_sum(e);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// Inner-product contribution of one thread for a kSwInnerDiag op.
+template <typename Real, int V>
+__device__ __forceinline__ void inner_diag(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                           const typename Vec2<Real>::T *__restrict__ c,
+                                           uint32_t base, double &sr, double &si) {
+  const auto *cb = c + (base << ct_popc<V>());
+#pragma unroll
+  for (int ri = 0; ri < kAdjAmps; ++ri) {
+    const auto d = cb[ct_ext<V>(ri)];
+    // K phi
+    const double kr = double(d.x) * double(F.re[ri]) - double(d.y) * double(F.im[ri]);
+    const double ki = double(d.x) * double(F.im[ri]) + double(d.y) * double(F.re[ri]);
+    // conj(lambda) * (K phi)
+    sr += double(G.re[ri]) * kr + double(G.im[ri]) * ki;
+    si += double(G.re[ri]) * ki - double(G.im[ri]) * kr;
+  }
+}
+
+// Inner-product contribution of one thread for a kSwInnerDense op on
+// register positions V (canonical coefficient order).
+template <typename Real, int V>
+__device__ __forceinline__ void inner_dense(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                            const typename Vec2<Real>::T *__restrict__ c, double &sr,
+                                            double &si) {
+  constexpr int D = 1 << ct_popc<V>();
+#pragma unroll
+  for (int g = 0; g < kAdjAmps; ++g) {
+    if (g & V) continue;
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+      double kr = 0.0, ki = 0.0;
+#pragma unroll
+      for (int x = 0; x < D; ++x) {
+        const auto m = c[r * D + x];
+        const int ix = g | ct_dep<V>(x);
+        kr += double(m.x) * double(F.re[ix]) - double(m.y) * double(F.im[ix]);
+        ki += double(m.x) * double(F.im[ix]) + double(m.y) * double(F.re[ix]);
+      }
+      const int ir = g | ct_dep<V>(r);
+      sr += double(G.re[ir]) * kr + double(G.im[ir]) * ki;
+      si += double(G.re[ir]) * ki - double(G.im[ir]) * kr;
+    }
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ void inner_op(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                         const typename Vec2<Real>::T *coef, const SweepOp &op,
+                                         uint64_t gbase, uint32_t jb, double &sr, double &si) {
+  const auto *c = coef + op.coef;
+  if (op.kind == kSwInnerDiag) {
+    const uint32_t base = diag_base<Real>(op, gbase, jb);
+    switch (op.vmask) {
+#define SQ_CASE(V) \
+  case V: inner_diag<Real, V>(F, G, c, base, sr, si); break;
+      SQ_CASE(0) SQ_CASE(1) SQ_CASE(2) SQ_CASE(3) SQ_CASE(4) SQ_CASE(5) SQ_CASE(6) SQ_CASE(7)
+#undef SQ_CASE
+    }
+  } else {
+    switch (op.vmask) {
+#define SQ_CASE(V) \
+  case V: inner_dense<Real, V>(F, G, c, sr, si); break;
+      SQ_CASE(1) SQ_CASE(2) SQ_CASE(3) SQ_CASE(4) SQ_CASE(5) SQ_CASE(6) SQ_CASE(7)
+#undef SQ_CASE
+    }
+  }
+}
+
+// Two-state fused sweep over 2^M-amplitude tiles; 2^(M-3) threads.
+// Dynamic shared memory: phi tiles (2 buffers) | lambda tiles (2 buffers) |
+// coefficients | high-bit table | per-warp inner-product slots.
+// partials[(block * warps + warp) * kMaxInner + slot] receives each warp's
+// sums (complex, FP64) at the end.
+template <typename Real, int M>
+__global__ void __launch_bounds__(1 << (M - kAdjRegBits), 1)
+    adjoint_sweep_kernel(typename Vec2<Real>::T *__restrict__ psi,
+                         typename Vec2<Real>::T *__restrict__ lam,
+                         const __grid_constant__ SweepParams<Real> P,
+                         double2 *__restrict__ partials) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int NT = 1 << (M - kAdjRegBits);
+  constexpr int NW = (NT + 31) / 32;
+  constexpr int L = sweep_low_bits(M);
+  constexpr uint32_t TS = 1u << M;
+  constexpr uint32_t PER = TS / NT;
+  constexpr uint32_t LOWMASK = (1u << L) - 1u;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SweepHeader &h = P.h;
+  C2 *fbufs = reinterpret_cast<C2 *>(smem_raw);
+  C2 *lbufs = fbufs + 2 * TS;
+  C2 *coef = lbufs + 2 * TS;
+  uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + ((h.ncoef + 1) & ~1u));
+  double2 *acc = reinterpret_cast<double2 *>(hitab + (1u << (M - L)));
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  for (uint32_t i = tid; i < h.ncoef; i += NT) {
+    C2 v;
+    v.x = P.coef[2 * i];
+    v.y = P.coef[2 * i + 1];
+    coef[i] = v;
+  }
+  for (uint32_t c = tid; c < (1u << (M - L)); c += NT) {
+    uint64_t a = 0;
+#pragma unroll
+    for (int i = 0; i < M - L; ++i)
+      if ((c >> i) & 1) a |= uint64_t(1) << h.hi[i];
+    hitab[c] = a;
+  }
+  for (uint32_t i = tid; i < NW * kMaxInner; i += NT) acc[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+
+  const uint32_t s_tid = swz<Real>(tid);
+  auto prefetch = [&](uint64_t t, C2 *fdst, C2 *ldst) {
+    const uint64_t gb = tile_base(t, h);
+#pragma unroll
+    for (uint32_t it = 0; it < PER; ++it) {
+      const uint32_t j = it * NT + tid;
+      const uint64_t g = gb | hitab[j >> L] | (j & LOWMASK);
+      const uint32_t slot = s_tid ^ swz<Real>(it * NT);
+      cp_async<sizeof(C2)>(fdst + slot, psi + g);
+      cp_async<sizeof(C2)>(ldst + slot, lam + g);
+    }
+  };
+
+  const uint32_t last = h.nphases - 1;
+  uint32_t cur = 0;
+  if (blockIdx.x < h.num_tiles) prefetch(blockIdx.x, fbufs, lbufs);
+  cp_async_commit();
+  for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
+    C2 *ftile = fbufs + cur * TS;
+    C2 *ltile = lbufs + cur * TS;
+    const uint64_t tn = t + gridDim.x;
+    if (tn < h.num_tiles) prefetch(tn, fbufs + (cur ^ 1) * TS, lbufs + (cur ^ 1) * TS);
+    cp_async_commit();
+    cp_async_wait_prev();
+    __syncthreads();
+    const uint64_t gbase = tile_base(t, h);
+    for (uint32_t p = 0; p <= last; ++p) {
+      const SweepPhase &ph = P.ph[p];
+      uint32_t jb = tid;
+#pragma unroll
+      for (int b = 0; b < kAdjRegBits; ++b) jb = uint32_t(insert_zero(jb, ph.reg[b]));
+      const uint32_t sb = swz<Real>(jb);
+      const uint32_t w0 = swz<Real>(1u << ph.reg[0]), w1 = swz<Real>(1u << ph.reg[1]);
+      const uint32_t w2 = swz<Real>(1u << ph.reg[2]);
+      Amps<Real, kAdjAmps> F, G;
+#pragma unroll
+      for (int ri = 0; ri < kAdjAmps; ++ri) {
+        const uint32_t s = sb ^ ((ri & 1) ? w0 : 0) ^ ((ri & 2) ? w1 : 0) ^ ((ri & 4) ? w2 : 0);
+        const C2 a = ftile[s], b = ltile[s];
+        F.re[ri] = a.x;
+        F.im[ri] = a.y;
+        G.re[ri] = b.x;
+        G.im[ri] = b.y;
+      }
+      for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+        const SweepOp &op = P.op[o];
+        if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
+          double sr = 0.0, si = 0.0;
+          inner_op<Real>(F, G, coef, op, gbase, jb, sr, si);
+          // Warp sum (the warp is partial when the tile has < 32 threads).
+          constexpr unsigned kMask = NT >= 32 ? 0xffffffffu : ((1u << NT) - 1u);
+#pragma unroll
+          for (int off = (NT >= 32 ? 16 : NT / 2); off > 0; off >>= 1) {
+            sr += __shfl_xor_sync(kMask, sr, off);
+            si += __shfl_xor_sync(kMask, si, off);
+          }
+          if (lane == 0) {
+            double2 &a = acc[warp * kMaxInner + op.slot];
+            a.x += sr;
+            a.y += si;
+          }
+        } else {
+          apply_op<Real, kAdjAmps>(F, coef, op, gbase, jb);
+          apply_op<Real, kAdjAmps>(G, coef, op, gbase, jb);
+        }
+      }
+#pragma unroll
+      for (int ri = 0; ri < kAdjAmps; ++ri) {
+        const uint32_t s = sb ^ ((ri & 1) ? w0 : 0) ^ ((ri & 2) ? w1 : 0) ^ ((ri & 4) ? w2 : 0);
+        C2 a, b;
+        a.x = F.re[ri];
+        a.y = F.im[ri];
+        b.x = G.re[ri];
+        b.y = G.im[ri];
+        ftile[s] = a;
+        ltile[s] = b;
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (uint32_t it = 0; it < PER; ++it) {
+      const uint32_t j = it * NT + tid;
+      const uint64_t g = gbase | hitab[j >> L] | (j & LOWMASK);
+      const uint32_t slot = s_tid ^ swz<Real>(it * NT);
+      psi[g] = ftile[slot];
+      lam[g] = ltile[slot];
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  cp_async_wait_prev();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  for (uint32_t i = tid; i < NW * kMaxInner; i += NT)
+    partials[size_t(blockIdx.x) * NW * kMaxInner + i] = acc[i];
+}
+
+struct InnerSlots {
+  uint32_t nslots;
+  uint32_t nrows;  // blocks x warps
+  uint32_t global[kMaxInner];
+};
+
+// ipvals[global[s]] += sum over rows of partials[row * kMaxInner + s], in row
+// order (deterministic).  One block per slot.
+static __global__ void __launch_bounds__(kReduceThreads)
+    inner_reduce_kernel(const double2 *__restrict__ partials, const __grid_constant__ InnerSlots S,
+                        double2 *__restrict__ ipvals) {
+  const uint32_t s = blockIdx.x;
+  double r = 0.0, i = 0.0;
+  for (uint32_t row = threadIdx.x; row < S.nrows; row += blockDim.x) {
+    const double2 v = partials[size_t(row) * kMaxInner + s];
+    r += v.x;
+    i += v.y;
+  }
+  r = block_sum(r);
+  i = block_sum(i);
+  if (threadIdx.x == 0) {
+    double2 &o = ipvals[S.global[s]];
+    o.x += r;
+    o.y += i;
+  }
+}
+
+}  // namespace sq

@@ -14,6 +14,8 @@
 #include <vector>
 
 #include "../../include/snuqs_b200.h"
+#include "adjoint_kernels.cuh"
+#include "adjoint_plan.h"
 #include "host_ops.h"
 #include "reduce_kernels.cuh"
 #include "sweep_kernels.cuh"
@@ -132,7 +134,52 @@ static uint32_t pick_tile_bits(int dtype, uint32_t n, uint32_t requested) {
 }
 
 template <typename Real>
+static const void *adjoint_fn(uint32_t m) {
+  if constexpr (sizeof(Real) == 8) {
+    switch (m) {
+      case 4: return SQ_ADJOINT_PTR_NAME(double, 4)();
+      case 7: return SQ_ADJOINT_PTR_NAME(double, 7)();
+      case 10: return SQ_ADJOINT_PTR_NAME(double, 10)();
+    }
+  } else {
+    switch (m) {
+      case 4: return SQ_ADJOINT_PTR_NAME(float, 4)();
+      case 7: return SQ_ADJOINT_PTR_NAME(float, 7)();
+      case 11: return SQ_ADJOINT_PTR_NAME(float, 11)();
+    }
+  }
+  return nullptr;
+}
+
+static uint32_t pick_adjoint_tile_bits(int dtype, uint32_t n) {
+  uint32_t best = 0;
+  if (dtype == SQ_C64) {
+    for (int m : sq::kAdjTileBitsC64)
+      if (uint32_t(m) <= n) best = uint32_t(m);
+  } else {
+    for (int m : sq::kAdjTileBitsC128)
+      if (uint32_t(m) <= n) best = uint32_t(m);
+  }
+  return best;
+}
+
+template <typename Real>
+static size_t adjoint_smem(uint32_t m, uint32_t ncoef) {
+  const uint32_t l = uint32_t(sq::sweep_low_bits(int(m)));
+  const uint32_t nt = 1u << (m - sq::kAdjRegBits);
+  const uint32_t nw = (nt + 31) / 32;
+  return 4 * (size_t(1) << m) * 2 * sizeof(Real) + size_t((ncoef + 1) & ~1u) * 2 * sizeof(Real) +
+         (size_t(1) << (m - l)) * 8 + size_t(nw) * sq::kMaxInner * sizeof(double2);
+}
+
+template <typename Real>
 static int set_sweep_attributes() {
+  for (uint32_t m = 4; m <= uint32_t(sq::kMaxTileBits); ++m) {
+    const void *fn = adjoint_fn<Real>(m);
+    if (!fn) continue;
+    SQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(adjoint_smem<Real>(m, sq::kMaxCoef))));
+  }
   for (uint32_t m = 4; m <= uint32_t(sq::kMaxTileBits); ++m) {
     const void *fn = sweep_fn<Real>(m);
     if (!fn) continue;
@@ -475,6 +522,17 @@ int sq_host_free(void *ptr) {
 }
 
 int sq_gate_qubits(int gate) { return sq::gate_qubits(gate); }
+
+int sq_gate_matrix_derivative(int gate, const double *angles, uint32_t nangles, uint32_t param,
+                              double *out, uint32_t *k) {
+  if (!out || (nangles && !angles)) return fail(SQ_ERR_INVALID, "null pointer");
+  std::vector<cplx> m;
+  const int kk = sq::gate_matrix_derivative(gate, angles, nangles, int(param), m);
+  if (kk < 0) return fail(SQ_ERR_INVALID, "gate %d has no angle %u", gate, param);
+  std::memcpy(out, m.data(), m.size() * sizeof(cplx));
+  if (k) *k = uint32_t(kk);
+  return SQ_OK;
+}
 
 int sq_gate_matrix(int gate, const double *angles, uint32_t nangles, double *out, uint32_t *k) {
   if (!out) return fail(SQ_ERR_INVALID, "null output");
@@ -834,3 +892,210 @@ int sq_norm2(sq_state *s, double *out, void *stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint gradient
+// ---------------------------------------------------------------------------
+namespace {
+
+// lambda = H psi (Pauli-string sum) and E = Re <psi|lambda>, on `st`.
+template <typename Real>
+int pauli_apply(sq_state *psi, sq_state *lam, const char *paulis, const double *w, uint32_t nt,
+                double *partial, uint32_t blocks, double *e_dev, cudaStream_t st) {
+  using C2 = typename sq::Vec2<Real>::T;
+  const uint32_t n = psi->n;
+  std::vector<uint64_t> xm(nt), zym(nt);
+  std::vector<int> ny(nt);
+  for (uint32_t t = 0; t < nt; ++t)
+    for (uint32_t q = 0; q < n; ++q) {
+      const uint64_t bit = uint64_t(1) << (n - 1 - q);
+      switch (paulis[size_t(t) * n + q]) {
+        case 'I': case 'i': break;
+        case 'X': case 'x': xm[t] |= bit; break;
+        case 'Y': case 'y': xm[t] |= bit; zym[t] |= bit; ny[t]++; break;
+        case 'Z': case 'z': zym[t] |= bit; break;
+        default: return fail(SQ_ERR_INVALID, "term %u: bad Pauli character", t);
+      }
+    }
+  std::vector<uint32_t> idx(nt);
+  for (uint32_t i = 0; i < nt; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return xm[a] < xm[b]; });
+  auto P = std::make_unique<sq::PauliApplyParams>();
+  std::memset(P.get(), 0, sizeof(*P));
+  P->n = n;
+  uint32_t k = 0;
+  for (uint32_t pos = 0; pos < nt;) {
+    uint32_t end = pos;
+    while (end < nt && xm[idx[end]] == xm[idx[pos]]) ++end;
+    if (P->ngroups >= uint32_t(sq::kMaxGroups) || nt > uint32_t(sq::kMaxTerms))
+      return fail(SQ_ERR_UNSUPPORTED, "adjoint: at most %d terms in %d flip groups",
+                  sq::kMaxTerms, sq::kMaxGroups);
+    sq::PauliApplyGroup &g = P->g[P->ngroups++];
+    g.x = xm[idx[pos]];
+    g.t0 = k;
+    for (uint32_t e = pos; e < end; ++e) {
+      const uint32_t t = idx[e];
+      static const double pr[4] = {1, 0, -1, 0}, pi[4] = {0, -1, 0, 1};  // (-i)^ny
+      P->zy[k] = zym[t];
+      P->wr[k] = w[t] * pr[ny[t] & 3];
+      P->wi[k] = w[t] * pi[ny[t] & 3];
+      ++k;
+    }
+    g.t1 = k;
+    pos = end;
+  }
+  sq::pauli_apply_kernel<Real><<<blocks, sq::kReduceThreads, 0, st>>>(
+      static_cast<const C2 *>(psi->data), static_cast<C2 *>(lam->data), *P, partial);
+  SQ_CUDA(cudaGetLastError());
+  sq::finalize_sum_kernel<<<1, sq::kReduceThreads, 0, st>>>(partial, blocks, e_dev);
+  SQ_CUDA(cudaGetLastError());
+  return SQ_OK;
+}
+
+template <typename Real>
+int adjoint_sweep(sq_state *psi, sq_state *lam, const sq::PlannedSweep &ps, double2 *partials,
+                  size_t partial_rows, double2 *ipvals, int sms, cudaStream_t st) {
+  using C2 = typename sq::Vec2<Real>::T;
+  auto P = std::make_unique<sq::SweepParams<Real>>();
+  std::memset(P.get(), 0, sizeof(*P));
+  P->h = ps.h;
+  std::copy(ps.ph.begin(), ps.ph.end(), P->ph);
+  std::copy(ps.op.begin(), ps.op.end(), P->op);
+  for (size_t i = 0; i < ps.coef.size(); ++i) {
+    P->coef[2 * i] = Real(ps.coef[i].real());
+    P->coef[2 * i + 1] = Real(ps.coef[i].imag());
+  }
+  const uint32_t m = ps.h.m;
+  const void *fn = adjoint_fn<Real>(m);
+  if (!fn) return fail(SQ_ERR_INVALID, "internal: no adjoint kernel for %u tile bits", m);
+  const int threads = 1 << (m - sq::kAdjRegBits);
+  const int nw = (threads + 31) / 32;
+  const size_t smem = adjoint_smem<Real>(m, ps.h.ncoef);
+  int per_sm = 0;
+  SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  if (per_sm < 1) per_sm = 1;
+  const uint64_t grid = std::min<uint64_t>(
+      std::min<uint64_t>(ps.h.num_tiles, uint64_t(per_sm) * sms), partial_rows / uint64_t(nw));
+  C2 *a = static_cast<C2 *>(psi->data);
+  C2 *b = static_cast<C2 *>(lam->data);
+  void *args[] = {&a, &b, P.get(), &partials};
+  SQ_CUDA(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(threads), args, smem, st));
+  psi->launches++;
+  if (!ps.inner_global.empty()) {
+    sq::InnerSlots S;
+    std::memset(&S, 0, sizeof(S));
+    S.nslots = uint32_t(ps.inner_global.size());
+    S.nrows = uint32_t(grid) * uint32_t(nw);
+    std::copy(ps.inner_global.begin(), ps.inner_global.end(), S.global);
+    sq::inner_reduce_kernel<<<S.nslots, sq::kReduceThreads, 0, st>>>(partials, S, ipvals);
+    SQ_CUDA(cudaGetLastError());
+  }
+  return SQ_OK;
+}
+
+template <typename Real>
+int adjoint_impl(sq_state *psi, sq_state *lam, const sq::AdjointPlan &ap, const char *paulis,
+                 const double *w, uint32_t nt, double *energy, std::vector<double2> &ip,
+                 cudaStream_t st) {
+  DeviceInfo di;
+  SQ_TRY(device_info(psi->device, di));
+  const uint32_t n = psi->n;
+  // Forward pass on psi.
+  SQ_TRY(sq_init_basis(psi, 0, st));
+  sq::PlanOptions fopt;
+  fopt.tile_bits = pick_tile_bits(psi->dtype, n, psi->tile_bits);
+  fopt.max_dense_k = sizeof(Real) == 4 ? 4 : 3;
+  std::vector<sq::PlannedLaunch> fplan, rplan;
+  sq::PlanOptions ropt;
+  ropt.tile_bits = pick_adjoint_tile_bits(psi->dtype, n);
+  ropt.reg_bits = sq::kAdjRegBits;
+  ropt.max_dense_k = sq::kAdjRegBits;
+  try {
+    fplan = sq::plan_sweeps(ap.forward, n, fopt);
+    rplan = sq::plan_sweeps(ap.reverse, n, ropt);
+  } catch (const std::exception &e) {
+    return fail(SQ_ERR_INVALID, "adjoint planner: %s", e.what());
+  }
+  for (const auto &pl : fplan) {
+    if (pl.is_sweep) {
+      SQ_TRY(launch_sweep<Real>(psi, pl.sweep, st));
+    } else {
+      SQ_TRY(launch_gate<Real>(psi->data, n, as_dense(pl.gate), nullptr, st, di.sms));
+    }
+  }
+  // Device scratch for this call (stream-ordered).
+  const uint32_t red_blocks = uint32_t(std::max<uint64_t>(
+      1, std::min<uint64_t>(((uint64_t(1) << n) + sq::kReduceThreads - 1) / sq::kReduceThreads,
+                            uint64_t(di.sms) * 4)));
+  const size_t rows = size_t(di.sms) * 64;  // blocks x warps of one adjoint launch, at most
+  const size_t nip = std::max<size_t>(1, ap.occurrences.size());
+  void *scratch = nullptr;
+  const size_t bytes = (red_blocks + 2) * sizeof(double) + nip * sizeof(double2) +
+                       rows * sq::kMaxInner * sizeof(double2) + 64;
+  SQ_CUDA(cudaMallocAsync(&scratch, bytes, st));
+  auto *red = static_cast<double *>(scratch);
+  auto *e_dev = red + red_blocks;
+  auto *ipvals = reinterpret_cast<double2 *>(
+      (reinterpret_cast<uintptr_t>(e_dev + 2) + 15) & ~uintptr_t(15));
+  auto *partials = ipvals + nip;
+  int status = SQ_OK;
+  auto run = [&]() -> int {
+    SQ_CUDA(cudaMemsetAsync(ipvals, 0, nip * sizeof(double2), st));
+    SQ_TRY(pauli_apply<Real>(psi, lam, paulis, w, nt, red, red_blocks, e_dev, st));
+    for (const auto &pl : rplan) {
+      if (pl.is_sweep) {
+        SQ_TRY(adjoint_sweep<Real>(psi, lam, pl.sweep, partials, rows, ipvals, di.sms, st));
+      } else {
+        const sq::HostOp d = as_dense(pl.gate);
+        SQ_TRY(launch_gate<Real>(psi->data, n, d, nullptr, st, di.sms));
+        SQ_TRY(launch_gate<Real>(lam->data, n, d, nullptr, st, di.sms));
+      }
+    }
+    ip.assign(nip, make_double2(0.0, 0.0));
+    SQ_CUDA(cudaMemcpyAsync(ip.data(), ipvals, nip * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    SQ_CUDA(cudaMemcpyAsync(energy, e_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SQ_CUDA(cudaStreamSynchronize(st));
+    return SQ_OK;
+  };
+  status = run();
+  cudaFreeAsync(scratch, st);
+  return status;
+}
+
+}  // namespace
+
+extern "C" int sq_adjoint_gradient(sq_state *psi, sq_state *lam, const sq_circuit_op *ops,
+                                   uint32_t nops, const char *paulis, const double *weights,
+                                   uint32_t n_terms, uint32_t n_params, double *energy,
+                                   double *grad, void *stream) {
+  if (!psi || !lam || (nops && !ops) || (n_terms && (!paulis || !weights)) || !energy ||
+      (n_params && !grad))
+    return fail(SQ_ERR_INVALID, "null pointer");
+  if (psi == lam || psi->n != lam->n || psi->dtype != lam->dtype)
+    return fail(SQ_ERR_INVALID, "adjoint: psi and lam must be two states of one size and precision");
+  if (psi->n < uint32_t(sq::kRegBits))
+    return fail(SQ_ERR_UNSUPPORTED, "adjoint: needs at least 4 qubits");
+  SQ_TRY(use_device(psi->device));
+  psi->pending.clear();
+  lam->pending.clear();
+  sq::AdjointPlan ap;
+  try {
+    sq::build_adjoint(ops, nops, psi->n, ap);
+  } catch (const std::exception &e) {
+    return fail(SQ_ERR_INVALID, "%s", e.what());
+  }
+  for (const auto &oc : ap.occurrences)
+    if (oc.first >= int32_t(n_params))
+      return fail(SQ_ERR_INVALID, "adjoint: parameter index %d >= n_params %u", oc.first, n_params);
+  std::vector<double2> ip;
+  auto st = static_cast<cudaStream_t>(stream);
+  SQ_TRY(psi->dtype == SQ_C64
+             ? adjoint_impl<float>(psi, lam, ap, paulis, weights, n_terms, energy, ip, st)
+             : adjoint_impl<double>(psi, lam, ap, paulis, weights, n_terms, energy, ip, st));
+  for (uint32_t p = 0; p < n_params; ++p) grad[p] = 0.0;
+  for (size_t s = 0; s < ap.occurrences.size(); ++s) {
+    const auto &oc = ap.occurrences[s];
+    if (oc.first >= 0) grad[oc.first] += 2.0 * ip[s].x * oc.second;
+  }
+  return SQ_OK;
+}

@@ -139,13 +139,95 @@ int gate_matrix(int g, const double *a, uint32_t na, std::vector<cplx> &out) {
   return k;
 }
 
+int gate_matrix_derivative(int g, const double *a, uint32_t na, int param, std::vector<cplx> &out) {
+  const int k = gate_qubits(g);
+  const int nang = gate_num_angles(g);
+  if (k < 0 || int(na) < nang || param < 0 || param >= nang) return -1;
+  const int d = 1 << k;
+  out.assign(size_t(d) * d, cplx(0, 0));
+  auto M = [&](int r, int c) -> cplx & { return out[size_t(r) * d + c]; };
+  const cplx I(0, 1);
+  const double th = a[0];
+  const double c = std::cos(th / 2), s = std::sin(th / 2);
+  switch (g) {
+    case SQ_GATE_PHASE_SHIFT: M(1, 1) = I * cis(th); break;
+    case SQ_GATE_CPHASE_SHIFT: M(3, 3) = I * cis(th); break;
+    case SQ_GATE_CPHASE_SHIFT00: M(0, 0) = I * cis(th); break;
+    case SQ_GATE_CPHASE_SHIFT01: M(1, 1) = I * cis(th); break;
+    case SQ_GATE_CPHASE_SHIFT10: M(2, 2) = I * cis(th); break;
+    case SQ_GATE_GPHASE: M(0, 0) = I * cis(th); break;
+    case SQ_GATE_ROT_X:
+      M(0, 0) = M(1, 1) = -s / 2;
+      M(0, 1) = M(1, 0) = cplx(0, -c / 2);
+      break;
+    case SQ_GATE_ROT_Y:
+      M(0, 0) = M(1, 1) = -s / 2;
+      M(0, 1) = -c / 2;
+      M(1, 0) = c / 2;
+      break;
+    case SQ_GATE_ROT_Z:
+      M(0, 0) = -I / 2.0 * cis(-th / 2.);
+      M(1, 1) = I / 2.0 * cis(th / 2.);
+      break;
+    case SQ_GATE_PSWAP: M(1, 2) = M(2, 1) = I * cis(th); break;
+    case SQ_GATE_XY:
+      M(1, 1) = M(2, 2) = -s / 2;
+      M(1, 2) = M(2, 1) = cplx(0, c / 2);
+      break;
+    case SQ_GATE_XX:
+      M(0, 0) = M(1, 1) = M(2, 2) = M(3, 3) = -s / 2;
+      M(0, 3) = M(1, 2) = M(2, 1) = M(3, 0) = cplx(0, -c / 2);
+      break;
+    case SQ_GATE_YY:
+      M(0, 0) = M(1, 1) = M(2, 2) = M(3, 3) = -s / 2;
+      M(0, 3) = M(3, 0) = cplx(0, c / 2);
+      M(1, 2) = M(2, 1) = cplx(0, -c / 2);
+      break;
+    case SQ_GATE_ZZ:
+      M(0, 0) = M(3, 3) = -I / 2.0 * cis(-th / 2.);
+      M(1, 1) = M(2, 2) = I / 2.0 * cis(th / 2.);
+      break;
+    case SQ_GATE_U: {
+      const cplx el = cis(a[2]), ep = cis(a[1]), epl = cis(a[1] + a[2]);
+      if (param == 0) {
+        M(0, 0) = -s / 2;
+        M(0, 1) = -el * (c / 2);
+        M(1, 0) = ep * (c / 2);
+        M(1, 1) = -epl * (s / 2);
+      } else if (param == 1) {
+        M(1, 0) = I * ep * s;
+        M(1, 1) = I * epl * c;
+      } else {
+        M(0, 1) = -I * el * s;
+        M(1, 1) = I * epl * c;
+      }
+    } break;
+    case SQ_GATE_PRX: {
+      const cplx em = cis(-a[1]), ep = cis(a[1]);
+      if (param == 0) {
+        M(0, 0) = M(1, 1) = -s / 2;
+        M(0, 1) = -I * em * (c / 2);
+        M(1, 0) = -I * ep * (c / 2);
+      } else {
+        M(0, 1) = -em * s;
+        M(1, 0) = ep * s;
+      }
+    } break;
+    default: return -1;
+  }
+  return k;
+}
+
 uint64_t HostOp::target_mask() const {
   uint64_t r = 0;
   for (int b : tbits) r |= uint64_t(1) << b;
   return r;
 }
 uint64_t HostOp::touched_mask() const { return target_mask() | cmask; }
-uint64_t HostOp::nondiag_mask() const { return kind == kOpDiag ? 0 : target_mask(); }
+uint64_t HostOp::nondiag_mask() const {
+  if (kind == kOpDiag || (kind == kOpInner && inner_diag)) return 0;
+  return target_mask();
+}
 
 namespace {
 

@@ -16,6 +16,10 @@ using cplx = std::complex<double>;
 int gate_matrix(int gate, const double *angles, uint32_t nangles, std::vector<cplx> &m);
 int gate_qubits(int gate);
 int gate_num_angles(int gate);
+// d/d angle[param] of gate_matrix(gate, angles) (analytic).  Returns k, or -1
+// for a gate without that parameter.
+int gate_matrix_derivative(int gate, const double *angles, uint32_t nangles, int param,
+                           std::vector<cplx> &m);
 
 // One queued gate after qubit -> index-bit translation.
 //   kind kOpDense: m is 4^k row-major, tbits[0] is the MSB of its index.
@@ -23,7 +27,11 @@ int gate_num_angles(int gate);
 // Controls (cmask/cval, index bits) apply to dense ops; diagonal ops fold
 // their controls into the diagonal.
 struct HostOp {
-  uint8_t kind = kOpDense;
+  uint8_t kind = kOpDense;  // kOpDense / kOpDiag / kOpInner
+  // kOpInner (adjoint): accumulate <lambda| K |phi> into inner-product slot
+  // `slot`; K is m (dense 4^k, or the 2^k diagonal when inner_diag).
+  bool inner_diag = false;
+  uint32_t slot = 0;
   std::vector<int> tbits;
   uint64_t cmask = 0, cval = 0;
   std::vector<cplx> m;
@@ -47,6 +55,8 @@ struct PlannedSweep {
   std::vector<SweepOp> op;
   std::vector<cplx> coef;
   uint32_t ngates = 0;  // queued ops it carries
+  // Adjoint sweeps: global inner-product slot of each local slot 0, 1, ...
+  std::vector<uint32_t> inner_global;
 };
 
 struct PlannedLaunch {
@@ -62,6 +72,9 @@ struct PlanOptions {
   // 4-qubit dense matrix needs a second copy of all 16 amplitudes), 4 for
   // complex64.  Wider dense gates run unfused.
   uint32_t max_dense_k = 3;
+  // Register bits per phase: 4 (16 amplitudes per thread, the sweep kernel)
+  // or 3 (8 amplitudes per state per thread, the two-state adjoint kernel).
+  uint32_t reg_bits = kRegBits;
 };
 
 // Packs ops (in circuit order) into fused sweeps for an n-qubit state.

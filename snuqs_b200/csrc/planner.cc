@@ -24,26 +24,30 @@ namespace {
 int popc64(uint64_t x) { return __builtin_popcountll(x); }
 
 struct SweepBuilder {
-  uint32_t n, m, l, max_dense_k = 3;
+  uint32_t n, m, l, max_dense_k = 3, reg_bits = kRegBits;
   uint64_t S;  // tile bits (global index bits)
   std::vector<const HostOp *> ops;
   std::vector<uint64_t> phase_regs;  // register bits (global) of each phase
   std::vector<uint32_t> phase_first; // first op index of each phase
-  uint32_t ncoef = 0;
+  uint32_t ncoef = 0, ninner = 0;
 
   SweepBuilder(uint32_t n_, uint32_t m_, uint32_t l_) : n(n_), m(m_), l(l_) {
     S = (l >= 64) ? ~uint64_t(0) : ((uint64_t(1) << l) - 1);
   }
 
+  static bool is_diag(const HostOp &op) {
+    return op.kind == kOpDiag || (op.kind == kOpInner && op.inner_diag);
+  }
   static uint32_t coef_count(const HostOp &op) {
-    return op.kind == kOpDiag ? (1u << op.tbits.size()) : (1u << (2 * op.tbits.size()));
+    return is_diag(op) ? (1u << op.tbits.size()) : (1u << (2 * op.tbits.size()));
   }
 
   // Would `op` fit (tile, register, budget)?  If so, add it.
   bool try_add(const HostOp &op) {
     if (ops.size() >= size_t(kMaxOps)) return false;
     if (ncoef + coef_count(op) > uint32_t(kMaxCoef)) return false;
-    if (op.kind == kOpDiag) {
+    if (op.kind == kOpInner && ninner >= uint32_t(kMaxInner)) return false;
+    if (is_diag(op)) {
       if (op.tbits.size() > size_t(kMaxDiagK)) return false;
       if (phase_regs.empty()) {
         phase_regs.push_back(0);
@@ -51,12 +55,14 @@ struct SweepBuilder {
       }
       ops.push_back(&op);
       ncoef += coef_count(op);
+      if (op.kind == kOpInner) ++ninner;
       return true;
     }
-    if (op.tbits.size() > size_t(max_dense_k)) return false;
+    const uint32_t kmax = op.kind == kOpInner ? reg_bits : max_dense_k;
+    if (op.tbits.size() > size_t(kmax)) return false;
     const uint64_t T = op.target_mask();
     if (uint32_t(popc64(S | T)) > m) return false;
-    const bool new_phase = phase_regs.empty() || popc64(phase_regs.back() | T) > kRegBits;
+    const bool new_phase = phase_regs.empty() || popc64(phase_regs.back() | T) > int(reg_bits);
     if (new_phase && phase_regs.size() >= size_t(kMaxPhases)) return false;
     S |= T;
     if (new_phase) {
@@ -67,6 +73,7 @@ struct SweepBuilder {
     }
     ops.push_back(&op);
     ncoef += coef_count(op);
+    if (op.kind == kOpInner) ++ninner;
     return true;
   }
 
@@ -164,7 +171,7 @@ PlannedSweep SweepBuilder::finish() const {
     uint32_t regpos = 0;  // bitmask of tile positions
     for (int b = 0; b < 64; ++b)
       if ((phase_regs[p] >> b) & 1) regpos |= 1u << rank_in(tile, b);
-    for (int pos = int(m) - 1; pos >= 0 && __builtin_popcount(regpos) < kRegBits; --pos)
+    for (int pos = int(m) - 1; pos >= 0 && __builtin_popcount(regpos) < int(reg_bits); --pos)
       regpos |= 1u << pos;
     SweepPhase ph{};
     int r = 0;
@@ -178,7 +185,7 @@ PlannedSweep SweepBuilder::finish() const {
   const uint32_t lowpos = (1u << std::min<uint32_t>(l, 5)) - 1;
   auto regmask = [&](const SweepPhase &ph) {
     uint32_t x = 0;
-    for (int b = 0; b < kRegBits; ++b) x |= 1u << ph.reg[b];
+    for (uint32_t b = 0; b < reg_bits; ++b) x |= 1u << ph.reg[b];
     return x;
   };
   if ((regmask(ps.ph.front()) & lowpos) == 0) h.flags |= kDirectLoad;
@@ -190,8 +197,8 @@ PlannedSweep SweepBuilder::finish() const {
     auto regof = [&](int gbit) -> int {  // register position of a global bit, or -1
       if (!((tile >> gbit) & 1)) return -1;
       const int pos = rank_in(tile, gbit);
-      for (int r = 0; r < kRegBits; ++r)
-        if (ph.reg[r] == pos) return r;
+      for (uint32_t r = 0; r < reg_bits; ++r)
+        if (ph.reg[r] == pos) return int(r);
       return -1;
     };
     // Route a condition bit (global bit b must equal v) to the register,
@@ -217,17 +224,21 @@ PlannedSweep SweepBuilder::finish() const {
       so.k = uint8_t(op.tbits.size());
       so.coef = uint32_t(ps.coef.size());
       const int k = int(op.tbits.size());
-      if (op.kind == kOpDiag) {
+      if (is_diag(op)) {
         int nonone = 0, e = -1;
         for (size_t x = 0; x < op.m.size(); ++x)
           if (op.m[x] != cplx(1, 0)) ++nonone, e = int(x);
-        if (nonone == 1) {
+        if (op.kind == kOpDiag && nonone == 1) {
           so.kind = kSwPhase;
           for (int t = 0; t < k; ++t) add_cond(so, op.tbits[t], (e >> (k - 1 - t)) & 1);
           if (op.m[e] == cplx(-1, 0)) so.aux |= kAuxPure;
           ps.coef.push_back(op.m[e]);
         } else {
-          so.kind = kSwDiag;
+          so.kind = op.kind == kOpInner ? kSwInnerDiag : kSwDiag;
+          if (op.kind == kOpInner) {
+            so.slot = uint32_t(ps.inner_global.size());
+            ps.inner_global.push_back(op.slot);
+          }
           // Register targets -> canonical low index bits; the rest -> high
           // bits, most significant first.
           uint32_t vmask = 0;
@@ -288,7 +299,14 @@ PlannedSweep SweepBuilder::finish() const {
           for (int c = 0; c < d; ++c) cm[size_t(remap(r)) * d + remap(c)] = op.m[size_t(r) * d + c];
         for (int b = 0; b < 64; ++b)
           if ((op.cmask >> b) & 1) add_cond(so, b, (op.cval >> b) & 1);
-        encode_dense(so, cm, k, ps.coef);
+        if (op.kind == kOpInner) {
+          so.kind = kSwInnerDense;
+          so.slot = uint32_t(ps.inner_global.size());
+          ps.inner_global.push_back(op.slot);
+          ps.coef.insert(ps.coef.end(), cm.begin(), cm.end());
+        } else {
+          encode_dense(so, cm, k, ps.coef);
+        }
       }
       so.code = uint8_t(sq_op_code(so.kind, so.vmask, so.aux));
       ps.op.push_back(so);
@@ -319,8 +337,11 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
   while (head < rem.size()) {
     const HostOp &first = *rem[head];
     const bool first_fusable =
-        !(first.kind == kOpDense && first.tbits.size() > size_t(std::min<uint32_t>(opt.max_dense_k, kRegBits))) &&
+        !(first.kind == kOpDense &&
+          first.tbits.size() > size_t(std::min<uint32_t>(opt.max_dense_k, opt.reg_bits))) &&
         !(first.kind == kOpDiag && first.tbits.size() > size_t(kMaxDiagK));
+    if (!first_fusable && first.kind == kOpInner)
+      throw std::logic_error("planner: inner-product op too wide for a sweep");
     if (!first_fusable) {
       PlannedLaunch pl;
       pl.is_sweep = false;
@@ -330,7 +351,8 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       continue;
     }
     SweepBuilder sb(n, m, l);
-    sb.max_dense_k = std::min<uint32_t>(opt.max_dense_k, kRegBits);
+    sb.reg_bits = opt.reg_bits;
+    sb.max_dense_k = std::min<uint32_t>(opt.max_dense_k, opt.reg_bits);
     std::vector<const HostOp *> skipped;
     uint64_t blockT = 0, blockAll = 0;  // non-diagonal / all bits of skipped gates
     size_t i = head;

@@ -22,9 +22,10 @@ constexpr int kMaxPhases = 24;
 constexpr int kMaxOps = 64;
 constexpr int kMaxCoef = 1024;              // complex coefficients per sweep
 constexpr int kMaxDiagK = 8;                // targets of one diagonal op
+constexpr int kMaxInner = 32;               // inner-product ops per adjoint sweep
 
 // HostOp kinds (structure analysis) ...
-enum OpKind : uint8_t { kOpDense = 1, kOpDiag = 2 };
+enum OpKind : uint8_t { kOpDense = 1, kOpDiag = 2, kOpInner = 3 };
 // ... and the specialised sweep-op kinds the planner encodes them as.  The
 // coefficient layout of each kind:
 //   kSwDense  4^k complex, canonical row-major (matrix bit b <-> b-th set bit
@@ -36,8 +37,12 @@ enum OpKind : uint8_t { kOpDense = 1, kOpDiag = 2 };
 //             out_r = c_r a_r + f s_r a_(r^x), f = i when aux & kAuxImag
 //   kSwSwap2  p12, p21:          out1 = p12 a2, out2 = p21 a1
 //   kSwPhase  p:                 a *= p where the op's condition holds
+//   kSwInnerDiag / kSwInnerDense (adjoint sweeps only): accumulate
+//             <lambda| K |phi> into inner-product slot `slot`, K laid out as
+//             kSwDiag / kSwDense; the states are not modified.
 enum SweepKind : uint8_t {
-  kSwDense = 1, kSwDiag = 2, kSwAnti1 = 3, kSwXRot = 4, kSwSwap2 = 5, kSwPhase = 6
+  kSwDense = 1, kSwDiag = 2, kSwAnti1 = 3, kSwXRot = 4, kSwSwap2 = 5, kSwPhase = 6,
+  kSwInnerDiag = 7, kSwInnerDense = 8
 };
 enum SweepAux : uint8_t {
   kAuxXMask = 3,  // XRot: partner XOR mask over the op's canonical local bits
@@ -60,6 +65,9 @@ SQ_HD constexpr int sweep_low_bits(int m) { return m >= kLowBits + kRegBits ? kL
 constexpr int kTileBitsC128[] = {4, 7, 10, 11, 12};
 constexpr int kTileBitsC64[] = {4, 7, 10, 12};
 constexpr int kDefaultTileBitsC128 = 11;
+// Two-state adjoint sweeps (twice the shared memory per tile).
+constexpr int kAdjTileBitsC128[] = {4, 7, 10};
+constexpr int kAdjTileBitsC64[] = {4, 7, 11};
 constexpr int kDefaultTileBitsC64 = 12;
 
 // Flat dispatch code of a sweep op: one switch in the kernel selects the
@@ -76,7 +84,9 @@ SQ_HD constexpr int sq_op_code(int kind, int v, int aux) {
          : kind == kSwXRot
              ? 52 + 2 * ((v & (v - 1)) == 0 ? sq_log2_4(v) : 4 + 3 * sq_pair_index(v) + (aux & 3) - 1) +
                    ((aux & kAuxImag) ? 1 : 0)
-             : 96 + v;  // kSwDense
+         : kind == kSwInnerDiag  ? 112 + v
+         : kind == kSwInnerDense ? 128 + v
+                                 : 96 + v;  // kSwDense
 }
 enum SweepFlags : uint32_t { kDirectLoad = 1u, kDirectStore = 2u };
 
@@ -92,7 +102,7 @@ struct SweepOp {
   uint32_t coef;   // offset of the op's coefficients (complex units)
   uint32_t lmask;  // in-tile, non-register control bits (tile-local index)
   uint32_t lval;
-  uint32_t pad1;
+  uint32_t slot;   // kSwInner*: inner-product slot within the sweep
   uint64_t gmask;  // control bits outside the tile (global index)
   uint64_t gval;
   // kSwDiag: the non-register targets, most significant first: each from a

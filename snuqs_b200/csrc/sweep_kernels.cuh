@@ -73,22 +73,24 @@ __device__ __forceinline__ constexpr int ct_ext(int x) {
 // Runs f(g) for every register group g (register index with the bits of V
 // clear).  Without register controls the loop is branch-free; with them each
 // group is predicated on its control bits.
-template <int V, class F>
+template <int NA, int V, class F>
 __device__ __forceinline__ void for_groups(int rmask, int rval, F &&f) {
   if (rmask == 0) {
 #pragma unroll
-    for (int g = 0; g < kRegAmps; ++g)
+    for (int g = 0; g < NA; ++g)
       if (!(g & V)) f(g);
   } else {
 #pragma unroll
-    for (int g = 0; g < kRegAmps; ++g)
+    for (int g = 0; g < NA; ++g)
       if (!(g & V) && ((g & rmask) == rval)) f(g);
   }
 }
 
-template <typename Real>
+// NA register-resident amplitudes of one thread (16 in the sweep kernel, 8
+// per state in the two-state adjoint kernel).
+template <typename Real, int NA = kRegAmps>
 struct Amps {
-  Real re[kRegAmps], im[kRegAmps];
+  Real re[NA], im[NA];
 };
 
 // out = p * a (complex)
@@ -99,11 +101,11 @@ __device__ __forceinline__ void cmul(Real pr, Real pi, Real ar, Real ai, Real &o
 }
 
 // kSwDense on register positions V: row r accumulated left to right.
-template <typename Real, int V>
-__device__ __forceinline__ void op_dense(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V>
+__device__ __forceinline__ void op_dense(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
                                          int rmask, int rval) {
   constexpr int D = 1 << ct_popc<V>();
-  for_groups<V>(rmask, rval, [&](int g) {
+  for_groups<NA, V>(rmask, rval, [&](int g) {
     Real ar[D], ai[D];
 #pragma unroll
     for (int x = 0; x < D; ++x) {
@@ -130,11 +132,11 @@ __device__ __forceinline__ void op_dense(Amps<Real> &A, const typename Vec2<Real
 }
 
 // kSwAnti1 on register bit V: out0 = p0 a1, out1 = p1 a0 (a swap when pure).
-template <typename Real, int V, bool PURE>
-__device__ __forceinline__ void op_anti1(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, bool PURE>
+__device__ __forceinline__ void op_anti1(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
                                          int rmask, int rval) {
   if constexpr (PURE) {
-    for_groups<V>(rmask, rval, [&](int g) {
+    for_groups<NA, V>(rmask, rval, [&](int g) {
       const Real tr = A.re[g], ti = A.im[g];
       A.re[g] = A.re[g | V];
       A.im[g] = A.im[g | V];
@@ -143,7 +145,7 @@ __device__ __forceinline__ void op_anti1(Amps<Real> &A, const typename Vec2<Real
     });
   } else {
     const auto p0 = c[0], p1 = c[1];
-    for_groups<V>(rmask, rval, [&](int g) {
+    for_groups<NA, V>(rmask, rval, [&](int g) {
       const Real a0r = A.re[g], a0i = A.im[g], a1r = A.re[g | V], a1i = A.im[g | V];
       cmul(p0.x, p0.y, a1r, a1i, A.re[g], A.im[g]);
       cmul(p1.x, p1.y, a0r, a0i, A.re[g | V], A.im[g | V]);
@@ -153,8 +155,8 @@ __device__ __forceinline__ void op_anti1(Amps<Real> &A, const typename Vec2<Real
 
 // kSwXRot on register positions V with partner mask X (canonical local bits):
 // out_r = c_r a_r + f s_r a_(r^X).
-template <typename Real, int V, int X, bool IMAG>
-__device__ __forceinline__ void op_xrot(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, int X, bool IMAG>
+__device__ __forceinline__ void op_xrot(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
                                         int rmask, int rval) {
   constexpr int D = 1 << ct_popc<V>();
   Real cr[D], sr[D];
@@ -164,7 +166,7 @@ __device__ __forceinline__ void op_xrot(Amps<Real> &A, const typename Vec2<Real>
     cr[r] = v.x;
     sr[r] = v.y;
   }
-  for_groups<V>(rmask, rval, [&](int g) {
+  for_groups<NA, V>(rmask, rval, [&](int g) {
     Real ar[D], ai[D];
 #pragma unroll
     for (int x = 0; x < D; ++x) {
@@ -189,12 +191,12 @@ __device__ __forceinline__ void op_xrot(Amps<Real> &A, const typename Vec2<Real>
 }
 
 // kSwSwap2 on register positions V (two bits): out1 = p12 a2, out2 = p21 a1.
-template <typename Real, int V, bool PURE>
-__device__ __forceinline__ void op_swap2(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, bool PURE>
+__device__ __forceinline__ void op_swap2(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
                                          int rmask, int rval) {
   constexpr int B1 = ct_dep<V>(1), B2 = ct_dep<V>(2);
   if constexpr (PURE) {
-    for_groups<V>(rmask, rval, [&](int g) {
+    for_groups<NA, V>(rmask, rval, [&](int g) {
       const Real tr = A.re[g | B1], ti = A.im[g | B1];
       A.re[g | B1] = A.re[g | B2];
       A.im[g | B1] = A.im[g | B2];
@@ -203,7 +205,7 @@ __device__ __forceinline__ void op_swap2(Amps<Real> &A, const typename Vec2<Real
     });
   } else {
     const auto p12 = c[0], p21 = c[1];
-    for_groups<V>(rmask, rval, [&](int g) {
+    for_groups<NA, V>(rmask, rval, [&](int g) {
       const Real a1r = A.re[g | B1], a1i = A.im[g | B1], a2r = A.re[g | B2], a2i = A.im[g | B2];
       cmul(p12.x, p12.y, a2r, a2i, A.re[g | B1], A.im[g | B1]);
       cmul(p21.x, p21.y, a1r, a1i, A.re[g | B2], A.im[g | B2]);
@@ -212,12 +214,12 @@ __device__ __forceinline__ void op_swap2(Amps<Real> &A, const typename Vec2<Real
 }
 
 // kSwDiag: coefficient index = thread part << popc(V) | register part.
-template <typename Real, int V>
-__device__ __forceinline__ void op_diag(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V>
+__device__ __forceinline__ void op_diag(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
                                         uint32_t base) {
   const auto *cb = c + (base << ct_popc<V>());
 #pragma unroll
-  for (int ri = 0; ri < kRegAmps; ++ri) {
+  for (int ri = 0; ri < NA; ++ri) {
     const auto d = cb[ct_ext<V>(ri)];
     const Real r = A.re[ri], i = A.im[ri];
     cmul(d.x, d.y, r, i, A.re[ri], A.im[ri]);
@@ -225,12 +227,12 @@ __device__ __forceinline__ void op_diag(Amps<Real> &A, const typename Vec2<Real>
 }
 
 // kSwPhase: a *= p on the register slots whose bits match (rmask, rval).
-template <typename Real, bool NEG>
-__device__ __forceinline__ void op_phase(Amps<Real> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, bool NEG>
+__device__ __forceinline__ void op_phase(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
                                          int rmask, int rval) {
   if constexpr (NEG) {
 #pragma unroll
-    for (int ri = 0; ri < kRegAmps; ++ri)
+    for (int ri = 0; ri < NA; ++ri)
       if ((ri & rmask) == rval) {
         A.re[ri] = -A.re[ri];
         A.im[ri] = -A.im[ri];
@@ -238,7 +240,7 @@ __device__ __forceinline__ void op_phase(Amps<Real> &A, const typename Vec2<Real
   } else {
     const auto p = c[0];
 #pragma unroll
-    for (int ri = 0; ri < kRegAmps; ++ri)
+    for (int ri = 0; ri < NA; ++ri)
       if ((ri & rmask) == rval) {
         const Real r = A.re[ri], i = A.im[ri];
         cmul(p.x, p.y, r, i, A.re[ri], A.im[ri]);
@@ -257,8 +259,8 @@ __device__ __forceinline__ uint32_t diag_base(const SweepOp &op, uint64_t gbase,
   return base;
 }
 
-template <typename Real>
-__device__ __forceinline__ void apply_op(Amps<Real> &A, const typename Vec2<Real>::T *coef,
+template <typename Real, int NA>
+__device__ __forceinline__ void apply_op(Amps<Real, NA> &A, const typename Vec2<Real>::T *coef,
                                          const SweepOp &op, uint64_t gbase, uint32_t jb) {
   // Controls outside the registers are constant for this thread.
   if ((gbase & op.gmask) != op.gval || (jb & op.lmask) != op.lval) return;
@@ -266,31 +268,35 @@ __device__ __forceinline__ void apply_op(Amps<Real> &A, const typename Vec2<Real
   const int rm = op.rmask, rv = op.rval;
 #define SQ_CODE(kind, v, aux) case sq_op_code(kind, v, aux):
   switch (op.code) {
-    SQ_CODE(kSwPhase, 0, 0) op_phase<Real, false>(A, c, rm, rv); break;
-    SQ_CODE(kSwPhase, 0, kAuxPure) op_phase<Real, true>(A, c, rm, rv); break;
-#define SQ_DIAG(V) SQ_CODE(kSwDiag, V, 0) op_diag<Real, V>(A, c, diag_base<Real>(op, gbase, jb)); break;
+    SQ_CODE(kSwPhase, 0, 0) op_phase<Real, NA, false>(A, c, rm, rv); break;
+    SQ_CODE(kSwPhase, 0, kAuxPure) op_phase<Real, NA, true>(A, c, rm, rv); break;
+    // Variants whose register mask V reaches past the NA registers are not
+    // instantiated (the planner never emits them for that register count).
+#define SQ_DIAG(V)                                                                      \
+  SQ_CODE(kSwDiag, V, 0) if constexpr (V < NA) op_diag<Real, NA, V>(A, c, diag_base<Real>(op, gbase, jb)); \
+  break;
     SQ_DIAG(0) SQ_DIAG(1) SQ_DIAG(2) SQ_DIAG(3) SQ_DIAG(4) SQ_DIAG(5) SQ_DIAG(6) SQ_DIAG(7)
     SQ_DIAG(8) SQ_DIAG(9) SQ_DIAG(10) SQ_DIAG(11) SQ_DIAG(12) SQ_DIAG(13) SQ_DIAG(14) SQ_DIAG(15)
 #undef SQ_DIAG
-#define SQ_ANTI(V)                                                               \
-  SQ_CODE(kSwAnti1, V, 0) op_anti1<Real, V, false>(A, c, rm, rv); break;         \
-  SQ_CODE(kSwAnti1, V, kAuxPure) op_anti1<Real, V, true>(A, c, rm, rv); break;
+#define SQ_ANTI(V)                                                                            \
+  SQ_CODE(kSwAnti1, V, 0) if constexpr (V < NA) op_anti1<Real, NA, V, false>(A, c, rm, rv); break; \
+  SQ_CODE(kSwAnti1, V, kAuxPure) if constexpr (V < NA) op_anti1<Real, NA, V, true>(A, c, rm, rv); break;
     SQ_ANTI(1) SQ_ANTI(2) SQ_ANTI(4) SQ_ANTI(8)
 #undef SQ_ANTI
-#define SQ_SWAP(V)                                                               \
-  SQ_CODE(kSwSwap2, V, 0) op_swap2<Real, V, false>(A, c, rm, rv); break;         \
-  SQ_CODE(kSwSwap2, V, kAuxPure) op_swap2<Real, V, true>(A, c, rm, rv); break;
+#define SQ_SWAP(V)                                                                            \
+  SQ_CODE(kSwSwap2, V, 0) if constexpr (V < NA) op_swap2<Real, NA, V, false>(A, c, rm, rv); break; \
+  SQ_CODE(kSwSwap2, V, kAuxPure) if constexpr (V < NA) op_swap2<Real, NA, V, true>(A, c, rm, rv); break;
     SQ_SWAP(3) SQ_SWAP(5) SQ_SWAP(6) SQ_SWAP(9) SQ_SWAP(10) SQ_SWAP(12)
 #undef SQ_SWAP
-#define SQ_XROT(V, X)                                                              \
-  SQ_CODE(kSwXRot, V, X) op_xrot<Real, V, X, false>(A, c, rm, rv); break;          \
-  SQ_CODE(kSwXRot, V, X | kAuxImag) op_xrot<Real, V, X, true>(A, c, rm, rv); break;
+#define SQ_XROT(V, X)                                                                            \
+  SQ_CODE(kSwXRot, V, X) if constexpr (V < NA) op_xrot<Real, NA, V, X, false>(A, c, rm, rv); break; \
+  SQ_CODE(kSwXRot, V, X | kAuxImag) if constexpr (V < NA) op_xrot<Real, NA, V, X, true>(A, c, rm, rv); break;
     SQ_XROT(1, 1) SQ_XROT(2, 1) SQ_XROT(4, 1) SQ_XROT(8, 1)
     SQ_XROT(3, 1) SQ_XROT(3, 2) SQ_XROT(3, 3) SQ_XROT(5, 1) SQ_XROT(5, 2) SQ_XROT(5, 3)
     SQ_XROT(6, 1) SQ_XROT(6, 2) SQ_XROT(6, 3) SQ_XROT(9, 1) SQ_XROT(9, 2) SQ_XROT(9, 3)
     SQ_XROT(10, 1) SQ_XROT(10, 2) SQ_XROT(10, 3) SQ_XROT(12, 1) SQ_XROT(12, 2) SQ_XROT(12, 3)
 #undef SQ_XROT
-#define SQ_DENSE(V) SQ_CODE(kSwDense, V, 0) op_dense<Real, V>(A, c, rm, rv); break;
+#define SQ_DENSE(V) SQ_CODE(kSwDense, V, 0) if constexpr (V < NA) op_dense<Real, NA, V>(A, c, rm, rv); break;
     SQ_DENSE(1) SQ_DENSE(2) SQ_DENSE(3) SQ_DENSE(4) SQ_DENSE(5) SQ_DENSE(6) SQ_DENSE(7)
     SQ_DENSE(8) SQ_DENSE(9) SQ_DENSE(10) SQ_DENSE(11) SQ_DENSE(12) SQ_DENSE(13) SQ_DENSE(14)
 #undef SQ_DENSE
@@ -298,7 +304,7 @@ __device__ __forceinline__ void apply_op(Amps<Real> &A, const typename Vec2<Real
     // the complex64 registers have room (the planner keeps complex128
     // 4-qubit dense gates out of sweeps).
     SQ_CODE(kSwDense, 15, 0)
-      if constexpr (sizeof(Real) == 4) op_dense<Real, 15>(A, c, rm, rv);
+      if constexpr (sizeof(Real) == 4 && NA == 16) op_dense<Real, NA, 15>(A, c, rm, rv);
       break;
     default: break;
   }
@@ -413,7 +419,8 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
         A.re[ri] = v.x;
         A.im[ri] = v.y;
       }
-      for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) apply_op<Real>(A, coef, P.op[o], gbase, jb);
+      for (uint32_t o = ph.op_begin; o < ph.op_end; ++o)
+        apply_op<Real, kRegAmps>(A, coef, P.op[o], gbase, jb);
       if (gstore) {
         // Global index of register slot ri = tbase | selected register-bit
         // weights (disjoint bits).

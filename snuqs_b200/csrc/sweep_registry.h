@@ -16,3 +16,13 @@ SQ_DECLARE_SWEEP(float, 7)
 SQ_DECLARE_SWEEP(float, 10)
 SQ_DECLARE_SWEEP(float, 12)
 #undef SQ_DECLARE_SWEEP
+
+#define SQ_ADJOINT_PTR_NAME(real, m) SQ_SWEEP_CAT(sq_adjoint_kernel_ptr, real, m)
+#define SQ_DECLARE_ADJOINT(real, m) const void *SQ_ADJOINT_PTR_NAME(real, m)();
+SQ_DECLARE_ADJOINT(double, 4)
+SQ_DECLARE_ADJOINT(double, 7)
+SQ_DECLARE_ADJOINT(double, 10)
+SQ_DECLARE_ADJOINT(float, 4)
+SQ_DECLARE_ADJOINT(float, 7)
+SQ_DECLARE_ADJOINT(float, 11)
+#undef SQ_DECLARE_ADJOINT

@@ -62,3 +62,22 @@ def plan_stats(n, gates, tile_bits=12, reorder=True):
     names = ["dense", "diag", "anti1", "xrot", "swap2", "phase"]
     return {"sweeps": int(out[0]), "phases": int(out[1]), "ops": int(out[2]),
             "kinds": {names[i]: int(out[3 + i]) for i in range(6)}, "unfused": int(out[9])}
+
+
+def adjoint(n, ops, terms, nparams, tile_bits=10):
+    """(energy, grad, sweeps) from the host emulation of the adjoint plan."""
+    from snuqs_b200 import capi
+    arr, keep = capi.circuit_ops(ops)
+    flat = "".join(p for _, p in terms).encode()
+    w = np.ascontiguousarray([x for x, _ in terms], dtype=np.float64)
+    e = ctypes.c_double(0)
+    g = np.zeros(max(1, nparams), dtype=np.float64)
+    lib().emu_adjoint.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p,
+                                  ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    r = lib().emu_adjoint(n, ctypes.cast(arr, ctypes.c_void_p), len(ops), flat,
+                          w.ctypes.data_as(ctypes.c_void_p), len(terms), nparams, tile_bits,
+                          ctypes.byref(e), g.ctypes.data_as(ctypes.c_void_p))
+    if r < 0:
+        raise RuntimeError("emulated adjoint failed")
+    return e.value, g[:nparams], r

@@ -9,6 +9,7 @@
 #include <stdexcept>
 #include <vector>
 
+#include "adjoint_plan.h"
 #include "host_ops.h"
 
 using namespace sq;
@@ -20,9 +21,131 @@ uint64_t insert_zero(uint64_t x, uint32_t p) {
   return ((x >> p) << (p + 1)) | lo;
 }
 
-void emulate_sweep(cplx *psi, const PlannedSweep &ps) {
+// Coefficient index of register slot ri for a (inner) diagonal op.
+uint32_t diag_index(const SweepOp &op, uint64_t gbase, uint32_t jb, int ri) {
+  uint32_t base = 0;
+  for (int t = 0; t < op.ndt; ++t) {
+    const uint32_t bit = op.dsrc[t] == kSrcGlobal ? uint32_t(gbase >> op.dpos[t]) & 1u
+                                                  : (jb >> op.dpos[t]) & 1u;
+    base = (base << 1) | bit;
+  }
+  const int V = op.vmask;
+  int r = 0, b = 0;
+  for (int pp = 0; pp < 4; ++pp)
+    if (V & (1 << pp)) {
+      if (ri & (1 << pp)) r |= 1 << b;
+      ++b;
+    }
+  return (base << __builtin_popcount(V)) | uint32_t(r);
+}
+
+// One sweep op on the NA register amplitudes v of one thread (the kernel's
+// apply_op).  Inner-product ops are handled by the caller.
+void apply_sweep_op(const SweepOp &op, const cplx *c, cplx *v, int NA, uint64_t gbase,
+                    uint32_t jb) {
+  if ((gbase & op.gmask) != op.gval || (jb & op.lmask) != op.lval) return;
+  const int V = op.vmask;
+  auto dep = [&](int x) {
+    int r = 0, b = 0;
+    for (int pp = 0; pp < 4; ++pp)
+      if (V & (1 << pp)) {
+        if (x & (1 << b)) r |= 1 << pp;
+        ++b;
+      }
+    return r;
+  };
+  auto groups = [&](auto f) {
+    for (int g = 0; g < NA; ++g)
+      if (!(g & V) && ((g & op.rmask) == op.rval)) f(g);
+  };
+  const bool pure = op.aux & kAuxPure;
+  switch (op.kind) {
+    case kSwPhase:
+      for (int ri = 0; ri < NA; ++ri)
+        if ((ri & op.rmask) == op.rval) v[ri] = pure ? -v[ri] : c[0] * v[ri];
+      break;
+    case kSwDiag:
+      for (int ri = 0; ri < NA; ++ri) v[ri] = c[diag_index(op, gbase, jb, ri)] * v[ri];
+      break;
+    case kSwAnti1:
+      groups([&](int g) {
+        const cplx a0 = v[g], a1 = v[g | V];
+        v[g] = pure ? a1 : c[0] * a1;
+        v[g | V] = pure ? a0 : c[1] * a0;
+      });
+      break;
+    case kSwSwap2: {
+      const int B1 = dep(1), B2 = dep(2);
+      groups([&](int g) {
+        const cplx a1 = v[g | B1], a2 = v[g | B2];
+        v[g | B1] = pure ? a2 : c[0] * a2;
+        v[g | B2] = pure ? a1 : c[1] * a1;
+      });
+    } break;
+    case kSwXRot: {
+      const int X = op.aux & kAuxXMask, D = 1 << __builtin_popcount(V);
+      const cplx f = (op.aux & kAuxImag) ? cplx(0, 1) : cplx(1, 0);
+      groups([&](int g) {
+        cplx a[16], out[16];
+        for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
+        for (int r = 0; r < D; ++r) out[r] = c[r].real() * a[r] + f * c[r].imag() * a[r ^ X];
+        for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
+      });
+    } break;
+    default: {
+      const int K = __builtin_popcount(V), D = 1 << K;
+      groups([&](int g) {
+        cplx a[16], out[16];
+        for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
+        for (int r = 0; r < D; ++r) {
+          cplx s = c[r * D] * a[0];
+          for (int x = 1; x < D; ++x) s += c[r * D + x] * a[x];
+          out[r] = s;
+        }
+        for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
+      });
+    } break;
+  }
+}
+
+// <lambda| K |phi> over one thread's NA amplitudes (the kernel's inner ops).
+cplx inner_sweep_op(const SweepOp &op, const cplx *c, const cplx *phi, const cplx *lam, int NA,
+                    uint64_t gbase, uint32_t jb) {
+  cplx acc(0, 0);
+  const int V = op.vmask;
+  if (op.kind == kSwInnerDiag) {
+    for (int ri = 0; ri < NA; ++ri) acc += std::conj(lam[ri]) * c[diag_index(op, gbase, jb, ri)] * phi[ri];
+    return acc;
+  }
+  auto dep = [&](int x) {
+    int r = 0, b = 0;
+    for (int pp = 0; pp < 4; ++pp)
+      if (V & (1 << pp)) {
+        if (x & (1 << b)) r |= 1 << pp;
+        ++b;
+      }
+    return r;
+  };
+  const int D = 1 << __builtin_popcount(V);
+  for (int g = 0; g < NA; ++g) {
+    if (g & V) continue;
+    for (int r = 0; r < D; ++r) {
+      cplx s(0, 0);
+      for (int x = 0; x < D; ++x) s += c[r * D + x] * phi[g | dep(x)];
+      acc += std::conj(lam[g | dep(r)]) * s;
+    }
+  }
+  return acc;
+}
+
+// Sweeps one state (lam == nullptr) or two states with inner products
+// accumulated into ip[global slot] (the adjoint kernel), with NA = 2^reg_bits
+// register amplitudes per thread.
+void emulate_sweep_n(cplx *psi, cplx *lam, const PlannedSweep &ps, int reg_bits,
+                     std::vector<cplx> *ip) {
   const SweepHeader &h = ps.h;
-  const uint32_t m = h.m, l = h.l, nthr = 1u << (m - kRegBits);
+  const int NA = 1 << reg_bits;
+  const uint32_t m = h.m, l = h.l, nthr = 1u << (m - reg_bits);
   std::vector<uint64_t> hitab(size_t(1) << (m - l));
   for (uint32_t c = 0; c < hitab.size(); ++c) {
     uint64_t a = 0;
@@ -33,114 +156,53 @@ void emulate_sweep(cplx *psi, const PlannedSweep &ps) {
   auto addr = [&](uint64_t gbase, uint32_t j) {
     return gbase | hitab[j >> l] | (j & ((1u << l) - 1));
   };
-  std::vector<cplx> tile(size_t(1) << m);
+  std::vector<cplx> tile(size_t(1) << m), ltile(size_t(1) << m);
   for (uint64_t t = 0; t < h.num_tiles; ++t) {
     uint64_t gbase = t << l;
     for (uint32_t i = 0; i < m - l; ++i) gbase = insert_zero(gbase, h.hi[i]);
-    for (uint32_t j = 0; j < (1u << m); ++j) tile[j] = psi[addr(gbase, j)];
+    for (uint32_t j = 0; j < (1u << m); ++j) {
+      tile[j] = psi[addr(gbase, j)];
+      if (lam) ltile[j] = lam[addr(gbase, j)];
+    }
     for (uint32_t p = 0; p < h.nphases; ++p) {
       const SweepPhase &ph = ps.ph[p];
       for (uint32_t tid = 0; tid < nthr; ++tid) {
         uint32_t jb = tid;
-        for (int b = 0; b < kRegBits; ++b) jb = uint32_t(insert_zero(jb, ph.reg[b]));
-        cplx v[kRegAmps];
-        uint32_t jj[kRegAmps];
-        for (int ri = 0; ri < kRegAmps; ++ri) {
+        for (int b = 0; b < reg_bits; ++b) jb = uint32_t(insert_zero(jb, ph.reg[b]));
+        cplx v[16], w[16];
+        uint32_t jj[16];
+        for (int ri = 0; ri < NA; ++ri) {
           uint32_t j = jb;
-          for (int b = 0; b < kRegBits; ++b)
+          for (int b = 0; b < reg_bits; ++b)
             if ((ri >> b) & 1) j |= 1u << ph.reg[b];
           jj[ri] = j;
           v[ri] = tile[j];
+          if (lam) w[ri] = ltile[j];
         }
         for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
           const SweepOp &op = ps.op[o];
           const cplx *c = ps.coef.data() + op.coef;
-          if ((gbase & op.gmask) != op.gval || (jb & op.lmask) != op.lval) continue;
-          const int V = op.vmask;
-          auto dep = [&](int x) {
-            int r = 0, b = 0;
-            for (int pp = 0; pp < 4; ++pp)
-              if (V & (1 << pp)) {
-                if (x & (1 << b)) r |= 1 << pp;
-                ++b;
-              }
-            return r;
-          };
-          auto ext = [&](int x) {
-            int r = 0, b = 0;
-            for (int pp = 0; pp < 4; ++pp)
-              if (V & (1 << pp)) {
-                if (x & (1 << pp)) r |= 1 << b;
-                ++b;
-              }
-            return r;
-          };
-          auto groups = [&](auto f) {
-            for (int g = 0; g < kRegAmps; ++g)
-              if (!(g & V) && ((g & op.rmask) == op.rval)) f(g);
-          };
-          const bool pure = op.aux & kAuxPure;
-          switch (op.kind) {
-            case kSwPhase:
-              for (int ri = 0; ri < kRegAmps; ++ri)
-                if ((ri & op.rmask) == op.rval) v[ri] = pure ? -v[ri] : c[0] * v[ri];
-              break;
-            case kSwDiag: {
-              uint32_t base = 0;
-              for (int t = 0; t < op.ndt; ++t) {
-                const uint32_t bit = op.dsrc[t] == kSrcGlobal ? uint32_t(gbase >> op.dpos[t]) & 1u
-                                                              : (jb >> op.dpos[t]) & 1u;
-                base = (base << 1) | bit;
-              }
-              const int nreg = __builtin_popcount(V);
-              for (int ri = 0; ri < kRegAmps; ++ri) v[ri] = c[(base << nreg) | ext(ri)] * v[ri];
-            } break;
-            case kSwAnti1:
-              groups([&](int g) {
-                const cplx a0 = v[g], a1 = v[g | V];
-                v[g] = pure ? a1 : c[0] * a1;
-                v[g | V] = pure ? a0 : c[1] * a0;
-              });
-              break;
-            case kSwSwap2: {
-              const int B1 = dep(1), B2 = dep(2);
-              groups([&](int g) {
-                const cplx a1 = v[g | B1], a2 = v[g | B2];
-                v[g | B1] = pure ? a2 : c[0] * a2;
-                v[g | B2] = pure ? a1 : c[1] * a1;
-              });
-            } break;
-            case kSwXRot: {
-              const int X = op.aux & kAuxXMask, D = 1 << __builtin_popcount(V);
-              const cplx f = (op.aux & kAuxImag) ? cplx(0, 1) : cplx(1, 0);
-              groups([&](int g) {
-                cplx a[16], out[16];
-                for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
-                for (int r = 0; r < D; ++r) out[r] = c[r].real() * a[r] + f * c[r].imag() * a[r ^ X];
-                for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
-              });
-            } break;
-            default: {
-              const int K = __builtin_popcount(V), D = 1 << K;
-              groups([&](int g) {
-                cplx a[16], out[16];
-                for (int x = 0; x < D; ++x) a[x] = v[g | dep(x)];
-                for (int r = 0; r < D; ++r) {
-                  cplx s = c[r * D] * a[0];
-                  for (int x = 1; x < D; ++x) s += c[r * D + x] * a[x];
-                  out[r] = s;
-                }
-                for (int r = 0; r < D; ++r) v[g | dep(r)] = out[r];
-              });
-            } break;
+          if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
+            (*ip)[ps.inner_global[op.slot]] += inner_sweep_op(op, c, v, w, NA, gbase, jb);
+          } else {
+            apply_sweep_op(op, c, v, NA, gbase, jb);
+            if (lam) apply_sweep_op(op, c, w, NA, gbase, jb);
           }
         }
-        for (int ri = 0; ri < kRegAmps; ++ri) tile[jj[ri]] = v[ri];
+        for (int ri = 0; ri < NA; ++ri) {
+          tile[jj[ri]] = v[ri];
+          if (lam) ltile[jj[ri]] = w[ri];
+        }
       }
     }
-    for (uint32_t j = 0; j < (1u << m); ++j) psi[addr(gbase, j)] = tile[j];
+    for (uint32_t j = 0; j < (1u << m); ++j) {
+      psi[addr(gbase, j)] = tile[j];
+      if (lam) lam[addr(gbase, j)] = ltile[j];
+    }
   }
 }
+
+void emulate_sweep(cplx *psi, const PlannedSweep &ps) { emulate_sweep_n(psi, nullptr, ps, kRegBits, nullptr); }
 
 void emulate_gate(cplx *psi, uint32_t n, const HostOp &op0) {
   HostOp op = op0;
@@ -267,6 +329,68 @@ int emu_plan_stats(int n, int nops, const int *k, const int *qoff, const int *qu
       for (const auto &o : pl.sweep.op) out[2 + o.kind]++;
     }
     return 0;
+  } catch (const std::exception &) {
+    return -1;
+  }
+}
+}
+
+extern "C" {
+// Adjoint gradient on the host with the engine's reverse plan (3 register bits,
+// two-state sweeps).  Returns the number of reverse sweeps, -1 on error.
+int emu_adjoint(int n, const sq_circuit_op *ops, uint32_t nops, const char *paulis,
+                const double *weights, uint32_t nterms, uint32_t nparams, int tile_bits,
+                double *energy, double *grad) {
+  try {
+    AdjointPlan ap;
+    build_adjoint(ops, nops, uint32_t(n), ap);
+    const size_t N = size_t(1) << n;
+    std::vector<cplx> psi(N, cplx(0, 0)), lam(N, cplx(0, 0));
+    psi[0] = 1.0;
+    for (const auto &op : ap.forward) emulate_gate(psi.data(), uint32_t(n), op);
+    // lambda = H psi
+    for (uint32_t t = 0; t < nterms; ++t) {
+      for (size_t i = 0; i < N; ++i) {
+        size_t j = i;
+        cplx ph(1, 0);
+        for (int q = 0; q < n; ++q) {
+          const size_t bit = size_t(1) << (n - 1 - q);
+          const int b = (i & bit) ? 1 : 0;
+          switch (paulis[size_t(t) * n + q]) {
+            case 'X': j ^= bit; break;
+            case 'Y': j ^= bit; ph *= b ? cplx(0, 1) : cplx(0, -1); break;
+            case 'Z': if (b) ph = -ph; break;
+            default: break;
+          }
+        }
+        lam[i] += weights[t] * ph * psi[j];
+      }
+    }
+    double e = 0;
+    for (size_t i = 0; i < N; ++i) e += (std::conj(psi[i]) * lam[i]).real();
+    *energy = e;
+    PlanOptions opt;
+    opt.tile_bits = uint32_t(tile_bits);
+    opt.reg_bits = 3;
+    opt.max_dense_k = 3;
+    auto plan = plan_sweeps(ap.reverse, uint32_t(n), opt);
+    std::vector<cplx> ip(ap.occurrences.size(), cplx(0, 0));
+    int sweeps = 0;
+    for (const auto &pl : plan) {
+      if (pl.is_sweep) {
+        emulate_sweep_n(psi.data(), lam.data(), pl.sweep, 3, &ip);
+        ++sweeps;
+      } else {
+        emulate_gate(psi.data(), uint32_t(n), pl.gate);
+        emulate_gate(lam.data(), uint32_t(n), pl.gate);
+      }
+    }
+    for (uint32_t p = 0; p < nparams; ++p) grad[p] = 0;
+    for (size_t s = 0; s < ip.size(); ++s) {
+      const auto &oc = ap.occurrences[s];
+      if (oc.first >= 0 && uint32_t(oc.first) < nparams) grad[oc.first] += 2.0 * ip[s].real() * oc.second;
+    }
+    return sweeps;
   } catch (const std::exception &) {
     return -1;
   }

@@ -58,3 +58,28 @@ def test_no_gpu_state_create_fails_cleanly():
     with pytest.raises(capi.SqError) as e:
         capi.State(4)
     assert e.value.status in (capi.SQ_ERR_CUDA, capi.SQ_ERR_OOM)
+
+
+PARAM_GATES = ["PhaseShift", "CPhaseShift", "CPhaseShift00", "CPhaseShift01", "CPhaseShift10",
+               "RotX", "RotY", "RotZ", "PSwap", "XY", "XX", "YY", "ZZ", "U", "GPhase", "PRx"]
+
+
+@pytest.mark.parametrize("name", PARAM_GATES)
+def test_gate_derivatives_match_finite_differences(name):
+    rng = np.random.default_rng(11)
+    na = oracle.gate_num_angles(name)
+    for _ in range(3):
+        a = rng.uniform(-3, 3, size=na)
+        for p in range(na):
+            d = capi.gate_matrix_derivative(name, a, p)
+            h = 1e-5
+            ap, am = a.copy(), a.copy()
+            ap[p] += h
+            am[p] -= h
+            fd = (capi.gate_matrix(name, ap) - capi.gate_matrix(name, am)) / (2 * h)
+            assert np.abs(d - fd).max() < 1e-9, (name, p)
+
+
+def test_derivative_of_fixed_gate_is_an_error():
+    with pytest.raises(capi.SqError):
+        capi.gate_matrix_derivative("CX", (), 0)
