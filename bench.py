@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-batch", action="store_true")
     p.add_argument("--tile-bits", type=int, default=0, help="override the engine's tile size")
     return p.parse_args()
 
@@ -313,6 +314,11 @@ def _run_ours(args, rank, world, local):
             out["adjoint"] = adjoint_metric(args.precision)
         except Exception as e:
             out["adjoint"] = {"note": f"adjoint failed: {e}"}
+    if world == 1 and rank == 0 and not args.no_batch:
+        try:
+            out["batch"] = batch_metric(args.precision)
+        except Exception as e:
+            out["batch"] = {"note": f"batch failed: {e}"}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(n, ops)
@@ -380,6 +386,45 @@ def adjoint_metric(precision: str):
             "speedup_vs_param_shift": round(t_eval * evals / t_adj, 1),
             "timing": "host wall clock around synchronous calls; parameter shift extrapolated "
                       f"from {done} evaluations"}
+
+
+def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED):
+    """Batched VQE energies: ncirc hardware-efficient ansatz circuits with
+    qubit counts uniform in 8..20 (6 layers of RY, RZ on every qubit and a CX
+    ladder, angles uniform in [0, 2pi)), one 64-term random Pauli-sum
+    Hamiltonian per qubit count, one energy per circuit, one launch."""
+    from snuqs_b200 import capi, circuits
+
+    dtype = capi.SQ_C128 if precision == "complex128" else capi.SQ_C64
+    rng = np.random.default_rng(seed)
+    b = capi.Batch(dtype)
+    hams = {n: b.add_hamiltonian(n, circuits.random_pauli_hamiltonian(n, 64, seed=seed + n))
+            for n in range(8, 21)}
+    sizes = rng.integers(8, 21, size=ncirc)
+    t0 = time.perf_counter()
+    for n in sizes:
+        n = int(n)
+        b.add_circuit(n, circuits.vqe_ansatz(n, rng.uniform(0, 2 * np.pi, 12 * n)), hams[n])
+    t_add = time.perf_counter() - t0
+    b.run()  # plans, allocates, captures the graph
+    reps = 3
+    t0 = time.perf_counter()
+    kms = []
+    for _ in range(reps):
+        b.run()
+        kms.append(b.last_timing()[0])
+    t_run = (time.perf_counter() - t0) / reps
+    ctas = b.last_timing()[1]
+    b.close()
+    amps = int(sum(1 << int(n) for n in sizes))
+    return {"workload": f"vqe_batch_{ncirc}x_8to20q_{precision}", "circuits": ncirc,
+            "total_amplitudes": amps, "kernel_ms": round(float(np.median(kms)), 3),
+            "run_ms": round(t_run * 1e3, 3),
+            "energies_per_s": round(ncirc / t_run, 1),
+            "energies_per_s_kernel": round(ncirc / (float(np.median(kms)) * 1e-3), 1),
+            "ctas": ctas, "add_circuits_s": round(t_add, 3),
+            "timing": "run_ms = host wall clock of sq_batch_run (planning + one graph launch); "
+                      "kernel_ms = CUDA events around the single batch kernel"}
 
 
 def e2e(n, ops, args, amp):

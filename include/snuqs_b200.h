@@ -229,6 +229,39 @@ int sq_expect_pauli_noalloc(const void *state, uint32_t num_qubits, int dtype,
                             const char *paulis, const double *weights,
                             uint32_t n_terms, double *out_device, void *stream);
 
+/* ---- batched circuits ----------------------------------------------------
+ * No counterpart in the reference (one circuit per run: simulator.py:152-155).
+ * Many small circuits (4..30 qubits each, uneven) and their Pauli-sum
+ * energies in ONE persistent kernel launch: CTAs take circuits from an
+ * atomic work queue, largest first; a circuit that fits one shared-memory
+ * tile (<= 11 qubits complex128, <= 12 complex64) never touches HBM. */
+typedef struct sq_batch sq_batch;
+typedef enum {
+  SQ_BOPT_KEEP_STATES = 0  /* 1: keep every final state for sq_batch_state */
+} sq_batch_option;
+int sq_batch_create(int dtype, sq_batch **out);
+int sq_batch_destroy(sq_batch *b);
+int sq_batch_set_option(sq_batch *b, int option, int64_t value);
+/* Pauli-sum observable on num_qubits qubits (paulis as in sq_expect_pauli). */
+int sq_batch_add_hamiltonian(sq_batch *b, uint32_t num_qubits, const char *paulis,
+                             const double *weights, uint32_t n_terms, uint32_t *ham_id);
+/* One circuit (gates as sq_circuit_op; param/scale are ignored) measured with
+ * Hamiltonian ham_id (same qubit count). */
+int sq_batch_add_circuit(sq_batch *b, uint32_t num_qubits, const sq_circuit_op *ops,
+                         uint32_t nops, uint32_t ham_id, uint32_t *circuit_id);
+/* Replace the angles of circuit `circuit` (same gates; nangles per op as
+ * given at add time, concatenated). */
+int sq_batch_set_angles(sq_batch *b, uint32_t circuit, const double *angles, uint32_t count);
+int sq_batch_num_circuits(const sq_batch *b, uint32_t *count);
+/* Plan, upload and run every circuit in one launch; energies (host,
+ * one double per circuit, in circuit-id order).  Synchronous. */
+int sq_batch_run(sq_batch *b, double *energies, void *stream);
+/* Final state of a circuit (needs SQ_BOPT_KEEP_STATES before sq_batch_run);
+ * host_dst receives 2^n amplitudes of the batch's precision. */
+int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream);
+/* Device time of the last sq_batch_run's kernel (ms) and its CTA count. */
+int sq_batch_last_timing(const sq_batch *b, double *kernel_ms, uint32_t *ctas);
+
 #ifdef __cplusplus
 }
 #endif

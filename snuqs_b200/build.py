@@ -24,7 +24,7 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-ENGINE_CU = ["engine.cu", "noalloc.cu"]
+ENGINE_CU = ["engine.cu", "noalloc.cu", "batch.cu"]
 ENGINE_CC = ["gates.cc", "planner.cc", "adjoint_plan.cc"]
 # Fused-sweep kernel instantiations: (precision, tile bits, CTAs per SM).
 # Tile sizes must match kTileBitsC128 / kTileBitsC64 in csrc/sq_plan.h; the
@@ -36,6 +36,8 @@ SWEEP_INSTANCES = [
 # Two-state adjoint kernels: (precision, tile bits); must match kAdjTileBits*.
 ADJOINT_INSTANCES = [("double", 4), ("double", 7), ("double", 10),
                      ("float", 4), ("float", 7), ("float", 11)]
+# Batched-circuit kernels: (precision, tile bits); must match kBatchTileBits*.
+BATCH_INSTANCES = [("double", 11), ("float", 12)]
 LIB = os.path.join(HERE, "libsnuqs_b200.so")
 
 
@@ -99,6 +101,18 @@ def build(force: bool = False, verbose: bool = False) -> None:
             cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
                    f"-DSQ_REAL={real}", f"-DSQ_M={m}",
                    "-Xptxas", "-warn-spills", "-c", adj_src, "-o", obj]
+            jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                               stderr=subprocess.STDOUT, text=True)))
+        objs.append(obj)
+    bat_src = os.path.join(CSRC, "batch_inst.cu")
+    bat_deps = inst_deps + [bat_src, os.path.join(CSRC, "batch_kernels.cuh"),
+                            os.path.join(CSRC, "reduce_kernels.cuh")]
+    for real, m in BATCH_INSTANCES:
+        obj = os.path.join(BUILD, f"batch_{real}_{m}.o")
+        if force or _stale(obj, bat_deps):
+            cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
+                   f"-DSQ_REAL={real}", f"-DSQ_M={m}",
+                   "-Xptxas", "-warn-spills", "-c", bat_src, "-o", obj]
             jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
                                                stderr=subprocess.STDOUT, text=True)))
         objs.append(obj)

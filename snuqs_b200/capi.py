@@ -80,6 +80,16 @@ SIGNATURES = {
     "sq_norm2": (_I, [_P, _PD, _P]),
     "sq_expect_pauli_noalloc": (_I, [_P, _U32, _I, ctypes.c_char_p, _PD, _U32, _P, _P]),
     "sq_adjoint_gradient": (_I, [_P, _P, _P, _U32, ctypes.c_char_p, _PD, _U32, _U32, _PD, _PD, _P]),
+    "sq_batch_create": (_I, [_I, ctypes.POINTER(_P)]),
+    "sq_batch_destroy": (_I, [_P]),
+    "sq_batch_set_option": (_I, [_P, _I, ctypes.c_int64]),
+    "sq_batch_add_hamiltonian": (_I, [_P, _U32, ctypes.c_char_p, _PD, _U32, _PU32]),
+    "sq_batch_add_circuit": (_I, [_P, _U32, _P, _U32, _U32, _PU32]),
+    "sq_batch_set_angles": (_I, [_P, _U32, _PD, _U32]),
+    "sq_batch_num_circuits": (_I, [_P, _PU32]),
+    "sq_batch_run": (_I, [_P, _PD, _P]),
+    "sq_batch_state": (_I, [_P, _U32, _P, _P]),
+    "sq_batch_last_timing": (_I, [_P, _PD, _PU32]),
 }
 
 
@@ -122,6 +132,69 @@ def circuit_ops(ops):
             for j, sc in enumerate(op[4]):
                 o.scale[j] = sc
     return arr, keep
+
+
+SQ_BOPT_KEEP_STATES = 0
+
+
+class Batch:
+    """Many small circuits and their Pauli-sum energies in one launch
+    (sq_batch_*)."""
+
+    def __init__(self, dtype: int = SQ_C128, keep_states: bool = False):
+        h = _P()
+        check(lib().sq_batch_create(dtype, ctypes.byref(h)))
+        self.h, self.dtype = h, dtype
+        self._hams = {}
+        self._n = []
+        if keep_states:
+            check(lib().sq_batch_set_option(h, SQ_BOPT_KEEP_STATES, 1))
+
+    def close(self):
+        if self.h:
+            check(lib().sq_batch_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_hamiltonian(self, n: int, terms) -> int:
+        flat = "".join(p for _, p in terms).encode()
+        w = np.ascontiguousarray([x for x, _ in terms] or [0.0], dtype=np.float64)
+        hid = _U32(0)
+        check(lib().sq_batch_add_hamiltonian(self.h, n, flat, _dp(w), len(terms), ctypes.byref(hid)))
+        return hid.value
+
+    def add_circuit(self, n: int, ops, ham: int) -> int:
+        arr, keep = circuit_ops(ops)
+        cid = _U32(0)
+        check(lib().sq_batch_add_circuit(self.h, n, ctypes.cast(arr, _P), len(ops), ham,
+                                         ctypes.byref(cid)))
+        self._n.append(n)
+        return cid.value
+
+    def set_angles(self, circuit: int, angles) -> None:
+        a = np.ascontiguousarray(angles, dtype=np.float64)
+        check(lib().sq_batch_set_angles(self.h, circuit, _dp(a), a.size))
+
+    def run(self, stream=None) -> np.ndarray:
+        out = np.zeros(max(1, len(self._n)), dtype=np.float64)
+        check(lib().sq_batch_run(self.h, _dp(out), stream))
+        return out[: len(self._n)]
+
+    def state(self, circuit: int) -> np.ndarray:
+        a = np.empty(1 << self._n[circuit],
+                     dtype=np.complex64 if self.dtype == SQ_C64 else np.complex128)
+        check(lib().sq_batch_state(self.h, circuit, a.ctypes.data_as(_P), None))
+        return a
+
+    def last_timing(self):
+        ms, ctas = _D(0), _U32(0)
+        check(lib().sq_batch_last_timing(self.h, ctypes.byref(ms), ctypes.byref(ctas)))
+        return ms.value, ctas.value
 
 
 class SqError(RuntimeError):

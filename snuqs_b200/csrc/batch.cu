@@ -1,0 +1,496 @@
+// Batched circuits: host side of sq_batch_* (include/snuqs_b200.h).
+//
+// sq_batch_run plans every circuit (in parallel on the host), packs the plans
+// into one pinned buffer, and replays a CUDA graph that uploads the plans and
+// the circuit table, resets the work counter, runs the persistent
+// batch_kernel once and downloads the energies.  The graph is re-captured
+// only when a buffer size changes, so a VQE loop that only changes angles
+// replays the same graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/snuqs_b200.h"
+#include "batch_kernels.cuh"
+#include "host_ops.h"
+#include "sweep_registry.h"
+
+int sq_detail_fail(int code, const char *msg);
+
+using sq::cplx;
+
+namespace {
+
+int fail(int code, const std::string &m) { return sq_detail_fail(code, m.c_str()); }
+
+#define SQB_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return fail(e_ == cudaErrorMemoryAllocation ? SQ_ERR_OOM : SQ_ERR_CUDA,                   \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+  } while (0)
+
+struct Circ {
+  uint32_t n = 0, ham = 0;
+  std::vector<sq_circuit_op> ops;
+  std::vector<std::vector<cplx>> fixed;  // copies of fixed matrices
+};
+
+// Device buffer that grows.
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return SQ_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    SQB_CUDA(cudaMalloc(&p, bytes));
+    cap = bytes;
+    return SQ_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct HostBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return SQ_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    SQB_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocDefault));
+    cap = bytes;
+    return SQ_OK;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+}  // namespace
+
+struct sq_batch {
+  int dtype = SQ_C128;
+  int device = 0;
+  int keep = 0;
+  std::vector<sq::PauliParams> hams;
+  std::vector<uint32_t> ham_n;
+  std::vector<Circ> circs;
+  DevBuf d_pool, d_plans, d_table, d_hams, d_energy, d_counter;
+  HostBuf h_plans, h_table, h_energy;
+  size_t hams_uploaded = 0;
+  std::vector<uint64_t> state_off;  // per circuit id; ~0 when not kept
+  std::vector<uint32_t> order;      // sorted position -> circuit id
+  cudaGraphExec_t graph = nullptr;
+  size_t graph_plan_bytes = 0, graph_ncirc = 0;
+  void *graph_stream = nullptr;
+  uint32_t graph_grid = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  uint32_t last_ctas = 0;
+};
+
+namespace {
+
+// Pauli-string sum -> grouped expectation parameters (as sq_expect_pauli).
+int build_pauli(uint32_t n, const char *paulis, const double *w, uint32_t nt, sq::PauliParams &P) {
+  if (nt > uint32_t(sq::kMaxTerms)) return fail(SQ_ERR_UNSUPPORTED, "batch: > 1024 Pauli terms");
+  std::vector<uint64_t> xm(nt), zym(nt);
+  std::vector<int> ny(nt);
+  for (uint32_t t = 0; t < nt; ++t)
+    for (uint32_t q = 0; q < n; ++q) {
+      const uint64_t bit = uint64_t(1) << (n - 1 - q);
+      switch (paulis[size_t(t) * n + q]) {
+        case 'I': case 'i': break;
+        case 'X': case 'x': xm[t] |= bit; break;
+        case 'Y': case 'y': xm[t] |= bit; zym[t] |= bit; ny[t]++; break;
+        case 'Z': case 'z': zym[t] |= bit; break;
+        default: return fail(SQ_ERR_INVALID, "batch: bad Pauli character");
+      }
+    }
+  std::vector<uint32_t> idx(nt);
+  for (uint32_t i = 0; i < nt; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+    if (xm[a] != xm[b]) return xm[a] < xm[b];
+    return (ny[a] & 1) < (ny[b] & 1);
+  });
+  std::memset(&P, 0, sizeof(P));
+  P.n = n;
+  uint32_t k = 0;
+  for (uint32_t pos = 0; pos < nt;) {
+    uint32_t end = pos;
+    while (end < nt && xm[idx[end]] == xm[idx[pos]] && (ny[idx[end]] & 1) == (ny[idx[pos]] & 1)) ++end;
+    if (P.ngroups >= uint32_t(sq::kMaxGroups))
+      return fail(SQ_ERR_UNSUPPORTED, "batch: > 256 Pauli groups");
+    sq::PauliGroup &g = P.g[P.ngroups++];
+    g.x = xm[idx[pos]];
+    g.odd = ny[idx[pos]] & 1;
+    g.t0 = k;
+    for (uint32_t e = pos; e < end; ++e) {
+      const uint32_t t = idx[e];
+      P.zy[k] = zym[t];
+      P.f[k] = w[t] * (((ny[t] / 2) & 1) ? -1.0 : 1.0);
+      ++k;
+    }
+    g.t1 = k;
+    pos = end;
+  }
+  return SQ_OK;
+}
+
+template <typename Real>
+void pack_sweep(const sq::PlannedSweep &ps, std::vector<unsigned char> &out) {
+  using C2 = typename sq::Vec2<Real>::T;
+  sq::PackedSweep hdr;
+  std::memset(&hdr, 0, sizeof(hdr));
+  hdr.h = ps.h;
+  hdr.nops = uint32_t(ps.op.size());
+  hdr.phase_off = uint32_t(align16(sizeof(hdr)));
+  hdr.op_off = uint32_t(align16(hdr.phase_off + ps.ph.size() * sizeof(sq::SweepPhase)));
+  hdr.coef_off = uint32_t(align16(hdr.op_off + ps.op.size() * sizeof(sq::SweepOp)));
+  hdr.bytes = uint32_t(align16(hdr.coef_off + ps.coef.size() * sizeof(C2)));
+  const size_t base = out.size();
+  out.resize(base + hdr.bytes, 0);
+  unsigned char *r = out.data() + base;
+  std::memcpy(r, &hdr, sizeof(hdr));
+  std::memcpy(r + hdr.phase_off, ps.ph.data(), ps.ph.size() * sizeof(sq::SweepPhase));
+  std::memcpy(r + hdr.op_off, ps.op.data(), ps.op.size() * sizeof(sq::SweepOp));
+  C2 *c = reinterpret_cast<C2 *>(r + hdr.coef_off);
+  for (size_t i = 0; i < ps.coef.size(); ++i) {
+    c[i].x = Real(ps.coef[i].real());
+    c[i].y = Real(ps.coef[i].imag());
+  }
+}
+
+// Plans one circuit into packed sweeps; returns the sweep count or < 0.
+template <typename Real>
+int plan_circuit(const Circ &c, uint32_t m, std::vector<unsigned char> &out, std::string &err) {
+  try {
+    std::vector<sq::HostOp> ops;
+    for (const auto &op : c.ops) {
+      std::vector<cplx> mat;
+      if (op.gate < 0) {
+        const size_t d = size_t(1) << op.k;
+        mat.resize(d * d);
+        std::memcpy(mat.data(), op.matrix, d * d * sizeof(cplx));
+      } else if (sq::gate_matrix(op.gate, op.angles, op.nangles, mat) < 0) {
+        err = "batch: bad gate or angle count";
+        return -1;
+      }
+      std::vector<int> tb;
+      for (uint32_t j = 0; j < op.k; ++j) tb.push_back(int(c.n - 1 - op.qubits[j]));
+      sq::HostOp h;
+      if (sq::analyse_op(mat, tb, 0, 0, h)) ops.push_back(h);
+    }
+    sq::PlanOptions opt;
+    opt.tile_bits = m;
+    opt.max_dense_k = sizeof(Real) == 4 ? 4 : 3;
+    const auto plan = sq::plan_sweeps(ops, c.n, opt);
+    int sweeps = 0;
+    for (const auto &pl : plan) {
+      if (!pl.is_sweep) {
+        err = "batch: a gate wider than a sweep's registers (use the single-state API)";
+        return -1;
+      }
+      pack_sweep<Real>(pl.sweep, out);
+      ++sweeps;
+    }
+    return sweeps;
+  } catch (const std::exception &e) {
+    err = std::string("batch planner: ") + e.what();
+    return -1;
+  }
+}
+
+template <typename Real>
+int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
+  using C2 = typename sq::Vec2<Real>::T;
+  const uint32_t M = sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128;
+  const size_t nc = b->circs.size();
+  if (nc == 0) return SQ_OK;
+  // Plan all circuits in parallel.
+  std::vector<std::vector<unsigned char>> packed(nc);
+  std::vector<int> nsweeps(nc, 0);
+  std::vector<std::string> errs(nc);
+  std::atomic<size_t> next{0};
+  const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nth; ++t)
+    pool.emplace_back([&]() {
+      for (size_t i = next++; i < nc; i = next++)
+        nsweeps[i] = plan_circuit<Real>(b->circs[i], M, packed[i], errs[i]);
+    });
+  for (auto &th : pool) th.join();
+  for (size_t i = 0; i < nc; ++i)
+    if (nsweeps[i] < 0) return fail(SQ_ERR_UNSUPPORTED, errs[i]);
+  // Largest circuits first (dynamic work queue).
+  b->order.resize(nc);
+  for (size_t i = 0; i < nc; ++i) b->order[i] = uint32_t(i);
+  std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) {
+    const uint64_t cx = (uint64_t(1) << b->circs[x].n) * (uint64_t(nsweeps[x]) + 1);
+    const uint64_t cy = (uint64_t(1) << b->circs[y].n) * (uint64_t(nsweeps[y]) + 1);
+    return cx > cy;
+  });
+  // State pool: circuits that do not fit one tile, or whose state is kept.
+  b->state_off.assign(nc, ~uint64_t(0));
+  uint64_t pool_amps = 0;
+  for (uint32_t id : b->order) {
+    const Circ &c = b->circs[id];
+    if (c.n > M || b->keep) {
+      b->state_off[id] = pool_amps;
+      pool_amps += uint64_t(1) << c.n;
+    }
+  }
+  size_t plan_bytes = 0;
+  for (size_t i = 0; i < nc; ++i) plan_bytes += packed[i].size();
+  SQB_CUDA(cudaSetDevice(b->device));
+  if (int s = b->d_pool.ensure(std::max<uint64_t>(pool_amps, 1) * sizeof(C2))) return s;
+  if (int s = b->d_plans.ensure(plan_bytes + 16)) return s;
+  if (int s = b->h_plans.ensure(plan_bytes + 16)) return s;
+  if (int s = b->d_table.ensure(nc * sizeof(sq::BatchCircuit))) return s;
+  if (int s = b->h_table.ensure(nc * sizeof(sq::BatchCircuit))) return s;
+  if (int s = b->d_energy.ensure(nc * sizeof(double))) return s;
+  if (int s = b->h_energy.ensure(nc * sizeof(double))) return s;
+  if (int s = b->d_counter.ensure(sizeof(unsigned))) return s;
+  if (b->hams_uploaded != b->hams.size()) {
+    if (int s = b->d_hams.ensure(b->hams.size() * sizeof(sq::PauliParams))) return s;
+    SQB_CUDA(cudaMemcpy(b->d_hams.p, b->hams.data(), b->hams.size() * sizeof(sq::PauliParams),
+                        cudaMemcpyHostToDevice));
+    b->hams_uploaded = b->hams.size();
+  }
+  // Pinned staging: packed plans and the sorted table.
+  auto *tab = static_cast<sq::BatchCircuit *>(b->h_table.p);
+  unsigned char *hp = static_cast<unsigned char *>(b->h_plans.p);
+  size_t off = 0;
+  for (size_t pos = 0; pos < nc; ++pos) {
+    const uint32_t id = b->order[pos];
+    const Circ &c = b->circs[id];
+    std::memcpy(hp + off, packed[id].data(), packed[id].size());
+    sq::BatchCircuit &t = tab[pos];
+    t.n = c.n;
+    t.nsweeps = uint32_t(nsweeps[id]);
+    t.ham = c.ham;
+    t.keep = b->keep ? 1u : 0u;
+    t.state_off = b->state_off[id] == ~uint64_t(0) ? 0 : b->state_off[id];
+    t.plan_off = off;
+    off += packed[id].size();
+  }
+  // Kernel configuration.
+  const void *fn = sizeof(Real) == 4 ? SQ_BATCH_PTR_NAME(float, 12)() : SQ_BATCH_PTR_NAME(double, 11)();
+  const uint32_t L = uint32_t(sq::sweep_low_bits(int(M)));
+  const size_t smem = (size_t(1) << M) * sizeof(C2) + size_t(sq::kMaxCoef) * sizeof(C2) +
+                      (size_t(1) << (M - L)) * sizeof(uint64_t);
+  SQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const int threads = 1 << (M - sq::kRegBits);
+  int per_sm = 0, sms = 0;
+  SQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  SQB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  const uint32_t grid = uint32_t(std::max<uint64_t>(
+      1, std::min<uint64_t>(nc, uint64_t(std::max(per_sm, 1)) * uint64_t(sms))));
+  if (!b->ev0) {
+    SQB_CUDA(cudaEventCreate(&b->ev0));
+    SQB_CUDA(cudaEventCreate(&b->ev1));
+  }
+  // (Re)capture the graph when sizes or the stream changed.
+  if (!b->graph || b->graph_plan_bytes != plan_bytes || b->graph_ncirc != nc ||
+      b->graph_stream != st || b->graph_grid != grid) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    cudaStream_t cs;
+    SQB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    sq::BatchParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.circuits = static_cast<const sq::BatchCircuit *>(b->d_table.p);
+    P.plans = static_cast<const unsigned char *>(b->d_plans.p);
+    P.hams = static_cast<const sq::PauliParams *>(b->d_hams.p);
+    P.ncircuits = uint32_t(nc);
+    P.counter = static_cast<unsigned *>(b->d_counter.p);
+    P.energies = static_cast<double *>(b->d_energy.p);
+    C2 *poolp = static_cast<C2 *>(b->d_pool.p);
+    void *args[] = {&poolp, &P};
+    cudaGraph_t g;
+    auto capture = [&]() -> int {
+      SQB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      cudaMemcpyAsync(b->d_plans.p, b->h_plans.p, plan_bytes, cudaMemcpyHostToDevice, cs);
+      cudaMemcpyAsync(b->d_table.p, b->h_table.p, nc * sizeof(sq::BatchCircuit),
+                      cudaMemcpyHostToDevice, cs);
+      cudaMemsetAsync(b->d_counter.p, 0, sizeof(unsigned), cs);
+      // External event nodes, so the kernel's device time can be read back.
+      cudaEventRecordWithFlags(b->ev0, cs, cudaEventRecordExternal);
+      cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, cs);
+      cudaEventRecordWithFlags(b->ev1, cs, cudaEventRecordExternal);
+      cudaMemcpyAsync(b->h_energy.p, b->d_energy.p, nc * sizeof(double), cudaMemcpyDeviceToHost, cs);
+      SQB_CUDA(cudaStreamEndCapture(cs, &g));
+      return SQ_OK;
+    };
+    const int s1 = capture();
+    cudaStreamDestroy(cs);
+    if (s1 != SQ_OK) return s1;
+    const cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(SQ_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    b->graph_plan_bytes = plan_bytes;
+    b->graph_ncirc = nc;
+    b->graph_stream = st;
+    b->graph_grid = grid;
+  }
+  SQB_CUDA(cudaGraphLaunch(b->graph, st));
+  SQB_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  SQB_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  b->last_ms = ms;
+  b->last_ctas = grid;
+  const double *he = static_cast<const double *>(b->h_energy.p);
+  for (size_t pos = 0; pos < nc; ++pos) energies[b->order[pos]] = he[pos];
+  return SQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sq_batch_create(int dtype, sq_batch **out) {
+  if (!out) return fail(SQ_ERR_INVALID, "null pointer");
+  if (dtype != SQ_C128 && dtype != SQ_C64) return fail(SQ_ERR_INVALID, "bad dtype");
+  auto b = std::make_unique<sq_batch>();
+  b->dtype = dtype;
+  SQB_CUDA(cudaGetDevice(&b->device));
+  *out = b.release();
+  return SQ_OK;
+}
+
+int sq_batch_destroy(sq_batch *b) {
+  if (!b) return SQ_OK;
+  std::unique_ptr<sq_batch> holder(b);
+  cudaSetDevice(b->device);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  b->d_pool.release();
+  b->d_plans.release();
+  b->d_table.release();
+  b->d_hams.release();
+  b->d_energy.release();
+  b->d_counter.release();
+  b->h_plans.release();
+  b->h_table.release();
+  b->h_energy.release();
+  return SQ_OK;
+}
+
+int sq_batch_set_option(sq_batch *b, int option, int64_t value) {
+  if (!b) return fail(SQ_ERR_INVALID, "null batch");
+  if (option == SQ_BOPT_KEEP_STATES) {
+    b->keep = value != 0;
+    return SQ_OK;
+  }
+  return fail(SQ_ERR_INVALID, "unknown batch option");
+}
+
+int sq_batch_add_hamiltonian(sq_batch *b, uint32_t num_qubits, const char *paulis,
+                             const double *weights, uint32_t n_terms, uint32_t *ham_id) {
+  if (!b || !ham_id || (n_terms && (!paulis || !weights))) return fail(SQ_ERR_INVALID, "null pointer");
+  if (num_qubits < 4 || num_qubits > 30) return fail(SQ_ERR_UNSUPPORTED, "batch: 4..30 qubits");
+  sq::PauliParams P;
+  if (int s = build_pauli(num_qubits, paulis, weights, n_terms, P)) return s;
+  b->hams.push_back(P);
+  b->ham_n.push_back(num_qubits);
+  *ham_id = uint32_t(b->hams.size() - 1);
+  return SQ_OK;
+}
+
+int sq_batch_add_circuit(sq_batch *b, uint32_t num_qubits, const sq_circuit_op *ops, uint32_t nops,
+                         uint32_t ham_id, uint32_t *circuit_id) {
+  if (!b || !circuit_id || (nops && !ops)) return fail(SQ_ERR_INVALID, "null pointer");
+  if (ham_id >= b->hams.size() || b->ham_n[ham_id] != num_qubits)
+    return fail(SQ_ERR_INVALID, "batch: Hamiltonian id / qubit count mismatch");
+  Circ c;
+  c.n = num_qubits;
+  c.ham = ham_id;
+  c.ops.assign(ops, ops + nops);
+  for (auto &op : c.ops) {
+    if (op.k > 4) return fail(SQ_ERR_UNSUPPORTED, "batch: gates act on at most 4 qubits");
+    uint64_t seen = 0;
+    for (uint32_t j = 0; j < op.k; ++j) {
+      if (op.qubits[j] >= num_qubits || ((seen >> op.qubits[j]) & 1))
+        return fail(SQ_ERR_INVALID, "batch: bad or repeated qubit");
+      seen |= uint64_t(1) << op.qubits[j];
+    }
+    if (op.gate < 0) {
+      if (!op.matrix) return fail(SQ_ERR_INVALID, "batch: null matrix");
+      const size_t d = size_t(1) << op.k;
+      c.fixed.emplace_back(d * d);
+      std::memcpy(c.fixed.back().data(), op.matrix, d * d * sizeof(cplx));
+      op.matrix = reinterpret_cast<const double *>(c.fixed.back().data());
+    } else if (sq::gate_qubits(op.gate) != int(op.k)) {
+      return fail(SQ_ERR_INVALID, "batch: qubit count does not match the gate");
+    }
+  }
+  b->circs.push_back(std::move(c));
+  *circuit_id = uint32_t(b->circs.size() - 1);
+  return SQ_OK;
+}
+
+int sq_batch_set_angles(sq_batch *b, uint32_t circuit, const double *angles, uint32_t count) {
+  if (!b || (count && !angles)) return fail(SQ_ERR_INVALID, "null pointer");
+  if (circuit >= b->circs.size()) return fail(SQ_ERR_INVALID, "batch: bad circuit id");
+  uint32_t k = 0;
+  for (auto &op : b->circs[circuit].ops)
+    for (uint32_t j = 0; j < op.nangles; ++j) {
+      if (k >= count) return fail(SQ_ERR_INVALID, "batch: too few angles");
+      op.angles[j] = angles[k++];
+    }
+  if (k != count) return fail(SQ_ERR_INVALID, "batch: angle count mismatch");
+  return SQ_OK;
+}
+
+int sq_batch_num_circuits(const sq_batch *b, uint32_t *count) {
+  if (!b || !count) return fail(SQ_ERR_INVALID, "null pointer");
+  *count = uint32_t(b->circs.size());
+  return SQ_OK;
+}
+
+int sq_batch_run(sq_batch *b, double *energies, void *stream) {
+  if (!b || (!energies && !b->circs.empty())) return fail(SQ_ERR_INVALID, "null pointer");
+  auto st = static_cast<cudaStream_t>(stream);
+  return b->dtype == SQ_C64 ? run_impl<float>(b, energies, st) : run_impl<double>(b, energies, st);
+}
+
+int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream) {
+  if (!b || !host_dst) return fail(SQ_ERR_INVALID, "null pointer");
+  if (circuit >= b->state_off.size() || b->state_off[circuit] == ~uint64_t(0))
+    return fail(SQ_ERR_INVALID, "batch: state not kept (set SQ_BOPT_KEEP_STATES before run)");
+  const size_t amp = b->dtype == SQ_C64 ? 8 : 16;
+  const size_t n = size_t(1) << b->circs[circuit].n;
+  auto st = static_cast<cudaStream_t>(stream);
+  SQB_CUDA(cudaMemcpyAsync(host_dst, static_cast<char *>(b->d_pool.p) + b->state_off[circuit] * amp,
+                           n * amp, cudaMemcpyDeviceToHost, st));
+  SQB_CUDA(cudaStreamSynchronize(st));
+  return SQ_OK;
+}
+
+int sq_batch_last_timing(const sq_batch *b, double *kernel_ms, uint32_t *ctas) {
+  if (!b || !kernel_ms || !ctas) return fail(SQ_ERR_INVALID, "null pointer");
+  *kernel_ms = b->last_ms;
+  *ctas = b->last_ctas;
+  return SQ_OK;
+}
+
+}  // extern "C"

@@ -65,6 +65,10 @@ SQ_HD constexpr int sweep_low_bits(int m) { return m >= kLowBits + kRegBits ? kL
 constexpr int kTileBitsC128[] = {4, 7, 10, 11, 12};
 constexpr int kTileBitsC64[] = {4, 7, 10, 12};
 constexpr int kDefaultTileBitsC128 = 11;
+// Batched-circuit kernel tile sizes (a circuit of n <= this many qubits stays
+// in shared memory).
+constexpr int kBatchTileBitsC128 = 11;
+constexpr int kBatchTileBitsC64 = 12;
 // Two-state adjoint sweeps (twice the shared memory per tile).
 constexpr int kAdjTileBitsC128[] = {4, 7, 10};
 constexpr int kAdjTileBitsC64[] = {4, 7, 11};

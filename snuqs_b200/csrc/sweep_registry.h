@@ -26,3 +26,7 @@ SQ_DECLARE_ADJOINT(float, 4)
 SQ_DECLARE_ADJOINT(float, 7)
 SQ_DECLARE_ADJOINT(float, 11)
 #undef SQ_DECLARE_ADJOINT
+
+#define SQ_BATCH_PTR_NAME(real, m) SQ_SWEEP_CAT(sq_batch_kernel_ptr, real, m)
+const void *SQ_BATCH_PTR_NAME(double, 11)();
+const void *SQ_BATCH_PTR_NAME(float, 12)();
