@@ -65,7 +65,9 @@ typedef enum {
   SQ_OPT_FUSION = 0,    /* 1 (default): fused tile sweeps; 0: one unfused kernel per gate */
   SQ_OPT_TILE_BITS = 1, /* log2 amplitudes per shared-memory tile (4..12; default 12) */
   SQ_OPT_REORDER = 2,   /* 1 (default): the planner may absorb later gates that commute */
-  SQ_OPT_TIMING = 3     /* 1: record a CUDA event pair around every fused-sweep launch */
+  SQ_OPT_TIMING = 3,    /* 1: record a CUDA event pair around every fused-sweep launch */
+  SQ_OPT_JIT = 4        /* -1 (default): JIT-specialised sweep kernels for states of >= 20
+                           qubits when NVRTC is present; 1: always; 0: never */
 } sq_option;
 
 /* ---- library / device ------------------------------------------------ */
@@ -152,6 +154,12 @@ int sq_launch_count(const sq_state *s, uint64_t *count);
  * launches recorded since the last call (synchronises on the recorded
  * events, then clears them). */
 int sq_sweep_timing(sq_state *s, double *total_ms, uint64_t *launches);
+/* JIT-specialised sweeps, process-wide: whether NVRTC could be loaded, and
+ * how many sweeps ran a JIT kernel / fell back to the generic kernel. */
+int sq_jit_info(int *available, uint64_t *jit_launches, uint64_t *fallbacks);
+/* Test hook: compile `source` with NVRTC for sm_100a (no GPU needed).
+ * SQ_OK, or SQ_ERR_INVALID with the compiler log in sq_last_error(). */
+int sq_jit_compile(const char *source);
 
 /* cu::applyGate (gate_operations_impl_cuda.cu:159-175), unqueued: apply
  * one gate to a raw complex128 device buffer of nelems = 2^nqubits
@@ -197,6 +205,13 @@ typedef struct {
   double scale[3];
   const double *matrix;
 } sq_circuit_op;
+
+/* Test hook: CUDA source of the JIT kernel of fused sweep `sweep_index` of
+ * the default plan of a circuit (params ignored).  Writes at most cap bytes (NUL-terminated), the full length to
+ * *len and the number of fused sweeps to *nsweeps.  Needs no GPU. */
+int sq_jit_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
+                  uint32_t sweep_index, char *buf, uint64_t cap, uint64_t *len,
+                  uint32_t *nsweeps);
 
 /* Energy E = <psi|H|psi> of psi = U(theta)|0...0> for H = sum_t w_t P_t, and
  * dE/dtheta for n_params parameters, by one forward pass and one reverse

@@ -24,7 +24,7 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-ENGINE_CU = ["engine.cu", "noalloc.cu", "batch.cu"]
+ENGINE_CU = ["engine.cu", "noalloc.cu", "batch.cu", "jit.cu"]
 ENGINE_CC = ["gates.cc", "planner.cc", "adjoint_plan.cc"]
 # Fused-sweep kernel instantiations: (precision, tile bits, CTAs per SM).
 # Tile sizes must match kTileBitsC128 / kTileBitsC64 in csrc/sq_plan.h; the
@@ -67,9 +67,24 @@ def _headers() -> list[str]:
     return hs + [os.path.join(INCLUDE, "snuqs_b200.h")]
 
 
+def _write_jit_sources() -> None:
+    """Embeds the sweep headers in the library (NVRTC compiles them at run time)."""
+    out = os.path.join(BUILD, "jit_sources.inc")
+    parts = []
+    for var, fname in (("kJitPlanSource", "sq_plan.h"), ("kJitSweepSource", "sweep_kernels.cuh")):
+        text = open(os.path.join(CSRC, fname)).read()
+        assert ")SQJIT\"" not in text
+        parts.append(f'static const char {var}[] = R"SQJIT({text})SQJIT";\n')
+    data = "".join(parts)
+    if not os.path.exists(out) or open(out).read() != data:
+        with open(out, "w") as f:
+            f.write(data)
+
+
 def build(force: bool = False, verbose: bool = False) -> None:
     os.makedirs(BUILD, exist_ok=True)
-    common = ["-O3", "-std=c++17", "-I", CSRC, "-I", INCLUDE]
+    _write_jit_sources()
+    common = ["-O3", "-std=c++17", "-I", CSRC, "-I", INCLUDE, "-I", BUILD]
     objs = []
     hdrs = _headers()
     for f in ENGINE_CU:
@@ -131,7 +146,7 @@ def build(force: bool = False, verbose: bool = False) -> None:
         objs.append(obj)
     if force or _stale(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static",
-              "-Xlinker", "--no-undefined"])
+              "-ldl", "-Xlinker", "--no-undefined"])
     import pybind11
 
     pysrc = os.path.join(CSRC, "pymodule.cc")

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(_HERE, "libsnuqs_b200.so")
 
 SQ_OK, SQ_ERR_INVALID, SQ_ERR_CUDA, SQ_ERR_OOM, SQ_ERR_UNSUPPORTED, SQ_ERR_TIMEOUT = range(6)
 SQ_C128, SQ_C64 = 0, 1
-SQ_OPT_FUSION, SQ_OPT_TILE_BITS, SQ_OPT_REORDER, SQ_OPT_TIMING = 0, 1, 2, 3
+SQ_OPT_FUSION, SQ_OPT_TILE_BITS, SQ_OPT_REORDER, SQ_OPT_TIMING, SQ_OPT_JIT = 0, 1, 2, 3, 4
 
 GATE_NAMES = [
     "Identity", "Hadamard", "PauliX", "PauliY", "PauliZ", "CX", "CY", "CZ", "S", "Si", "T",
@@ -71,6 +71,9 @@ SIGNATURES = {
     "sq_pending": (_I, [_P, _PU32]),
     "sq_launch_count": (_I, [_P, _PU64]),
     "sq_sweep_timing": (_I, [_P, _PD, _PU64]),
+    "sq_jit_info": (_I, [ctypes.POINTER(_I), _PU64, _PU64]),
+    "sq_jit_compile": (_I, [ctypes.c_char_p]),
+    "sq_jit_source": (_I, [_U32, _I, _P, _U32, _U32, ctypes.c_char_p, _U64, _PU64, _PU32]),
     "sq_apply_gate_buffer": (_I, [_P, _P, _PU64, _U32, _U32, _U64, _P]),
     "sq_copy_to_host": (_I, [_P, _P, _P]),
     "sq_copy_from_host": (_I, [_P, _P, _P]),
@@ -99,6 +102,36 @@ class SqCircuitOp(ctypes.Structure):
                 ("nangles", ctypes.c_uint32), ("angles", ctypes.c_double * 3),
                 ("param", ctypes.c_int32 * 3), ("scale", ctypes.c_double * 3),
                 ("matrix", ctypes.POINTER(ctypes.c_double))]
+
+
+def jit_info():
+    """(NVRTC available, JIT sweep launches, fallbacks to the generic kernel)."""
+    av, a, b = ctypes.c_int(0), _U64(0), _U64(0)
+    check(lib().sq_jit_info(ctypes.byref(av), ctypes.byref(a), ctypes.byref(b)))
+    return bool(av.value), a.value, b.value
+
+
+def jit_sources(n: int, ops, dtype: int = SQ_C128, limit: int | None = None):
+    """CUDA sources of the JIT kernels of the fused sweeps of a circuit."""
+    arr, keep = circuit_ops(ops)
+    ln, ns = _U64(0), _U32(0)
+    check(lib().sq_jit_source(n, dtype, ctypes.cast(arr, _P), len(ops), 0, None, 0,
+                              ctypes.byref(ln), ctypes.byref(ns)))
+    out = []
+    for i in range(ns.value if limit is None else min(limit, ns.value)):
+        check(lib().sq_jit_source(n, dtype, ctypes.cast(arr, _P), len(ops), i, None, 0,
+                                  ctypes.byref(ln), ctypes.byref(ns)))
+        buf = ctypes.create_string_buffer(ln.value + 1)
+        check(lib().sq_jit_source(n, dtype, ctypes.cast(arr, _P), len(ops), i, buf, ln.value + 1,
+                                  ctypes.byref(ln), ctypes.byref(ns)))
+        out.append(buf.value.decode())
+    del keep
+    return out
+
+
+def jit_compile(source: str) -> None:
+    """NVRTC-compiles a kernel source for sm_100a; raises SqError with the log."""
+    check(lib().sq_jit_compile(source.encode()))
 
 
 def circuit_ops(ops):

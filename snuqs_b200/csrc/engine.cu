@@ -3,7 +3,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -17,6 +19,7 @@
 #include "adjoint_kernels.cuh"
 #include "adjoint_plan.h"
 #include "host_ops.h"
+#include "jit.h"
 #include "reduce_kernels.cuh"
 #include "sweep_kernels.cuh"
 #include "sweep_registry.h"
@@ -79,8 +82,24 @@ struct sq_state {
   uint32_t scratch_len = 0;
   uint64_t launches = 0;
   int timing = 0;
+  int jit = -1;  // -1: automatic (states of >= kJitMinQubits qubits), 0: off, 1: on
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sweep_events;
 };
+
+// JIT-specialised sweeps pay a one-off NVRTC compile per distinct sweep
+// structure; below this size the generic kernel's sweeps are too short for
+// the compile to pay back within a few circuit runs.
+static constexpr uint32_t kJitMinQubits = 20;
+
+static bool use_jit(const sq_state *s) {
+  static const bool env_off = [] {
+    const char *e = std::getenv("SQ_JIT");
+    return e && e[0] == '0';
+  }();
+  if (s->jit == 0 || !sq::jit_available()) return false;
+  if (s->jit == 1) return true;
+  return !env_off && s->n >= kJitMinQubits;
+}
 
 static size_t amp_bytes(int dtype) { return dtype == SQ_C64 ? 8 : 16; }
 
@@ -237,9 +256,25 @@ static int launch_sweep(sq_state *s, const sq::PlannedSweep &ps, cudaStream_t st
                       size_t((ps.h.ncoef + 1) & ~1u) * sizeof(C2) +
                       (size_t(1) << (m - l)) * sizeof(uint64_t);
   int per_sm = 0;
-  const void *fn = sweep_fn<Real>(m);
-  if (!fn) return fail(SQ_ERR_INVALID, "internal: no sweep kernel for %u tile bits", m);
-  SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  const void *fn = nullptr;
+  if (use_jit(s)) {
+    std::string err;
+    fn = sq::jit_sweep_kernel(ps, sizeof(Real) == 4, err);
+    if (fn && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
+      cudaGetLastError();
+      fn = nullptr;
+    }
+    if (fn && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = sq::jit_minb(sizeof(Real) == 4, m);
+    }
+    sq::jit_note_launch(fn != nullptr);
+  }
+  if (!fn) {
+    fn = sweep_fn<Real>(m);
+    if (!fn) return fail(SQ_ERR_INVALID, "internal: no sweep kernel for %u tile bits", m);
+    SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  }
   if (per_sm < 1) per_sm = 1;
   const uint64_t grid = std::min<uint64_t>(ps.h.num_tiles, uint64_t(per_sm) * di.sms);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -409,6 +444,12 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
     plan = sq::plan_sweeps(ops, n, opt);
   } catch (const std::exception &e) {
     return fail(SQ_ERR_INVALID, "planner: %s", e.what());
+  }
+  if (use_jit(s)) {
+    std::vector<const sq::PlannedSweep *> sweeps;
+    for (const auto &pl : plan)
+      if (pl.is_sweep) sweeps.push_back(&pl.sweep);
+    sq::jit_prepare(sweeps, c64);
   }
   for (const auto &pl : plan) {
     if (pl.is_sweep) {
@@ -604,6 +645,10 @@ int sq_set_option(sq_state *s, int option, int64_t value) {
       return SQ_OK;
     case SQ_OPT_REORDER: s->reorder = value != 0; return SQ_OK;
     case SQ_OPT_TIMING: s->timing = value != 0; return SQ_OK;
+    case SQ_OPT_JIT:
+      if (value < -1 || value > 1) return fail(SQ_ERR_INVALID, "SQ_OPT_JIT takes -1, 0 or 1");
+      s->jit = int(value);
+      return SQ_OK;
     default: return fail(SQ_ERR_INVALID, "unknown option %d", option);
   }
 }

@@ -1,0 +1,25 @@
+// JIT-specialised sweep kernels (see jit.cu).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "host_ops.h"
+
+namespace sq {
+
+bool jit_available();
+// Counts a sweep launch that ran a JIT kernel (true) or fell back (false).
+void jit_note_launch(bool jit);
+// CUDA source of the kernel specialised for `ps` (`minb` CTAs per SM).
+std::string jit_source(const PlannedSweep &ps, bool c64, int minb);
+// The part of that source that depends on `ps` (the cache key).
+std::string jit_body(const PlannedSweep &ps, bool c64, int minb);
+// CTAs per SM the kernels of (precision, tile bits) are built for.
+int jit_minb(bool c64, uint32_t m);
+// Launchable kernel (a cudaKernel_t as const void*) for `ps`, compiling and
+// caching it on first use; nullptr with `err` set when it cannot be built.
+const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err);
+// Compiles the kernels of several sweeps in parallel (fills the cache).
+void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64);
+
+}  // namespace sq

@@ -10,7 +10,9 @@
 // lie in R.  Controls and diagonal gates may sit on any index bit, inside or
 // outside the tile: a thread knows the full index of every amplitude it holds.
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <stdint.h>
+#endif
 
 namespace sq {
 

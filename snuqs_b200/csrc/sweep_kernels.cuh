@@ -10,10 +10,12 @@
 //   fusion is off, for k > 4 dense matrices and for cu::applyGate's literal
 //   replacement.
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "sq_plan.h"
+#endif
 
 namespace sq {
 
@@ -457,6 +459,134 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
       }
     }
     // Everyone is done with `tile` before the next iteration prefetches into it.
+    __syncthreads();
+    cur ^= 1;
+  }
+  cp_async_wait_prev();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Building blocks of the JIT-specialised sweep kernels (snuqs_b200/csrc/jit.cu
+// generates one kernel per planned sweep from these).  Register positions,
+// op kinds, masks and coefficient offsets become compile-time constants, so
+// each phase compiles to straight-line code: no op dispatch, and no register
+// shuffling back to fixed registers between gates.
+// ---------------------------------------------------------------------------
+template <typename Real, int M, int R0, int R1, int R2, int R3>
+struct JitPhase {
+  using C2 = typename Vec2<Real>::T;
+  static constexpr int L = sweep_low_bits(M);
+  __device__ __forceinline__ static uint32_t jb(uint32_t tid) {
+    uint32_t x = tid;
+    x = uint32_t(insert_zero(x, R0));
+    x = uint32_t(insert_zero(x, R1));
+    x = uint32_t(insert_zero(x, R2));
+    x = uint32_t(insert_zero(x, R3));
+    return x;
+  }
+  __device__ __forceinline__ static uint32_t slot(uint32_t sb, int ri) {
+    return sb ^ ((ri & 1) ? swz<Real>(1u << R0) : 0u) ^ ((ri & 2) ? swz<Real>(1u << R1) : 0u) ^
+           ((ri & 4) ? swz<Real>(1u << R2) : 0u) ^ ((ri & 8) ? swz<Real>(1u << R3) : 0u);
+  }
+  __device__ __forceinline__ static void gather(Amps<Real> &A, const C2 *tile, uint32_t jbv) {
+    const uint32_t sb = swz<Real>(jbv);
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri) {
+      const C2 v = tile[slot(sb, ri)];
+      A.re[ri] = v.x;
+      A.im[ri] = v.y;
+    }
+  }
+  __device__ __forceinline__ static void scatter(const Amps<Real> &A, C2 *tile, uint32_t jbv) {
+    const uint32_t sb = swz<Real>(jbv);
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri) {
+      C2 v;
+      v.x = A.re[ri];
+      v.y = A.im[ri];
+      tile[slot(sb, ri)] = v;
+    }
+  }
+  // Straight to HBM from registers (the last phase, when its register bits
+  // leave the low tile bits to the lanes).
+  __device__ __forceinline__ static void store(const Amps<Real> &A, C2 *psi, const SweepHeader &h,
+                                               const uint64_t *hitab, uint64_t gbase, uint32_t jbv) {
+    auto gw = [&](int pos) -> uint64_t {
+      return pos < L ? (uint64_t(1) << pos) : (uint64_t(1) << h.hi[pos - L]);
+    };
+    const uint64_t tbase = gbase | hitab[jbv >> L] | (jbv & ((1u << L) - 1u));
+    const uint64_t g0 = gw(R0), g1 = gw(R1), g2 = gw(R2), g3 = gw(R3);
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri) {
+      C2 v;
+      v.x = A.re[ri];
+      v.y = A.im[ri];
+      psi[tbase + ((ri & 1) ? g0 : 0) + ((ri & 2) ? g1 : 0) + ((ri & 4) ? g2 : 0) +
+          ((ri & 8) ? g3 : 0)] = v;
+    }
+  }
+};
+
+// The tile loop of sweep_kernel with the phases supplied by the generated
+// kernel: phases(tile, coef, gbase, hitab) runs every phase of one tile.
+template <typename Real, int M, class Phases>
+__device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ psi,
+                                          const SweepParams<Real> &P, Phases phases) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int NT = 1 << (M - kRegBits);
+  constexpr int L = sweep_low_bits(M);
+  constexpr uint32_t TS = 1u << M;
+  constexpr uint32_t PER = TS / NT;
+  constexpr uint32_t LOWMASK = (1u << L) - 1u;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SweepHeader &h = P.h;
+  C2 *bufs = reinterpret_cast<C2 *>(smem_raw);
+  C2 *coef = bufs + 2 * TS;
+  uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + ((h.ncoef + 1) & ~1u));
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t i = tid; i < h.ncoef; i += NT) {
+    C2 v;
+    v.x = P.coef[2 * i];
+    v.y = P.coef[2 * i + 1];
+    coef[i] = v;
+  }
+  for (uint32_t c = tid; c < (1u << (M - L)); c += NT) {
+    uint64_t a = 0;
+#pragma unroll
+    for (int i = 0; i < M - L; ++i)
+      if ((c >> i) & 1) a |= uint64_t(1) << h.hi[i];
+    hitab[c] = a;
+  }
+  __syncthreads();
+  const uint32_t s_tid = swz<Real>(tid);
+  auto prefetch = [&](uint64_t t, C2 *dst) {
+    const uint64_t gb = tile_base(t, h);
+#pragma unroll
+    for (uint32_t it = 0; it < PER; ++it) {
+      const uint32_t j = it * NT + tid;
+      cp_async<sizeof(C2)>(dst + (s_tid ^ swz<Real>(it * NT)), psi + (gb | hitab[j >> L] | (j & LOWMASK)));
+    }
+  };
+  uint32_t cur = 0;
+  if (blockIdx.x < h.num_tiles) prefetch(blockIdx.x, bufs);
+  cp_async_commit();
+  for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
+    C2 *tile = bufs + cur * TS;
+    const uint64_t tn = t + gridDim.x;
+    if (tn < h.num_tiles) prefetch(tn, bufs + (cur ^ 1) * TS);
+    cp_async_commit();
+    cp_async_wait_prev();
+    __syncthreads();
+    const uint64_t gbase = tile_base(t, h);
+    phases(tile, coef, gbase, hitab);
+    if (!(h.flags & kDirectStore)) {
+#pragma unroll
+      for (uint32_t it = 0; it < PER; ++it) {
+        const uint32_t j = it * NT + tid;
+        psi[gbase | hitab[j >> L] | (j & LOWMASK)] = tile[s_tid ^ swz<Real>(it * NT)];
+      }
+    }
     __syncthreads();
     cur ^= 1;
   }

@@ -1,0 +1,66 @@
+"""JIT-specialised sweep kernels, without a GPU: the generated CUDA source of
+every fused sweep compiles with NVRTC for sm_100a, depends on the circuit's
+structure only (angles are kernel parameters, so one compiled kernel serves
+every parameter value), and covers every sweep-op kind the planner emits."""
+import re
+
+import numpy as np
+import pytest
+
+from snuqs_b200 import capi, circuits
+
+pytestmark = pytest.mark.skipif(not capi.jit_info()[0], reason="NVRTC is not available")
+
+OP_ROUTINES = ("op_phase", "op_diag", "op_anti1", "op_swap2", "op_xrot", "op_dense")
+
+
+def _cases():
+    return [
+        ("all_gates_14q_c128", 14, circuits.random_all_gates(14, 300, seed=5), capi.SQ_C128),
+        ("all_gates_14q_c64", 14, circuits.random_all_gates(14, 300, seed=6), capi.SQ_C64),
+        ("random_mix_26q_c128", 26, circuits.random_mix(26, 120, seed=7), capi.SQ_C128),
+        ("quantum_volume_12q_c64", 12, circuits.quantum_volume(12, 4, seed=8), capi.SQ_C64),
+    ]
+
+
+@pytest.mark.parametrize("case", _cases(), ids=lambda c: c[0])
+def test_generated_sources_compile(case):
+    _, n, ops, dtype = case
+    srcs = capi.jit_sources(n, ops, dtype)
+    assert srcs
+    for src in srcs[:12]:
+        capi.jit_compile(src)
+
+
+def test_sources_cover_every_op_kind():
+    seen = set()
+    for _, n, ops, dtype in _cases():
+        for src in capi.jit_sources(n, ops, dtype):
+            body = src[src.rindex("sq_jit_sweep"):]
+            seen |= {r for r in OP_ROUTINES if r + "<" in body}
+            if "gbase & 0x" in body:
+                seen.add("global_control")
+            if "jb & 0x" in body:
+                seen.add("tile_control")
+            if "Ph::store(" in body:
+                seen.add("direct_store")
+    assert seen >= set(OP_ROUTINES) | {"global_control", "direct_store"}, seen
+
+
+def test_sources_depend_on_structure_not_angles():
+    n = 24
+    a = circuits.random_mix(n, 150, seed=11)
+    rng = np.random.default_rng(3)
+    b = [(name, q, tuple(rng.uniform(0.1, 3.0, size=len(ang)))) for name, q, ang in a]
+    sa, sb = capi.jit_sources(n, a), capi.jit_sources(n, b)
+    assert sa == sb
+
+
+def test_compile_errors_are_reported():
+    with pytest.raises(capi.SqError, match="NVRTC compile failed"):
+        capi.jit_compile("extern \"C\" __global__ void sq_jit_sweep() { undefined_name(); }")
+
+
+def test_kernel_signature():
+    src = capi.jit_sources(20, circuits.random_mix(20, 30, seed=2), capi.SQ_C64, limit=1)[0]
+    assert re.search(r'extern "C" __global__ void __launch_bounds__\(256, 2\)\s*sq_jit_sweep', src)
