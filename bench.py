@@ -260,6 +260,7 @@ def _run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     l0 = st.launches()
     st.set_option(capi.SQ_OPT_TIMING, 1)
+    jit0 = capi.jit_info()[1]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -274,6 +275,7 @@ def _run_ours(args, rank, world, local):
     ms = ev0.elapsed_time(ev1) / args.steps
     sweep_ms, sweeps = st.sweep_timing()
     launches = st.launches() - l0
+    jit_sweeps = capi.jit_info()[1] - jit0
     if world > 1:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -297,8 +299,10 @@ def _run_ours(args, rank, world, local):
         "gates_per_sweep": round(args.gates / max(1e-9, sweeps_per_step), 2),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                     "kernel": "sq::sweep_kernel<double>" if dtype == capi.SQ_C128 else
-                     "sq::sweep_kernel<float>",
+                     "kernel": ("sq_jit_sweep (NVRTC-specialised sweep, " if jit_sweeps == sweeps
+                                else "sq::sweep_kernel (") +
+                               ("double)" if dtype == capi.SQ_C128 else "float)"),
+                     "jit_sweeps": jit_sweeps,
                      "per_launch_ms": round(per_launch_ms, 4),
                      "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
         "gpu_launches": launches, "clocks": clocks,

@@ -17,6 +17,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -33,6 +34,7 @@
 #include "adjoint_plan.h"
 #include "host_ops.h"
 #include "jit.h"
+#include "sweep_kernels.cuh"
 
 int sq_detail_fail(int code, const char *msg);  // engine.cu: sets sq_last_error()
 
@@ -251,6 +253,43 @@ bool jit_available() { return nvrtc().ok; }
 
 void jit_note_launch(bool jit) { (jit ? g_launches : g_fallbacks)++; }
 
+// Tile positions of the thread bits of a phase: the lane bits that share a
+// shared-memory wavefront (the low W) go on non-register positions whose
+// swizzle images are linearly independent, the rest ascending.  A phase that
+// stores straight to HBM keeps all thread bits ascending (the lanes then
+// cover contiguous amplitudes).
+std::vector<int> thread_positions(const SweepPhase &ph, int m, bool c64, bool direct_store) {
+  const int W = c64 ? Swz<float>::W : Swz<double>::W;
+  const uint8_t *img = c64 ? Swz<float>::kImage : Swz<double>::kImage;
+  uint32_t regs = 0;
+  for (int b = 0; b < kRegBits; ++b) regs |= 1u << ph.reg[b];
+  std::vector<int> nonreg;
+  for (int p = 0; p < m; ++p)
+    if (!((regs >> p) & 1)) nonreg.push_back(p);
+  if (direct_store) return nonreg;
+  std::vector<int> lanes;
+  int basis[8] = {0};
+  for (int p : nonreg) {
+    if (int(lanes.size()) == W) break;
+    int x = img[p];
+    for (int b = W - 1; b >= 0 && x; --b)
+      if ((x >> b) & 1) {
+        if (!basis[b]) {
+          basis[b] = x;
+          lanes.push_back(p);
+          x = 0;
+        } else {
+          x ^= basis[b];
+        }
+      }
+  }
+  if (int(lanes.size()) < W || int(nonreg.size()) < W) return nonreg;
+  std::vector<int> out = lanes;
+  for (int p : nonreg)
+    if (std::find(lanes.begin(), lanes.end(), p) == lanes.end()) out.push_back(p);
+  return out;
+}
+
 std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
   const char *R = c64 ? "float" : "double";
   const int M = int(ps.h.m);
@@ -265,7 +304,9 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
   for (uint32_t p = 0; p < ps.h.nphases; ++p) {
     const SweepPhase &ph = ps.ph[p];
     s << "    {\n      using Ph = JitPhase<" << R << ", " << M << ", " << int(ph.reg[0]) << ", "
-      << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]) << ">;\n";
+      << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]);
+    for (int t : thread_positions(ph, M, c64, p == last && (ps.h.flags & kDirectStore))) s << ", " << t;
+    s << ">;\n";
     s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << "> A;\n"
       << "      Ph::gather(A, tile, jb);\n";
     for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {

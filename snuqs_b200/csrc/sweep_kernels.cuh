@@ -23,18 +23,61 @@ template <typename Real> struct Vec2;
 template <> struct Vec2<double> { using T = double2; };
 template <> struct Vec2<float> { using T = float2; };
 
-// Shared-memory swizzle for the amplitude tile: XOR the low W bits of the
-// tile index with the fold of its higher W-bit groups.  W = log2 of the
-// number of amplitudes one 128-byte shared-memory wavefront holds, so the
-// lanes of a warp that differ in any three (c128) / four (c64) tile bits of
-// distinct residue land in distinct banks.
+// Shared-memory swizzle for the amplitude tile: slot(j) = j ^ S(j >> W),
+// S linear over GF(2): tile position p >= W adds the W-bit image kSwzImage[p]
+// to the low W bits.  W = log2 of the amplitudes one 128-byte shared-memory
+// wavefront holds (3 for complex128, 4 for complex64), so the 2^W lanes that
+// share a wavefront are conflict-free exactly when the images of the tile
+// positions their lane bits sit on are linearly independent (position p < W
+// has image e_p).  The images were chosen by exhaustive search so that
+//  - for every choice of 4 register positions in tiles of 10..12 bits
+//    (complex128) / 11..12 bits (complex64), the remaining positions span
+//    GF(2)^W: the JIT kernels can always place the lane bits conflict-free;
+//  - with the lane bits on the lowest non-register positions (the generic
+//    kernels) 96 % (complex128) / 81 % (complex64) of those register choices
+//    are conflict-free, against 48 % / 32 % for the plain fold of the
+//    high bits.
+// The map is a bijection that only changes the low W bits, and XOR-linear:
+// slot(a ^ b) = slot(a) ^ slot(b).
+template <typename Real> struct Swz;
+template <> struct Swz<double> {
+  static constexpr int W = 3;
+  static constexpr uint8_t kImage[12] = {1, 2, 4, 7, 3, 5, 6, 4, 5, 7, 6, 6};
+};
+template <> struct Swz<float> {
+  static constexpr int W = 4;
+  static constexpr uint8_t kImage[12] = {1, 2, 4, 8, 14, 11, 7, 13, 10, 15, 6, 10};
+};
+
+// Positions p >= W whose image has bit i set.
+template <typename Real>
+__host__ __device__ constexpr uint32_t swz_mask(int i) {
+  uint32_t m = 0;
+  for (int p = Swz<Real>::W; p < kMaxTileBits; ++p)
+    if ((Swz<Real>::kImage[p] >> i) & 1) m |= 1u << p;
+  return m;
+}
+
+// Compile-time form (constant arguments).
+template <typename Real>
+__host__ __device__ constexpr uint32_t swz_c(uint32_t j) {
+  uint32_t low = 0;
+  for (int i = 0; i < Swz<Real>::W; ++i) {
+    uint32_t x = j & swz_mask<Real>(i), par = 0;
+    for (; x; x &= x - 1) par ^= 1u;
+    low |= par << i;
+  }
+  return j ^ low;
+}
+
 template <typename Real>
 __device__ __forceinline__ uint32_t swz(uint32_t j) {
-  constexpr int W = sizeof(Real) == 8 ? 3 : 4;
-  uint32_t x = j >> W, f = 0;
-#pragma unroll
-  for (int s = 0; s < 16; s += W) f ^= x >> s;
-  return j ^ (f & ((1u << W) - 1u));
+  constexpr uint32_t m0 = swz_mask<Real>(0), m1 = swz_mask<Real>(1), m2 = swz_mask<Real>(2);
+  constexpr uint32_t m3 = Swz<Real>::W > 3 ? swz_mask<Real>(3) : 0u;
+  uint32_t low = (uint32_t(__popc(j & m0)) & 1u) | ((uint32_t(__popc(j & m1)) & 1u) << 1) |
+                 ((uint32_t(__popc(j & m2)) & 1u) << 2);
+  if constexpr (Swz<Real>::W > 3) low |= (uint32_t(__popc(j & m3)) & 1u) << 3;
+  return j ^ low;
 }
 
 // Insert a zero bit at position p of x (shifts bits >= p up by one).
@@ -473,21 +516,24 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
 // each phase compiles to straight-line code: no op dispatch, and no register
 // shuffling back to fixed registers between gates.
 // ---------------------------------------------------------------------------
-template <typename Real, int M, int R0, int R1, int R2, int R3>
+template <typename Real, int M, int R0, int R1, int R2, int R3, int... T>
 struct JitPhase {
   using C2 = typename Vec2<Real>::T;
   static constexpr int L = sweep_low_bits(M);
+  static_assert(sizeof...(T) == M - kRegBits, "one tile position per thread bit");
+  // Thread bit i sits on tile position T[i]: the code generator places the
+  // lane bits that share a shared-memory wavefront on positions whose swizzle
+  // images are independent (conflict-free gathers and scatters).
   __device__ __forceinline__ static uint32_t jb(uint32_t tid) {
-    uint32_t x = tid;
-    x = uint32_t(insert_zero(x, R0));
-    x = uint32_t(insert_zero(x, R1));
-    x = uint32_t(insert_zero(x, R2));
-    x = uint32_t(insert_zero(x, R3));
+    uint32_t x = 0;
+    int i = 0;
+    ((x |= ((tid >> i++) & 1u) << T), ...);
     return x;
   }
   __device__ __forceinline__ static uint32_t slot(uint32_t sb, int ri) {
-    return sb ^ ((ri & 1) ? swz<Real>(1u << R0) : 0u) ^ ((ri & 2) ? swz<Real>(1u << R1) : 0u) ^
-           ((ri & 4) ? swz<Real>(1u << R2) : 0u) ^ ((ri & 8) ? swz<Real>(1u << R3) : 0u);
+    constexpr uint32_t W0 = swz_c<Real>(1u << R0), W1 = swz_c<Real>(1u << R1);
+    constexpr uint32_t W2 = swz_c<Real>(1u << R2), W3 = swz_c<Real>(1u << R3);
+    return sb ^ ((ri & 1) ? W0 : 0u) ^ ((ri & 2) ? W1 : 0u) ^ ((ri & 4) ? W2 : 0u) ^ ((ri & 8) ? W3 : 0u);
   }
   __device__ __forceinline__ static void gather(Amps<Real> &A, const C2 *tile, uint32_t jbv) {
     const uint32_t sb = swz<Real>(jbv);

@@ -64,3 +64,38 @@ def test_compile_errors_are_reported():
 def test_kernel_signature():
     src = capi.jit_sources(20, circuits.random_mix(20, 30, seed=2), capi.SQ_C64, limit=1)[0]
     assert re.search(r'extern "C" __global__ void __launch_bounds__\(256, 2\)\s*sq_jit_sweep', src)
+
+
+SWZ_IMAGES = {  # sweep_kernels.cuh, Swz<Real>::kImage
+    capi.SQ_C128: (3, [1, 2, 4, 7, 3, 5, 6, 4, 5, 7, 6, 6]),
+    capi.SQ_C64: (4, [1, 2, 4, 8, 14, 11, 7, 13, 10, 15, 6, 10]),
+}
+
+
+def _rank(vectors):
+    basis = []
+    for v in vectors:
+        for b in basis:
+            v = min(v, v ^ b)
+        if v:
+            basis.append(v)
+    return len(basis)
+
+
+@pytest.mark.parametrize("dtype", [capi.SQ_C128, capi.SQ_C64])
+def test_lane_placement_is_a_permutation_and_conflict_free(dtype):
+    n = 26
+    W, img = SWZ_IMAGES[dtype]
+    phases = conflict_free = 0
+    for src in capi.jit_sources(n, circuits.random_mix(n, 200, seed=13), dtype):
+        body = src[src.rindex("sq_jit_sweep"):]
+        for args in re.findall(r"JitPhase<\w+, ([\d, ]+)>", body):
+            vals = [int(x) for x in args.split(",")]
+            m, regs, threads = vals[0], vals[1:5], vals[5:]
+            assert sorted(regs + threads) == list(range(m))
+            phases += 1
+            conflict_free += _rank([img[p] for p in threads[:W]]) == W
+    assert phases > 0
+    # Every phase except the direct-store ones (ascending lanes from tile
+    # position 0, also conflict-free) gets independent lane images.
+    assert conflict_free == phases
