@@ -75,7 +75,16 @@ struct PlanOptions {
   // Register bits per phase: 4 (16 amplitudes per thread, the sweep kernel)
   // or 3 (8 amplitudes per state per thread, the two-state adjoint kernel).
   uint32_t reg_bits = kRegBits;
+  // Low index bits every tile contains (contiguous runs of 2^low_bits
+  // amplitudes per global access); 0: sweep_low_bits(tile bits).
+  uint32_t low_bits = 0;
+  // Tile selection and phase scheduling (needs reorder): 1 = choose each
+  // sweep's tile bits to absorb the most upcoming gates and order the gates
+  // of a sweep into the fewest register phases; 0 = take gates first come
+  // first served; -1 = 1 for states of >= kSelectMinQubits qubits.
+  int select = -1;
 };
+constexpr uint32_t kSelectMinQubits = 18;
 
 // Packs ops (in circuit order) into fused sweeps for an n-qubit state.
 std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t n,

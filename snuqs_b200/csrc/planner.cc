@@ -317,6 +317,140 @@ PlannedSweep SweepBuilder::finish() const {
   return ps;
 }
 
+// ---------------------------------------------------------------------------
+// Tile selection and phase scheduling.
+// ---------------------------------------------------------------------------
+bool fusable_size(const HostOp &op, const PlanOptions &opt) {
+  if (SweepBuilder::is_diag(op)) return op.tbits.size() <= size_t(kMaxDiagK);
+  const uint32_t kmax = op.kind == kOpInner ? opt.reg_bits : std::min(opt.max_dense_k, opt.reg_bits);
+  return op.tbits.size() <= size_t(kmax);
+}
+
+// Gates from rem[head..] that a sweep with tile bits S takes (same rules as
+// the collection below, without growing S).
+uint32_t absorbed(const std::vector<const HostOp *> &rem, size_t head, uint64_t S, uint32_t n,
+                  const PlanOptions &opt, size_t window) {
+  uint32_t cnt = 0, ncoef = 0, ninner = 0;
+  uint64_t blockT = 0, blockA = 0;
+  size_t skipped = 0;
+  for (size_t i = head; i < rem.size(); ++i) {
+    const HostOp &op = *rem[i];
+    const uint64_t T = op.nondiag_mask(), A = op.touched_mask();
+    const bool commutes = (T & blockA) == 0 && (A & blockT) == 0;
+    const bool diag = SweepBuilder::is_diag(op);
+    const uint32_t c = SweepBuilder::coef_count(op);
+    const bool fits = fusable_size(op, opt) && (diag || (op.target_mask() & ~S) == 0) &&
+                      cnt < uint32_t(kMaxOps) && ncoef + c <= uint32_t(kMaxCoef) &&
+                      !(op.kind == kOpInner && ninner >= uint32_t(kMaxInner));
+    if (commutes && fits) {
+      ++cnt;
+      ncoef += c;
+      if (op.kind == kOpInner) ++ninner;
+      if (cnt >= uint32_t(kMaxOps)) break;
+      continue;
+    }
+    blockT |= T;
+    blockA |= A;
+    if (++skipped >= window || popc64(blockT) >= int(n)) break;
+  }
+  return cnt;
+}
+
+// Tile bits (the l low bits plus up to m - l more) that maximise the gates
+// the sweep absorbs: grown one bit, or one pair of a two-target gate's
+// bits, at a time by the best gain per added bit.
+uint64_t select_tile(const std::vector<const HostOp *> &rem, size_t head, uint32_t n, uint32_t m,
+                     uint32_t l, const PlanOptions &opt, size_t window) {
+  uint64_t S = (uint64_t(1) << l) - 1;
+  uint32_t cur = absorbed(rem, head, S, n, opt, window);
+  while (uint32_t(popc64(S)) < m) {
+    // Candidate bits: targets of the next gates outside S.
+    uint64_t cand = 0;
+    std::vector<uint64_t> pairs;
+    for (size_t i = head, seen = 0; i < rem.size() && seen < 2 * window; ++i, ++seen) {
+      const HostOp &op = *rem[i];
+      if (SweepBuilder::is_diag(op) || !fusable_size(op, opt)) continue;
+      const uint64_t out = op.target_mask() & ~S;
+      cand |= out;
+      if (popc64(out) == 2 && std::find(pairs.begin(), pairs.end(), out) == pairs.end() &&
+          pairs.size() < 48)
+        pairs.push_back(out);
+    }
+    if (!cand) break;
+    double best = 0.0;
+    uint64_t best_add = 0;
+    for (uint32_t b = 0; b < n; ++b) {
+      if (!((cand >> b) & 1)) continue;
+      const uint64_t add = uint64_t(1) << b;
+      const double g = double(absorbed(rem, head, S | add, n, opt, window)) - cur;
+      if (g > best) best = g, best_add = add;
+    }
+    if (uint32_t(popc64(S)) + 2 <= m)
+      for (uint64_t pr : pairs) {
+        const double g = (double(absorbed(rem, head, S | pr, n, opt, window)) - cur) / 2.0;
+        if (g > best) best = g, best_add = pr;
+      }
+    if (!best_add) break;
+    S |= best_add;
+    cur = absorbed(rem, head, S, n, opt, window);
+  }
+  return S;
+}
+
+// Orders the ops of one sweep (circuit order, at most 64) into phases: a
+// phase opens with the ready op that adds the fewest new register bits and
+// takes every ready op that fits its register set (diagonal ops fit any
+// phase).  Op j depends on an earlier op i when they do not commute.
+// Returns the new order and the first index of each phase.
+void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits,
+                     std::vector<const HostOp *> &order, std::vector<uint64_t> &phase_regs,
+                     std::vector<uint32_t> &phase_first) {
+  const size_t N = ops.size();
+  std::vector<uint64_t> pred(N, 0);
+  for (size_t j = 0; j < N; ++j) {
+    const uint64_t Tj = ops[j]->nondiag_mask(), Aj = ops[j]->touched_mask();
+    for (size_t i = 0; i < j; ++i) {
+      const uint64_t Ti = ops[i]->nondiag_mask(), Ai = ops[i]->touched_mask();
+      if ((Ti & Aj) || (Ai & Tj)) pred[j] |= uint64_t(1) << i;
+    }
+  }
+  const uint64_t all = N == 64 ? ~uint64_t(0) : ((uint64_t(1) << N) - 1);
+  uint64_t placed = 0;
+  order.clear();
+  phase_regs.clear();
+  phase_first.clear();
+  while (placed != all) {
+    uint64_t R = 0;
+    phase_first.push_back(uint32_t(order.size()));
+    for (;;) {
+      bool progress = false;
+      for (size_t x = 0; x < N; ++x) {
+        const uint64_t bit = uint64_t(1) << x;
+        if ((placed & bit) || (pred[x] & ~placed)) continue;
+        const bool fits = SweepBuilder::is_diag(*ops[x]) || (ops[x]->target_mask() & ~R) == 0;
+        if (!fits) continue;
+        placed |= bit;
+        order.push_back(ops[x]);
+        progress = true;
+      }
+      if (progress) continue;
+      // Open the register set to the ready op that adds the fewest bits.
+      int best = -1, best_new = 99;
+      for (size_t x = 0; x < N; ++x) {
+        const uint64_t bit = uint64_t(1) << x;
+        if ((placed & bit) || (pred[x] & ~placed)) continue;
+        const uint64_t T = ops[x]->target_mask();
+        if (popc64(R | T) > int(reg_bits)) continue;
+        const int nb = popc64(T & ~R);
+        if (nb < best_new) best_new = nb, best = int(x);
+      }
+      if (best < 0) break;
+      R |= ops[size_t(best)]->target_mask();
+    }
+    phase_regs.push_back(R);
+  }
+}
+
 }  // namespace
 
 std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t n,
@@ -328,8 +462,11 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
   const uint32_t m = std::min<uint32_t>(opt.tile_bits, n);
   if (m < uint32_t(kRegBits) || m > uint32_t(kMaxTileBits))
     throw std::invalid_argument("tile bits out of range");
-  const uint32_t l = uint32_t(sweep_low_bits(int(m)));
+  const uint32_t l = opt.low_bits ? opt.low_bits : uint32_t(sweep_low_bits(int(m)));
+  if (l + opt.reg_bits > m) throw std::invalid_argument("low bits leave no register set free");
   const size_t kWindow = 256;  // lookahead when reordering
+  const bool select =
+      opt.reorder && (opt.select == 1 || (opt.select < 0 && n >= kSelectMinQubits && n > m));
 
   std::vector<const HostOp *> rem;
   for (const auto &o : ops) rem.push_back(&o);
@@ -353,6 +490,82 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
     SweepBuilder sb(n, m, l);
     sb.reg_bits = opt.reg_bits;
     sb.max_dense_k = std::min<uint32_t>(opt.max_dense_k, opt.reg_bits);
+    if (select) {
+      // Tile bits chosen up front; gates that fit them (or grow them while
+      // there is room) are collected in circuit order, then scheduled.
+      uint64_t S = select_tile(rem, head, n, m, l, opt, kWindow);
+      if (absorbed(rem, head, S, n, opt, kWindow) == 0) S = ((uint64_t(1) << l) - 1) | first.target_mask();
+      std::vector<const HostOp *> chosen;
+      std::vector<size_t> chosen_idx, skipped_idx;
+      uint64_t blockT = 0, blockAll = 0;
+      uint32_t ncoef = 0, ninner = 0;
+      size_t i = head;
+      for (; i < rem.size(); ++i) {
+        const HostOp &op = *rem[i];
+        const uint64_t T = op.nondiag_mask(), A = op.touched_mask();
+        const bool commutes = (T & blockAll) == 0 && (A & blockT) == 0;
+        const bool diag = SweepBuilder::is_diag(op);
+        const uint32_t c = SweepBuilder::coef_count(op);
+        const bool fits = fusable_size(op, opt) &&
+                          (diag || uint32_t(popc64(S | op.target_mask())) <= m) &&
+                          chosen.size() < size_t(kMaxOps) && ncoef + c <= uint32_t(kMaxCoef) &&
+                          !(op.kind == kOpInner && ninner >= uint32_t(kMaxInner));
+        if (commutes && fits) {
+          if (!diag) S |= op.target_mask();
+          chosen.push_back(&op);
+          chosen_idx.push_back(i);
+          ncoef += c;
+          if (op.kind == kOpInner) ++ninner;
+          if (chosen.size() >= size_t(kMaxOps)) {
+            ++i;
+            break;
+          }
+          continue;
+        }
+        skipped_idx.push_back(i);
+        blockT |= T;
+        blockAll |= A;
+        if (skipped_idx.size() >= kWindow || popc64(blockT) >= int(n)) {
+          ++i;
+          break;
+        }
+      }
+      if (chosen.empty()) throw std::logic_error("planner: empty sweep");
+      std::vector<const HostOp *> order;
+      schedule_phases(chosen, sb.reg_bits, order, sb.phase_regs, sb.phase_first);
+      // More phases than a sweep holds: the ops of the excess phases go back
+      // to the queue (every op they precede is among them).
+      std::vector<size_t> back_idx;
+      if (sb.phase_regs.size() > size_t(kMaxPhases)) {
+        const size_t keep = sb.phase_first[kMaxPhases];
+        for (size_t x = keep; x < order.size(); ++x) {
+          const size_t pos = size_t(std::find(chosen.begin(), chosen.end(), order[x]) - chosen.begin());
+          back_idx.push_back(chosen_idx[pos]);
+        }
+        order.resize(keep);
+        sb.phase_regs.resize(kMaxPhases);
+        sb.phase_first.resize(kMaxPhases);
+      }
+      sb.S = S;
+      sb.ops = order;
+      for (const HostOp *op : order) {
+        sb.ncoef += SweepBuilder::coef_count(*op);
+        if (op->kind == kOpInner) ++sb.ninner;
+      }
+      PlannedLaunch pl;
+      pl.is_sweep = true;
+      pl.sweep = sb.finish();
+      out.push_back(std::move(pl));
+      std::vector<size_t> again(skipped_idx);
+      again.insert(again.end(), back_idx.begin(), back_idx.end());
+      std::sort(again.begin(), again.end());
+      std::vector<const HostOp *> next;
+      for (size_t x : again) next.push_back(rem[x]);
+      next.insert(next.end(), rem.begin() + i, rem.end());
+      rem.swap(next);
+      head = 0;
+      continue;
+    }
     std::vector<const HostOp *> skipped;
     uint64_t blockT = 0, blockAll = 0;  // non-diagonal / all bits of skipped gates
     size_t i = head;

@@ -21,7 +21,8 @@ def lib():
 
 def run(state, n, gates, tile_bits=12, reorder=True):
     """gates: list of (matrix, qubits, controls, control_values). Returns
-    (state, sweeps, unfused)."""
+    (state, sweeps, unfused).  reorder: False/True, or "select" / "noselect"
+    to force tile selection on / off."""
     psi = np.array(state, dtype=np.complex128)
     k, qoff, qs, nc, coff, cs, cv, moff, mats = [], [], [], [], [], [], [], [], []
     mo = 0
@@ -36,13 +37,17 @@ def run(state, n, gates, tile_bits=12, reorder=True):
     unf = ctypes.c_int(0)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     r = lib().emu_run(P(psi), n, len(gates), P(K), P(QO), P(QS), P(NC), P(CO), P(CS), P(CV),
-                      P(MO), P(M), tile_bits, int(reorder), ctypes.byref(unf))
+                      P(MO), P(M), tile_bits, _reorder_code(reorder), ctypes.byref(unf))
     if r < 0:
         raise RuntimeError("emulator failed")
     return psi, r, unf.value
 
 
-def plan_stats(n, gates, tile_bits=12, reorder=True):
+def _reorder_code(reorder):
+    return {"select": 2, "noselect": 3}.get(reorder, int(bool(reorder)))
+
+
+def plan_stats(n, gates, tile_bits=12, reorder=True, low_bits=0):
     """{sweeps, phases, ops, kinds{...}, unfused} of the engine's plan."""
     k, qoff, qs, nc, coff, cs, cv, moff, mats = [], [], [], [], [], [], [], [], []
     mo = 0
@@ -57,14 +62,14 @@ def plan_stats(n, gates, tile_bits=12, reorder=True):
     out = np.zeros(10, dtype=np.int64)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     if lib().emu_plan_stats(n, len(gates), P(K), P(QO), P(QS), P(NC), P(CO), P(CS), P(CV),
-                            P(MO), P(M), tile_bits, int(reorder), P(out)) != 0:
+                            P(MO), P(M), tile_bits, _reorder_code(reorder), low_bits, P(out)) != 0:
         raise RuntimeError("planner failed")
     names = ["dense", "diag", "anti1", "xrot", "swap2", "phase"]
     return {"sweeps": int(out[0]), "phases": int(out[1]), "ops": int(out[2]),
             "kinds": {names[i]: int(out[3 + i]) for i in range(6)}, "unfused": int(out[9])}
 
 
-def adjoint(n, ops, terms, nparams, tile_bits=10):
+def adjoint(n, ops, terms, nparams, tile_bits=10, select=-1):
     """(energy, grad, sweeps) from the host emulation of the adjoint plan."""
     from snuqs_b200 import capi
     arr, keep = capi.circuit_ops(ops)
@@ -74,10 +79,10 @@ def adjoint(n, ops, terms, nparams, tile_bits=10):
     g = np.zeros(max(1, nparams), dtype=np.float64)
     lib().emu_adjoint.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p,
                                   ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
-                                  ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+                                  ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
     r = lib().emu_adjoint(n, ctypes.cast(arr, ctypes.c_void_p), len(ops), flat,
                           w.ctypes.data_as(ctypes.c_void_p), len(terms), nparams, tile_bits,
-                          ctypes.byref(e), g.ctypes.data_as(ctypes.c_void_p))
+                          select, ctypes.byref(e), g.ctypes.data_as(ctypes.c_void_p))
     if r < 0:
         raise RuntimeError("emulated adjoint failed")
     return e.value, g[:nparams], r

@@ -268,6 +268,8 @@ int emu_run(double *state, int n, int nops, const int *k, const int *qoff, const
     PlanOptions opt;
     opt.tile_bits = uint32_t(tile_bits);
     opt.reorder = reorder != 0;
+    // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection
+    opt.select = reorder == 2 ? 1 : reorder == 3 ? 0 : -1;
     auto plan = plan_sweeps(ops, uint32_t(n), opt);
     int sweeps = 0, unfused = 0;
     cplx *psi = reinterpret_cast<cplx *>(state);
@@ -295,7 +297,7 @@ extern "C" {
 int emu_plan_stats(int n, int nops, const int *k, const int *qoff, const int *qubits,
                    const int *nc, const int *coff, const int *controls, const int *cvals,
                    const long *moff, const double *mats, int tile_bits, int reorder,
-                   long *out) {
+                   int low_bits, long *out) {
   try {
     std::vector<HostOp> ops;
     for (int i = 0; i < nops; ++i) {
@@ -316,6 +318,9 @@ int emu_plan_stats(int n, int nops, const int *k, const int *qoff, const int *qu
     PlanOptions opt;
     opt.tile_bits = uint32_t(tile_bits);
     opt.reorder = reorder != 0;
+    // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection
+    opt.select = reorder == 2 ? 1 : reorder == 3 ? 0 : -1;
+    opt.low_bits = uint32_t(low_bits);
     auto plan = plan_sweeps(ops, uint32_t(n), opt);
     for (int i = 0; i < 10; ++i) out[i] = 0;
     for (const auto &pl : plan) {
@@ -340,7 +345,7 @@ extern "C" {
 // two-state sweeps).  Returns the number of reverse sweeps, -1 on error.
 int emu_adjoint(int n, const sq_circuit_op *ops, uint32_t nops, const char *paulis,
                 const double *weights, uint32_t nterms, uint32_t nparams, int tile_bits,
-                double *energy, double *grad) {
+                int select, double *energy, double *grad) {
   try {
     AdjointPlan ap;
     build_adjoint(ops, nops, uint32_t(n), ap);
@@ -373,6 +378,7 @@ int emu_adjoint(int n, const sq_circuit_op *ops, uint32_t nops, const char *paul
     opt.tile_bits = uint32_t(tile_bits);
     opt.reg_bits = 3;
     opt.max_dense_k = 3;
+    opt.select = select;
     auto plan = plan_sweeps(ap.reverse, uint32_t(n), opt);
     std::vector<cplx> ip(ap.occurrences.size(), cplx(0, 0));
     int sweeps = 0;

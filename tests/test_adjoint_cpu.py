@@ -71,13 +71,14 @@ def random_param_circuit(n, ngates, nparams, seed):
     return ops
 
 
+@pytest.mark.parametrize("select,tile_bits", [(0, 10), (0, 7), (1, 7)])
 @pytest.mark.parametrize("n,seed", [(5, 0), (8, 1), (11, 2), (13, 3)])
-def test_adjoint_plan_matches_finite_differences(n, seed):
+def test_adjoint_plan_matches_finite_differences(n, seed, select, tile_bits):
     nparams = 6
     ops = random_param_circuit(n, 40, nparams, seed)
     theta = np.random.default_rng(seed + 100).uniform(-3, 3, nparams)
     terms = circuits.random_pauli_hamiltonian(n, 12, seed=seed)
-    e, g, sweeps = emulator.adjoint(n, bind(ops, theta), terms, nparams)
+    e, g, sweeps = emulator.adjoint(n, bind(ops, theta), terms, nparams, tile_bits=tile_bits, select=select)
     assert abs(e - energy(n, ops, theta, terms)) < 1e-12
     assert np.abs(g - fd_grad(n, ops, theta, terms)).max() < 1e-8
 

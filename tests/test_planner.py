@@ -15,12 +15,12 @@ def gates_of(ops):
 
 
 @pytest.mark.parametrize("n", [4, 5, 7, 9, 11, 12, 13, 15])
-@pytest.mark.parametrize("reorder", [True, False])
+@pytest.mark.parametrize("reorder", [True, False, "select", "noselect"])
 def test_plans_match_oracle_all_gates(n, reorder):
     for seed in range(2):
         ops = circuits.random_all_gates(n, 120, seed=seed)
         ref = oracle.run_ops(ops, n)
-        for tb in (12, 9):
+        for tb in (12, 9, 7):
             psi, sweeps, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops), tb, reorder)
             assert np.abs(psi - ref).max() <= 1e-12, (n, seed, tb)
 
@@ -62,9 +62,30 @@ def test_controls_and_large_unitaries():
         blk = cidx << len(q)
         full[blk:blk + (1 << len(q)), blk:blk + (1 << len(q))] = u
         oracle.apply_matrix(ref, n, full, list(c) + list(q))
-    psi, sweeps, unfused = emulator.run(psi0, n, gates)
-    assert np.abs(psi - ref).max() <= 1e-12
-    assert unfused > 0
+    for reorder in (True, "select"):
+        psi, sweeps, unfused = emulator.run(psi0, n, gates, 9, reorder)
+        assert np.abs(psi - ref).max() <= 1e-12
+        assert unfused > 0
+
+
+def test_tile_selection_and_phase_scheduling_reduce_work():
+    n = 24
+    g = gates_of(circuits.random_mix(n, 400, seed=77))
+    plain = emulator.plan_stats(n, g, tile_bits=11, reorder="noselect")
+    sel = emulator.plan_stats(n, g, tile_bits=11, reorder="select")
+    assert sel["ops"] == plain["ops"] == 400
+    assert sel["sweeps"] < plain["sweeps"]
+    assert sel["phases"] < 0.85 * plain["phases"]
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_selected_plans_match_oracle_on_larger_states(seed):
+    n = 16
+    ops = circuits.random_all_gates(n, 300, seed=40 + seed)
+    ref = oracle.run_ops(ops, n)
+    for tb in (7, 9, 11):
+        psi, _, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops), tb, "select")
+        assert np.abs(psi - ref).max() <= 1e-12, tb
 
 
 def test_diagonal_and_identity_gates_fold():
