@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--tile-bits", type=int, default=0, help="override the engine's tile size")
+    p.add_argument("--low-bits", type=int, default=0,
+                   help="override the contiguous low bits of every tile")
     return p.parse_args()
 
 
@@ -249,6 +251,8 @@ def _run_ours(args, rank, world, local):
     st.init_basis(0)
     if args.tile_bits:
         st.set_option(capi.SQ_OPT_TILE_BITS, args.tile_bits)
+    if args.low_bits:
+        st.set_option(capi.SQ_OPT_LOW_BITS, args.low_bits)
 
     def step():
         for op, m in zip(ops, mats):

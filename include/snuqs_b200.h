@@ -66,8 +66,12 @@ typedef enum {
   SQ_OPT_TILE_BITS = 1, /* log2 amplitudes per shared-memory tile (4..12; default 12) */
   SQ_OPT_REORDER = 2,   /* 1 (default): the planner may absorb later gates that commute */
   SQ_OPT_TIMING = 3,    /* 1: record a CUDA event pair around every fused-sweep launch */
-  SQ_OPT_JIT = 4        /* -1 (default): JIT-specialised sweep kernels for states of >= 20
+  SQ_OPT_JIT = 4,       /* -1 (default): JIT-specialised sweep kernels for states of >= 20
                            qubits when NVRTC is present; 1: always; 0: never */
+  SQ_OPT_LOW_BITS = 5   /* contiguous low index bits in every tile (each global access
+                           covers runs of 2^value amplitudes); 0 (default): 3 for
+                           complex128, 4 for complex64 (128-byte runs) when the state
+                           spans several tiles; ignored unless value + 4 <= tile bits */
 } sq_option;
 
 /* ---- library / device ------------------------------------------------ */

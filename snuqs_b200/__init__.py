@@ -8,20 +8,15 @@
   reference's Python driver layer for the no-offload CUDA path.
 
 The native libraries are built in-tree by ``python -m snuqs_b200.build``.
-Importing the package without them raises: the engine has no CPU fallback.
+Without them every engine entry point raises (``import snuqs_b200._C`` fails,
+``capi.lib()`` raises ImportError): the engine has no CPU fallback.  The
+package itself imports without them so that the build module can run.
 """
 from __future__ import annotations
 
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-
-try:
-    from . import _C  # noqa: F401
-except ImportError as e:  # pragma: no cover - exercised only on a broken install
-    raise ImportError(
-        "snuqs_b200 native extension not built (run `python -m snuqs_b200.build`): " + str(e)
-    ) from e
 
 __version__ = "0.1.0"
 LIB_PATH = os.path.join(_HERE, "libsnuqs_b200.so")

@@ -298,12 +298,22 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
     << ")\nsq_jit_sweep(Vec2<" << R << ">::T *__restrict__ psi, const __grid_constant__ SweepParams<"
     << R << "> P) {\n";
   s << "  using C2 = Vec2<" << R << ">::T;\n";
-  s << "  jit_sweep<" << R << ", " << M
+  // Coefficients come from the parameter block, except for diagonal ops
+  // indexed by tile bits that differ across the lanes (shared-memory copy).
+  auto lane_indexed = [](const SweepOp &op) {
+    if (op.kind != kSwDiag) return false;
+    for (int t = 0; t < op.ndt; ++t)
+      if (op.dsrc[t] != kSrcGlobal) return true;
+    return false;
+  };
+  bool smem_coef = false;
+  for (const SweepOp &op : ps.op) smem_coef |= lane_indexed(op);
+  s << "  jit_sweep<" << R << ", " << M << ", " << ps.h.l << ", " << (smem_coef ? "true" : "false")
     << ">(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase, const uint64_t *hitab) {\n";
   const uint32_t last = ps.h.nphases - 1;
   for (uint32_t p = 0; p < ps.h.nphases; ++p) {
     const SweepPhase &ph = ps.ph[p];
-    s << "    {\n      using Ph = JitPhase<" << R << ", " << M << ", " << int(ph.reg[0]) << ", "
+    s << "    {\n      using Ph = JitPhase<" << R << ", " << M << ", " << ps.h.l << ", " << int(ph.reg[0]) << ", "
       << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]);
     for (int t : thread_positions(ph, M, c64, p == last && (ps.h.flags & kDirectStore))) s << ", " << t;
     s << ">;\n";
@@ -323,6 +333,11 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
       }
       std::string tmpl;
       op_routine(op, c64, tmpl);
+      std::ostringstream cexpr;
+      if (lane_indexed(op))
+        cexpr << "coef + " << op.coef;
+      else
+        cexpr << "ParamCoef<" << R << ", " << op.coef << ">{P.coef}";
       if (op.kind == kSwDiag) {
         s << "{ uint32_t b = 0;";
         for (int t = 0; t < op.ndt; ++t) {
@@ -331,9 +346,9 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
           else
             s << " b = (b << 1) | ((jb >> " << int(op.dpos[t]) << ") & 1u);";
         }
-        s << " " << tmpl << "(A, coef + " << op.coef << ", b); }\n";
+        s << " " << tmpl << "(A, " << cexpr.str() << ", b); }\n";
       } else {
-        s << tmpl << "(A, coef + " << op.coef << ", " << int(op.rmask) << ", " << int(op.rval)
+        s << tmpl << "(A, " << cexpr.str() << ", " << int(op.rmask) << ", " << int(op.rval)
           << ");\n";
       }
     }

@@ -146,8 +146,8 @@ __device__ __forceinline__ void cmul(Real pr, Real pi, Real ar, Real ai, Real &o
 }
 
 // kSwDense on register positions V: row r accumulated left to right.
-template <typename Real, int NA, int V>
-__device__ __forceinline__ void op_dense(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, class CP>
+__device__ __forceinline__ void op_dense(Amps<Real, NA> &A, CP c,
                                          int rmask, int rval) {
   constexpr int D = 1 << ct_popc<V>();
   for_groups<NA, V>(rmask, rval, [&](int g) {
@@ -177,8 +177,8 @@ __device__ __forceinline__ void op_dense(Amps<Real, NA> &A, const typename Vec2<
 }
 
 // kSwAnti1 on register bit V: out0 = p0 a1, out1 = p1 a0 (a swap when pure).
-template <typename Real, int NA, int V, bool PURE>
-__device__ __forceinline__ void op_anti1(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, bool PURE, class CP>
+__device__ __forceinline__ void op_anti1(Amps<Real, NA> &A, CP c,
                                          int rmask, int rval) {
   if constexpr (PURE) {
     for_groups<NA, V>(rmask, rval, [&](int g) {
@@ -200,8 +200,8 @@ __device__ __forceinline__ void op_anti1(Amps<Real, NA> &A, const typename Vec2<
 
 // kSwXRot on register positions V with partner mask X (canonical local bits):
 // out_r = c_r a_r + f s_r a_(r^X).
-template <typename Real, int NA, int V, int X, bool IMAG>
-__device__ __forceinline__ void op_xrot(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, int X, bool IMAG, class CP>
+__device__ __forceinline__ void op_xrot(Amps<Real, NA> &A, CP c,
                                         int rmask, int rval) {
   constexpr int D = 1 << ct_popc<V>();
   Real cr[D], sr[D];
@@ -236,8 +236,8 @@ __device__ __forceinline__ void op_xrot(Amps<Real, NA> &A, const typename Vec2<R
 }
 
 // kSwSwap2 on register positions V (two bits): out1 = p12 a2, out2 = p21 a1.
-template <typename Real, int NA, int V, bool PURE>
-__device__ __forceinline__ void op_swap2(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, bool PURE, class CP>
+__device__ __forceinline__ void op_swap2(Amps<Real, NA> &A, CP c,
                                          int rmask, int rval) {
   constexpr int B1 = ct_dep<V>(1), B2 = ct_dep<V>(2);
   if constexpr (PURE) {
@@ -259,21 +259,21 @@ __device__ __forceinline__ void op_swap2(Amps<Real, NA> &A, const typename Vec2<
 }
 
 // kSwDiag: coefficient index = thread part << popc(V) | register part.
-template <typename Real, int NA, int V>
-__device__ __forceinline__ void op_diag(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, int V, class CP>
+__device__ __forceinline__ void op_diag(Amps<Real, NA> &A, CP c,
                                         uint32_t base) {
-  const auto *cb = c + (base << ct_popc<V>());
+  const uint32_t cb = base << ct_popc<V>();
 #pragma unroll
   for (int ri = 0; ri < NA; ++ri) {
-    const auto d = cb[ct_ext<V>(ri)];
+    const auto d = c[cb + ct_ext<V>(ri)];
     const Real r = A.re[ri], i = A.im[ri];
     cmul(d.x, d.y, r, i, A.re[ri], A.im[ri]);
   }
 }
 
 // kSwPhase: a *= p on the register slots whose bits match (rmask, rval).
-template <typename Real, int NA, bool NEG>
-__device__ __forceinline__ void op_phase(Amps<Real, NA> &A, const typename Vec2<Real>::T *__restrict__ c,
+template <typename Real, int NA, bool NEG, class CP>
+__device__ __forceinline__ void op_phase(Amps<Real, NA> &A, CP c,
                                          int rmask, int rval) {
   if constexpr (NEG) {
 #pragma unroll
@@ -394,12 +394,13 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
                  const __grid_constant__ SweepParams<Real> P) {
   using C2 = typename Vec2<Real>::T;
   constexpr int NT = 1 << (M - kRegBits);
-  constexpr int L = sweep_low_bits(M);
   constexpr uint32_t TS = 1u << M;
   constexpr uint32_t PER = TS / NT;  // amplitudes each thread copies per tile
-  constexpr uint32_t LOWMASK = (1u << L) - 1u;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SweepHeader &h = P.h;
+  // Low contiguous bits: the plan's (every tile holds runs of 2^L amplitudes).
+  const uint32_t L = h.l;
+  const uint32_t LOWMASK = (1u << L) - 1u;
   C2 *bufs = reinterpret_cast<C2 *>(smem_raw);
   C2 *coef = bufs + 2 * TS;
   uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + ((h.ncoef + 1) & ~1u));
@@ -413,15 +414,14 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
   }
   for (uint32_t c = tid; c < (1u << (M - L)); c += NT) {
     uint64_t a = 0;
-#pragma unroll
-    for (int i = 0; i < M - L; ++i)
+    for (uint32_t i = 0; i < M - L; ++i)
       if ((c >> i) & 1) a |= uint64_t(1) << h.hi[i];
     hitab[c] = a;
   }
   __syncthreads();
 
-  // Element j = it * NT + tid of a tile; for M >= 9 the lanes of a warp cover
-  // 32 contiguous amplitudes of one chunk.
+  // Element j = it * NT + tid of a tile; consecutive lanes cover runs of 2^L
+  // contiguous amplitudes.
   const uint32_t s_tid = swz<Real>(tid);
   auto prefetch = [&](uint64_t t, C2 *dst) {
     const uint64_t gb = tile_base(t, h);
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
         // Global index of register slot ri = tbase | selected register-bit
         // weights (disjoint bits).
         auto gw = [&](uint32_t pos) -> uint64_t {
-          return pos < uint32_t(L) ? (uint64_t(1) << pos) : (uint64_t(1) << h.hi[pos - L]);
+          return pos < L ? (uint64_t(1) << pos) : (uint64_t(1) << h.hi[pos - L]);
         };
         const uint64_t tbase = gbase | hitab[jb >> L] | (jb & LOWMASK);
         const uint64_t g0 = gw(ph.reg[0]), g1 = gw(ph.reg[1]), g2 = gw(ph.reg[2]), g3 = gw(ph.reg[3]);
@@ -516,10 +516,23 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
 // each phase compiles to straight-line code: no op dispatch, and no register
 // shuffling back to fixed registers between gates.
 // ---------------------------------------------------------------------------
-template <typename Real, int M, int R0, int R1, int R2, int R3, int... T>
+// Coefficients read straight from the kernel's parameter block (constant
+// bank) at compile-time offsets: no shared-memory load per coefficient, and
+// one compiled kernel still serves every coefficient value.
+template <typename Real, int OFF>
+struct ParamCoef {
+  const Real *p;  // SweepParams::coef
+  __device__ __forceinline__ typename Vec2<Real>::T operator[](uint32_t i) const {
+    typename Vec2<Real>::T v;
+    v.x = p[2 * (OFF + i)];
+    v.y = p[2 * (OFF + i) + 1];
+    return v;
+  }
+};
+
+template <typename Real, int M, int L, int R0, int R1, int R2, int R3, int... T>
 struct JitPhase {
   using C2 = typename Vec2<Real>::T;
-  static constexpr int L = sweep_low_bits(M);
   static_assert(sizeof...(T) == M - kRegBits, "one tile position per thread bit");
   // Thread bit i sits on tile position T[i]: the code generator places the
   // lane bits that share a shared-memory wavefront on positions whose swizzle
@@ -576,12 +589,13 @@ struct JitPhase {
 
 // The tile loop of sweep_kernel with the phases supplied by the generated
 // kernel: phases(tile, coef, gbase, hitab) runs every phase of one tile.
-template <typename Real, int M, class Phases>
+// SMEM_COEF: the phases also read coefficients from shared memory (diagonal
+// ops indexed by tile bits that vary across the lanes).
+template <typename Real, int M, int L, bool SMEM_COEF, class Phases>
 __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ psi,
                                           const SweepParams<Real> &P, Phases phases) {
   using C2 = typename Vec2<Real>::T;
   constexpr int NT = 1 << (M - kRegBits);
-  constexpr int L = sweep_low_bits(M);
   constexpr uint32_t TS = 1u << M;
   constexpr uint32_t PER = TS / NT;
   constexpr uint32_t LOWMASK = (1u << L) - 1u;
@@ -591,12 +605,13 @@ __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ p
   C2 *coef = bufs + 2 * TS;
   uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + ((h.ncoef + 1) & ~1u));
   const uint32_t tid = threadIdx.x;
-  for (uint32_t i = tid; i < h.ncoef; i += NT) {
-    C2 v;
-    v.x = P.coef[2 * i];
-    v.y = P.coef[2 * i + 1];
-    coef[i] = v;
-  }
+  if constexpr (SMEM_COEF)
+    for (uint32_t i = tid; i < h.ncoef; i += NT) {
+      C2 v;
+      v.x = P.coef[2 * i];
+      v.y = P.coef[2 * i + 1];
+      coef[i] = v;
+    }
   for (uint32_t c = tid; c < (1u << (M - L)); c += NT) {
     uint64_t a = 0;
 #pragma unroll

@@ -19,7 +19,7 @@ def lib():
     return _lib
 
 
-def run(state, n, gates, tile_bits=12, reorder=True):
+def run(state, n, gates, tile_bits=12, reorder=True, low_bits=0):
     """gates: list of (matrix, qubits, controls, control_values). Returns
     (state, sweeps, unfused).  reorder: False/True, or "select" / "noselect"
     to force tile selection on / off."""
@@ -37,7 +37,8 @@ def run(state, n, gates, tile_bits=12, reorder=True):
     unf = ctypes.c_int(0)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     r = lib().emu_run(P(psi), n, len(gates), P(K), P(QO), P(QS), P(NC), P(CO), P(CS), P(CV),
-                      P(MO), P(M), tile_bits, _reorder_code(reorder), ctypes.byref(unf))
+                      P(MO), P(M), tile_bits, _reorder_code(reorder), low_bits,
+                      ctypes.byref(unf))
     if r < 0:
         raise RuntimeError("emulator failed")
     return psi, r, unf.value
@@ -48,7 +49,9 @@ def _reorder_code(reorder):
 
 
 def plan_stats(n, gates, tile_bits=12, reorder=True, low_bits=0):
-    """{sweeps, phases, ops, kinds{...}, unfused} of the engine's plan."""
+    """{sweeps, phases, ops, kinds{...}, unfused, direct_load, direct_store}
+    of the engine's plan (the last two count sweeps whose first / last phase
+    leaves the low tile bits to the lanes)."""
     k, qoff, qs, nc, coff, cs, cv, moff, mats = [], [], [], [], [], [], [], [], []
     mo = 0
     for m, q, c, v in gates:
@@ -59,14 +62,15 @@ def plan_stats(n, gates, tile_bits=12, reorder=True, low_bits=0):
     K, QO, QS, NC, CO, CS, CV = (arr(x, np.int32) for x in (k, qoff, qs, nc, coff, cs, cv))
     MO = arr(moff, np.int64)
     M = np.ascontiguousarray(np.concatenate(mats))
-    out = np.zeros(10, dtype=np.int64)
+    out = np.zeros(12, dtype=np.int64)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     if lib().emu_plan_stats(n, len(gates), P(K), P(QO), P(QS), P(NC), P(CO), P(CS), P(CV),
                             P(MO), P(M), tile_bits, _reorder_code(reorder), low_bits, P(out)) != 0:
         raise RuntimeError("planner failed")
     names = ["dense", "diag", "anti1", "xrot", "swap2", "phase"]
     return {"sweeps": int(out[0]), "phases": int(out[1]), "ops": int(out[2]),
-            "kinds": {names[i]: int(out[3 + i]) for i in range(6)}, "unfused": int(out[9])}
+            "kinds": {names[i]: int(out[3 + i]) for i in range(6)}, "unfused": int(out[9]),
+            "direct_load": int(out[10]), "direct_store": int(out[11])}
 
 
 def adjoint(n, ops, terms, nparams, tile_bits=10, select=-1):

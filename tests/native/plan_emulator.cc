@@ -247,7 +247,7 @@ extern "C" {
 int emu_run(double *state, int n, int nops, const int *k, const int *qoff, const int *qubits,
             const int *nc, const int *coff, const int *controls, const int *cvals,
             const long *moff, const double *mats, int tile_bits, int reorder,
-            int *unfused_out) {
+            int low_bits, int *unfused_out) {
   try {
     std::vector<HostOp> ops;
     for (int i = 0; i < nops; ++i) {
@@ -270,6 +270,7 @@ int emu_run(double *state, int n, int nops, const int *k, const int *qoff, const
     opt.reorder = reorder != 0;
     // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection
     opt.select = reorder == 2 ? 1 : reorder == 3 ? 0 : -1;
+    opt.low_bits = uint32_t(low_bits);
     auto plan = plan_sweeps(ops, uint32_t(n), opt);
     int sweeps = 0, unfused = 0;
     cplx *psi = reinterpret_cast<cplx *>(state);
@@ -322,13 +323,15 @@ int emu_plan_stats(int n, int nops, const int *k, const int *qoff, const int *qu
     opt.select = reorder == 2 ? 1 : reorder == 3 ? 0 : -1;
     opt.low_bits = uint32_t(low_bits);
     auto plan = plan_sweeps(ops, uint32_t(n), opt);
-    for (int i = 0; i < 10; ++i) out[i] = 0;
+    for (int i = 0; i < 12; ++i) out[i] = 0;
     for (const auto &pl : plan) {
       if (!pl.is_sweep) {
         out[9]++;
         continue;
       }
       out[0]++;
+      if (pl.sweep.h.flags & kDirectLoad) out[10]++;
+      if (pl.sweep.h.flags & kDirectStore) out[11]++;
       out[1] += pl.sweep.h.nphases;
       out[2] += long(pl.sweep.op.size());
       for (const auto &o : pl.sweep.op) out[2 + o.kind]++;

@@ -22,10 +22,11 @@ def _gpu(cuda_required):
     yield
 
 
-def run(ops, n, dtype=capi.SQ_C128, jit=1, psi0=None, tile_bits=12):
+def run(ops, n, dtype=capi.SQ_C128, jit=1, psi0=None, tile_bits=12, low_bits=0):
     st = capi.State(n, dtype)
     st.set_option(capi.SQ_OPT_JIT, jit)
     st.set_option(capi.SQ_OPT_TILE_BITS, tile_bits)
+    st.set_option(capi.SQ_OPT_LOW_BITS, low_bits)
     if psi0 is None:
         st.init_basis(0)
     else:
@@ -85,3 +86,24 @@ def test_cached_kernel_serves_new_angles():
     a = run(ops2, n, jit=1)
     b = run(ops2, n, jit=0)
     assert np.abs(a - b).max() <= 1e-13
+
+
+@pytest.mark.parametrize("jit", [0, 1])
+@pytest.mark.parametrize("low_bits", [2, 3, 4])
+def test_low_bits_against_oracle(jit, low_bits):
+    n = 16
+    ops = circuits.random_all_gates(n, 250, seed=200 + low_bits)
+    ref = oracle.run_ops(ops, n)
+    got = run(ops, n, capi.SQ_C128, jit=jit, tile_bits=11, low_bits=low_bits)
+    assert np.abs(got - ref).max() <= TOL128
+    got = run(ops, n, capi.SQ_C64, jit=jit, tile_bits=12, low_bits=low_bits)
+    assert np.abs(got - ref).max() <= TOL64
+
+
+@pytest.mark.parametrize("dtype", [capi.SQ_C128, capi.SQ_C64])
+def test_low_bits_large_state_matches_default(dtype):
+    n = 24
+    ops = circuits.random_mix(n, 300, seed=23)
+    a = run(ops, n, dtype, jit=1, low_bits=5)
+    b = run(ops, n, dtype, jit=0)
+    assert np.abs(a - b).max() <= (1e-13 if dtype == capi.SQ_C128 else 1e-6)

@@ -91,7 +91,7 @@ def test_lane_placement_is_a_permutation_and_conflict_free(dtype):
         body = src[src.rindex("sq_jit_sweep"):]
         for args in re.findall(r"JitPhase<\w+, ([\d, ]+)>", body):
             vals = [int(x) for x in args.split(",")]
-            m, regs, threads = vals[0], vals[1:5], vals[5:]
+            m, regs, threads = vals[0], vals[2:6], vals[6:]
             assert sorted(regs + threads) == list(range(m))
             phases += 1
             conflict_free += _rank([img[p] for p in threads[:W]]) == W

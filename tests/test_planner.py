@@ -88,6 +88,16 @@ def test_selected_plans_match_oracle_on_larger_states(seed):
         assert np.abs(psi - ref).max() <= 1e-12, tb
 
 
+@pytest.mark.parametrize("low_bits", [1, 2, 3, 4, 6])
+def test_low_bit_counts_match_oracle(low_bits):
+    n = 15
+    ops = circuits.random_all_gates(n, 200, seed=60 + low_bits)
+    ref = oracle.run_ops(ops, n)
+    for tb, ro in ((11, "select"), (10, True), (12, "noselect")):
+        psi, _, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops), tb, ro, low_bits)
+        assert np.abs(psi - ref).max() <= 1e-12, (tb, ro)
+
+
 def test_diagonal_and_identity_gates_fold():
     n = 10
     ops = [("Hadamard", (q,), ()) for q in range(n)]
