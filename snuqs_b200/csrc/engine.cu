@@ -258,17 +258,20 @@ static int launch_sweep(sq_state *s, const sq::PlannedSweep &ps, cudaStream_t st
                       (size_t(1) << (m - l)) * sizeof(uint64_t);
   int per_sm = 0;
   const void *fn = nullptr;
+  size_t launch_smem = smem;
   if (use_jit(s)) {
     std::string err;
+    const size_t jsmem = sq::jit_smem(ps, sizeof(Real) == 4);
     fn = sq::jit_sweep_kernel(ps, sizeof(Real) == 4, err);
-    if (fn && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
+    if (fn && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(jsmem)) != cudaSuccess) {
       cudaGetLastError();
       fn = nullptr;
     }
-    if (fn && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
+    if (fn && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, jsmem) != cudaSuccess) {
       cudaGetLastError();
       per_sm = sq::jit_minb(sizeof(Real) == 4, m);
     }
+    if (fn) launch_smem = jsmem;
     sq::jit_note_launch(fn != nullptr);
   }
   if (!fn) {
@@ -286,7 +289,7 @@ static int launch_sweep(sq_state *s, const sq::PlannedSweep &ps, cudaStream_t st
   }
   C2 *psi = reinterpret_cast<C2 *>(s->data);
   void *args[] = {&psi, P.get()};
-  SQ_CUDA(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(threads), args, smem, st));
+  SQ_CUDA(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(threads), args, launch_smem, st));
   SQ_CUDA(cudaGetLastError());
   if (s->timing) {
     SQ_CUDA(cudaEventRecord(e1, st));
@@ -442,11 +445,13 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
     if (opt.tile_bits < uint32_t(sq::kRegBits)) return fail(SQ_ERR_INVALID, "internal: no tile size");
     opt.reorder = s->reorder != 0;
     opt.max_dense_k = c64 ? 4 : 3;
-    // Runs of 128 bytes (8 complex128 / 16 complex64 amplitudes) leave the
-    // planner more free tile bits than 512-byte runs and still read whole
-    // cache lines; measured faster on B200 for multi-tile states.
-    const uint32_t lb = s->low_bits ? s->low_bits : (n > opt.tile_bits ? (c64 ? 4u : 3u) : 0u);
-    if (lb && lb + uint32_t(sq::kRegBits) <= opt.tile_bits) opt.low_bits = lb;
+    // Runs of 128 bytes leave the planner more free tile bits than 512-byte
+    // runs and still read whole cache lines; measured faster on B200 for
+    // multi-tile states.
+    if (s->low_bits && s->low_bits + uint32_t(sq::kRegBits) <= opt.tile_bits)
+      opt.low_bits = s->low_bits;
+    else
+      opt.low_bits = sq::auto_low_bits(c64, n, opt.tile_bits);
     plan = sq::plan_sweeps(ops, n, opt);
   } catch (const std::exception &e) {
     return fail(SQ_ERR_INVALID, "planner: %s", e.what());

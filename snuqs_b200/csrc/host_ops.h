@@ -86,6 +86,14 @@ struct PlanOptions {
 };
 constexpr uint32_t kSelectMinQubits = 18;
 
+// Low bits the engine plans with by default: runs of 128 bytes (8 complex128
+// / 16 complex64 amplitudes) when the state spans several tiles of m bits;
+// 0 (the planner's own default) otherwise.
+inline uint32_t auto_low_bits(bool c64, uint32_t n, uint32_t m) {
+  const uint32_t lb = n > m ? (c64 ? 4u : 3u) : 0u;
+  return lb && lb + uint32_t(kRegBits) <= m ? lb : 0u;
+}
+
 // Packs ops (in circuit order) into fused sweeps for an n-qubit state.
 std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t n,
                                        const PlanOptions &opt);

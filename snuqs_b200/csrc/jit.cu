@@ -290,35 +290,65 @@ std::vector<int> thread_positions(const SweepPhase &ph, int m, bool c64, bool di
   return out;
 }
 
+// Diagonal op whose coefficient index depends on tile bits that differ across
+// the lanes: its coefficients are read from a shared-memory copy (a
+// lane-divergent read of the parameter block would serialise).
+bool lane_indexed(const SweepOp &op) {
+  if (op.kind != kSwDiag) return false;
+  for (int t = 0; t < op.ndt; ++t)
+    if (op.dsrc[t] != kSrcGlobal) return true;
+  return false;
+}
+
+struct JitShape {
+  bool smem_coef = false, dload = false, dstore = false;
+};
+
+// Direct loads (first phase from HBM, no prefetch into a second tile buffer)
+// measured faster on B200 for complex128 (7.10 vs 7.38 ms per 30-qubit sweep)
+// and slightly slower for complex64 (3.86 vs 3.76 ms); SQ_JIT_DLOAD=0/1
+// overrides the choice for both precisions.
+JitShape jit_shape(const PlannedSweep &ps, bool c64) {
+  static const int dload_env = [] {
+    const char *e = std::getenv("SQ_JIT_DLOAD");
+    return e && *e ? (e[0] == '0' ? 0 : 1) : -1;
+  }();
+  const bool dload_on = dload_env < 0 ? !c64 : dload_env == 1;
+  JitShape j;
+  for (const SweepOp &op : ps.op) j.smem_coef |= lane_indexed(op);
+  j.dload = dload_on && (ps.h.flags & kDirectLoad);
+  j.dstore = (ps.h.flags & kDirectStore) != 0;
+  return j;
+}
+
 std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
   const char *R = c64 ? "float" : "double";
   const int M = int(ps.h.m);
+  const JitShape js = jit_shape(ps, c64);
   std::ostringstream s;
   s << "extern \"C\" __global__ void __launch_bounds__(" << (1 << (M - kRegBits)) << ", " << minb
     << ")\nsq_jit_sweep(Vec2<" << R << ">::T *__restrict__ psi, const __grid_constant__ SweepParams<"
     << R << "> P) {\n";
   s << "  using C2 = Vec2<" << R << ">::T;\n";
-  // Coefficients come from the parameter block, except for diagonal ops
-  // indexed by tile bits that differ across the lanes (shared-memory copy).
-  auto lane_indexed = [](const SweepOp &op) {
-    if (op.kind != kSwDiag) return false;
-    for (int t = 0; t < op.ndt; ++t)
-      if (op.dsrc[t] != kSrcGlobal) return true;
-    return false;
-  };
-  bool smem_coef = false;
-  for (const SweepOp &op : ps.op) smem_coef |= lane_indexed(op);
-  s << "  jit_sweep<" << R << ", " << M << ", " << ps.h.l << ", " << (smem_coef ? "true" : "false")
-    << ">(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase, const uint64_t *hitab) {\n";
+  s << "  using Tile = JitTile<" << M << ", " << ps.h.l;
+  for (uint32_t i = 0; i < ps.h.m - ps.h.l; ++i) s << ", " << int(ps.h.hi[i]);
+  s << ">;\n";
+  auto tf = [](bool b) { return b ? "true" : "false"; };
+  s << "  jit_sweep<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dload) << ", "
+    << tf(js.dstore) << ">(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
   const uint32_t last = ps.h.nphases - 1;
   for (uint32_t p = 0; p < ps.h.nphases; ++p) {
     const SweepPhase &ph = ps.ph[p];
-    s << "    {\n      using Ph = JitPhase<" << R << ", " << M << ", " << ps.h.l << ", " << int(ph.reg[0]) << ", "
+    const bool from_hbm = p == 0 && js.dload, to_hbm = p == last && js.dstore;
+    s << "    {\n      using Ph = JitPhase<" << R << ", " << M << ", Tile, " << int(ph.reg[0]) << ", "
       << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]);
-    for (int t : thread_positions(ph, M, c64, p == last && (ps.h.flags & kDirectStore))) s << ", " << t;
+    for (int t : thread_positions(ph, M, c64, from_hbm || to_hbm)) s << ", " << t;
     s << ">;\n";
-    s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << "> A;\n"
-      << "      Ph::gather(A, tile, jb);\n";
+    s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << "> A;\n";
+    if (from_hbm)
+      s << "      Ph::load(A, psi, gbase, jb);\n";
+    else
+      s << "      Ph::gather(A, tile, jb);\n";
     for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
       const SweepOp &op = ps.op[oi];
       s << "      ";
@@ -352,8 +382,8 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
           << ");\n";
       }
     }
-    if (p == last && (ps.h.flags & kDirectStore)) {
-      s << "      Ph::store(A, psi, P.h, hitab, gbase, jb);\n    }\n";
+    if (p == last && js.dstore) {
+      s << "      Ph::store(A, psi, gbase, jb);\n    }\n";
     } else {
       s << "      Ph::scatter(A, tile, jb);\n      __syncthreads();\n    }\n";
     }
@@ -364,6 +394,11 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
 
 std::string jit_source(const PlannedSweep &ps, bool c64, int minb) {
   return prelude() + jit_body(ps, c64, minb);
+}
+
+size_t jit_smem(const PlannedSweep &ps, bool c64) {
+  const JitShape js = jit_shape(ps, c64);
+  return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload, js.smem_coef ? (ps.h.ncoef + 1) & ~1u : 0u);
 }
 
 int jit_minb(bool c64, uint32_t m) {
@@ -429,6 +464,7 @@ extern "C" int sq_jit_source(uint32_t num_qubits, int dtype, const sq_circuit_op
         if (uint32_t(m) <= want) opt.tile_bits = uint32_t(m);
     }
     opt.max_dense_k = c64 ? 4 : 3;
+    opt.low_bits = sq::auto_low_bits(c64, num_qubits, opt.tile_bits);
     plan = sq::plan_sweeps(ap.forward, num_qubits, opt);
   } catch (const std::exception &e) {
     return sq_detail_fail(SQ_ERR_INVALID, e.what());

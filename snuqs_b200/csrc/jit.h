@@ -14,6 +14,8 @@ void jit_note_launch(bool jit);
 std::string jit_source(const PlannedSweep &ps, bool c64, int minb);
 // The part of that source that depends on `ps` (the cache key).
 std::string jit_body(const PlannedSweep &ps, bool c64, int minb);
+// Dynamic shared memory the JIT kernel of `ps` needs.
+size_t jit_smem(const PlannedSweep &ps, bool c64);
 // CTAs per SM the kernels of (precision, tile bits) are built for.
 int jit_minb(bool c64, uint32_t m);
 // Launchable kernel (a cudaKernel_t as const void*) for `ps`, compiling and

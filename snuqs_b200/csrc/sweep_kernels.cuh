@@ -530,13 +530,39 @@ struct ParamCoef {
   }
 };
 
-template <typename Real, int M, int L, int R0, int R1, int R2, int R3, int... T>
+// Tile geometry of one sweep with its high tile bits as constants: tile
+// position L+i holds global index bit HI[i] (ascending); positions below L
+// are the L lowest global bits.  Global addresses then need no lookup table.
+template <int M, int L, int... HI>
+struct JitTile {
+  static_assert(sizeof...(HI) == M - L, "one global bit per high tile position");
+  // Global offset of tile-local index j.  Bitwise: off(a | b) = off(a) | off(b)
+  // for disjoint a, b.
+  __host__ __device__ static constexpr uint64_t off(uint32_t j) {
+    uint64_t x = j & ((1u << L) - 1u);
+    int i = L;
+    ((x |= uint64_t((j >> i++) & 1u) << HI), ...);
+    return x;
+  }
+  // Global index of element 0 of tile t: the bits of t fill the non-tile
+  // positions, ascending.
+  __device__ __forceinline__ static uint64_t base(uint64_t t) {
+    uint64_t x = t << L;
+    ((x = ((x >> HI) << (HI + 1)) | (x & ((uint64_t(1) << HI) - 1))), ...);
+    return x;
+  }
+};
+
+// One phase: register bits R0..R3 (tile positions, ascending), thread bit i
+// on tile position T[i].
+template <typename Real, int M, class Tile, int R0, int R1, int R2, int R3, int... T>
 struct JitPhase {
   using C2 = typename Vec2<Real>::T;
   static_assert(sizeof...(T) == M - kRegBits, "one tile position per thread bit");
-  // Thread bit i sits on tile position T[i]: the code generator places the
-  // lane bits that share a shared-memory wavefront on positions whose swizzle
-  // images are independent (conflict-free gathers and scatters).
+  // The code generator places the lane bits that share a shared-memory
+  // wavefront on positions whose swizzle images are independent
+  // (conflict-free gathers and scatters), or, in a phase that moves data
+  // straight between registers and HBM, on the lowest positions (coalesced).
   __device__ __forceinline__ static uint32_t jb(uint32_t tid) {
     uint32_t x = 0;
     int i = 0;
@@ -547,6 +573,11 @@ struct JitPhase {
     constexpr uint32_t W0 = swz_c<Real>(1u << R0), W1 = swz_c<Real>(1u << R1);
     constexpr uint32_t W2 = swz_c<Real>(1u << R2), W3 = swz_c<Real>(1u << R3);
     return sb ^ ((ri & 1) ? W0 : 0u) ^ ((ri & 2) ? W1 : 0u) ^ ((ri & 4) ? W2 : 0u) ^ ((ri & 8) ? W3 : 0u);
+  }
+  // Global offset of register slot ri relative to the thread's base.
+  __device__ __forceinline__ static constexpr uint64_t goff(int ri) {
+    return ((ri & 1) ? Tile::off(1u << R0) : 0) + ((ri & 2) ? Tile::off(1u << R1) : 0) +
+           ((ri & 4) ? Tile::off(1u << R2) : 0) + ((ri & 8) ? Tile::off(1u << R3) : 0);
   }
   __device__ __forceinline__ static void gather(Amps<Real> &A, const C2 *tile, uint32_t jbv) {
     const uint32_t sb = swz<Real>(jbv);
@@ -567,92 +598,109 @@ struct JitPhase {
       tile[slot(sb, ri)] = v;
     }
   }
-  // Straight to HBM from registers (the last phase, when its register bits
+  // Straight from HBM into registers (a first phase whose register bits
   // leave the low tile bits to the lanes).
-  __device__ __forceinline__ static void store(const Amps<Real> &A, C2 *psi, const SweepHeader &h,
-                                               const uint64_t *hitab, uint64_t gbase, uint32_t jbv) {
-    auto gw = [&](int pos) -> uint64_t {
-      return pos < L ? (uint64_t(1) << pos) : (uint64_t(1) << h.hi[pos - L]);
-    };
-    const uint64_t tbase = gbase | hitab[jbv >> L] | (jbv & ((1u << L) - 1u));
-    const uint64_t g0 = gw(R0), g1 = gw(R1), g2 = gw(R2), g3 = gw(R3);
+  __device__ __forceinline__ static void load(Amps<Real> &A, const C2 *__restrict__ psi, uint64_t gbase,
+                                              uint32_t jbv) {
+    const C2 *p = psi + (gbase | Tile::off(jbv));
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri) {
+      const C2 v = p[goff(ri)];
+      A.re[ri] = v.x;
+      A.im[ri] = v.y;
+    }
+  }
+  // Straight from registers to HBM (the mirror case for a last phase).
+  __device__ __forceinline__ static void store(const Amps<Real> &A, C2 *psi, uint64_t gbase, uint32_t jbv) {
+    C2 *p = psi + (gbase | Tile::off(jbv));
 #pragma unroll
     for (int ri = 0; ri < kRegAmps; ++ri) {
       C2 v;
       v.x = A.re[ri];
       v.y = A.im[ri];
-      psi[tbase + ((ri & 1) ? g0 : 0) + ((ri & 2) ? g1 : 0) + ((ri & 4) ? g2 : 0) +
-          ((ri & 8) ? g3 : 0)] = v;
+      p[goff(ri)] = v;
     }
   }
 };
 
-// The tile loop of sweep_kernel with the phases supplied by the generated
-// kernel: phases(tile, coef, gbase, hitab) runs every phase of one tile.
-// SMEM_COEF: the phases also read coefficients from shared memory (diagonal
-// ops indexed by tile bits that vary across the lanes).
-template <typename Real, int M, int L, bool SMEM_COEF, class Phases>
+// Dynamic shared memory of a JIT sweep kernel: one tile buffer when the first
+// phase loads from HBM (DLOAD), else two (the next tile streams into the
+// second), then the coefficients when a phase reads them from shared memory.
+__host__ __device__ constexpr size_t jit_smem_bytes(int m, size_t amp_bytes, bool dload, uint32_t smem_coef) {
+  return (dload ? 1 : 2) * (size_t(1) << m) * amp_bytes + size_t(smem_coef) * amp_bytes;
+}
+
+// The tile loop with the phases supplied by the generated kernel:
+// phases(tile, coef, gbase) runs every phase of one tile.
+//  SMEM_COEF: the phases also read coefficients from shared memory (diagonal
+//             ops indexed by tile bits that vary across the lanes);
+//  DLOAD:     the first phase loads from HBM itself (no tile prefetch);
+//  DSTORE:    the last phase stores to HBM itself (no copy-out).
+template <typename Real, int M, class Tile, bool SMEM_COEF, bool DLOAD, bool DSTORE, class Phases>
 __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ psi,
                                           const SweepParams<Real> &P, Phases phases) {
   using C2 = typename Vec2<Real>::T;
   constexpr int NT = 1 << (M - kRegBits);
   constexpr uint32_t TS = 1u << M;
   constexpr uint32_t PER = TS / NT;
-  constexpr uint32_t LOWMASK = (1u << L) - 1u;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const SweepHeader &h = P.h;
   C2 *bufs = reinterpret_cast<C2 *>(smem_raw);
-  C2 *coef = bufs + 2 * TS;
-  uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + ((h.ncoef + 1) & ~1u));
+  C2 *coef = bufs + (DLOAD ? 1 : 2) * TS;
   const uint32_t tid = threadIdx.x;
-  if constexpr (SMEM_COEF)
+  if constexpr (SMEM_COEF) {
     for (uint32_t i = tid; i < h.ncoef; i += NT) {
       C2 v;
       v.x = P.coef[2 * i];
       v.y = P.coef[2 * i + 1];
       coef[i] = v;
     }
-  for (uint32_t c = tid; c < (1u << (M - L)); c += NT) {
-    uint64_t a = 0;
-#pragma unroll
-    for (int i = 0; i < M - L; ++i)
-      if ((c >> i) & 1) a |= uint64_t(1) << h.hi[i];
-    hitab[c] = a;
+    __syncthreads();
   }
-  __syncthreads();
+  // Element j = it * NT + tid of a tile: global offset off(it * NT) | off(tid).
   const uint32_t s_tid = swz<Real>(tid);
-  auto prefetch = [&](uint64_t t, C2 *dst) {
-    const uint64_t gb = tile_base(t, h);
+  const uint64_t toff = Tile::off(tid);
+  if constexpr (DLOAD) {
+    for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
+      const uint64_t gbase = Tile::base(t);
+      phases(bufs, coef, gbase);
+      if constexpr (!DSTORE) {
 #pragma unroll
-    for (uint32_t it = 0; it < PER; ++it) {
-      const uint32_t j = it * NT + tid;
-      cp_async<sizeof(C2)>(dst + (s_tid ^ swz<Real>(it * NT)), psi + (gb | hitab[j >> L] | (j & LOWMASK)));
-    }
-  };
-  uint32_t cur = 0;
-  if (blockIdx.x < h.num_tiles) prefetch(blockIdx.x, bufs);
-  cp_async_commit();
-  for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
-    C2 *tile = bufs + cur * TS;
-    const uint64_t tn = t + gridDim.x;
-    if (tn < h.num_tiles) prefetch(tn, bufs + (cur ^ 1) * TS);
-    cp_async_commit();
-    cp_async_wait_prev();
-    __syncthreads();
-    const uint64_t gbase = tile_base(t, h);
-    phases(tile, coef, gbase, hitab);
-    if (!(h.flags & kDirectStore)) {
-#pragma unroll
-      for (uint32_t it = 0; it < PER; ++it) {
-        const uint32_t j = it * NT + tid;
-        psi[gbase | hitab[j >> L] | (j & LOWMASK)] = tile[s_tid ^ swz<Real>(it * NT)];
+        for (uint32_t it = 0; it < PER; ++it)
+          psi[gbase | toff | Tile::off(it * NT)] = bufs[s_tid ^ swz<Real>(it * NT)];
       }
+      __syncthreads();
     }
-    __syncthreads();
-    cur ^= 1;
+  } else {
+    auto prefetch = [&](uint64_t t, C2 *dst) {
+      const C2 *src = psi + (Tile::base(t) | toff);
+#pragma unroll
+      for (uint32_t it = 0; it < PER; ++it)
+        cp_async<sizeof(C2)>(dst + (s_tid ^ swz<Real>(it * NT)), src + Tile::off(it * NT));
+    };
+    uint32_t cur = 0;
+    if (blockIdx.x < h.num_tiles) prefetch(blockIdx.x, bufs);
+    cp_async_commit();
+    for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
+      C2 *tile = bufs + cur * TS;
+      const uint64_t tn = t + gridDim.x;
+      if (tn < h.num_tiles) prefetch(tn, bufs + (cur ^ 1) * TS);
+      cp_async_commit();
+      cp_async_wait_prev();
+      __syncthreads();
+      const uint64_t gbase = Tile::base(t);
+      phases(tile, coef, gbase);
+      if constexpr (!DSTORE) {
+#pragma unroll
+        for (uint32_t it = 0; it < PER; ++it)
+          psi[gbase | toff | Tile::off(it * NT)] = tile[s_tid ^ swz<Real>(it * NT)];
+      }
+      __syncthreads();
+      cur ^= 1;
+    }
+    cp_async_wait_prev();
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
   }
-  cp_async_wait_prev();
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------

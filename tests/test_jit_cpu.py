@@ -44,7 +44,9 @@ def test_sources_cover_every_op_kind():
                 seen.add("tile_control")
             if "Ph::store(" in body:
                 seen.add("direct_store")
-    assert seen >= set(OP_ROUTINES) | {"global_control", "direct_store"}, seen
+            if "Ph::load(" in body:
+                seen.add("direct_load")
+    assert seen >= set(OP_ROUTINES) | {"global_control", "direct_store", "direct_load"}, seen
 
 
 def test_sources_depend_on_structure_not_angles():
@@ -89,9 +91,9 @@ def test_lane_placement_is_a_permutation_and_conflict_free(dtype):
     phases = conflict_free = 0
     for src in capi.jit_sources(n, circuits.random_mix(n, 200, seed=13), dtype):
         body = src[src.rindex("sq_jit_sweep"):]
-        for args in re.findall(r"JitPhase<\w+, ([\d, ]+)>", body):
+        for mm, args in re.findall(r"JitPhase<\w+, (\d+), Tile, ([\d, ]+)>", body):
             vals = [int(x) for x in args.split(",")]
-            m, regs, threads = vals[0], vals[2:6], vals[6:]
+            m, regs, threads = int(mm), vals[:4], vals[4:]
             assert sorted(regs + threads) == list(range(m))
             phases += 1
             conflict_free += _rank([img[p] for p in threads[:W]]) == W
