@@ -402,7 +402,12 @@ uint64_t select_tile(const std::vector<const HostOp *> &rem, size_t head, uint32
 // takes every ready op that fits its register set (diagonal ops fit any
 // phase).  Op j depends on an earlier op i when they do not commute.
 // Returns the new order and the first index of each phase.
-void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits,
+// `low`: the tile's lowest bits.  A first phase whose register set avoids
+// them can load from HBM straight into registers, and a last phase that
+// avoids them can store straight back (the lanes then cover contiguous
+// amplitudes), so the first phase prefers ops off those bits and later
+// phases take the ops on them as early as they can.
+void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits, uint64_t low,
                      std::vector<const HostOp *> &order, std::vector<uint64_t> &phase_regs,
                      std::vector<uint32_t> &phase_first) {
   const size_t N = ops.size();
@@ -434,15 +439,18 @@ void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits,
         progress = true;
       }
       if (progress) continue;
-      // Open the register set to the ready op that adds the fewest bits.
-      int best = -1, best_new = 99;
+      // Open the register set to the ready op that adds the fewest bits
+      // (low-bit ops last in the first phase, first in the others).
+      const bool first_phase = phase_first.size() == 1;
+      int best = -1, best_key = 1 << 20;
       for (size_t x = 0; x < N; ++x) {
         const uint64_t bit = uint64_t(1) << x;
         if ((placed & bit) || (pred[x] & ~placed)) continue;
         const uint64_t T = ops[x]->target_mask();
         if (popc64(R | T) > int(reg_bits)) continue;
-        const int nb = popc64(T & ~R);
-        if (nb < best_new) best_new = nb, best = int(x);
+        const bool on_low = (T & low) != 0;
+        const int key = (on_low == first_phase ? 16 : 0) + popc64(T & ~R);
+        if (key < best_key) best_key = key, best = int(x);
       }
       if (best < 0) break;
       R |= ops[size_t(best)]->target_mask();
@@ -532,7 +540,8 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       }
       if (chosen.empty()) throw std::logic_error("planner: empty sweep");
       std::vector<const HostOp *> order;
-      schedule_phases(chosen, sb.reg_bits, order, sb.phase_regs, sb.phase_first);
+      schedule_phases(chosen, sb.reg_bits, (uint64_t(1) << std::min<uint32_t>(l, 5)) - 1, order,
+                      sb.phase_regs, sb.phase_first);
       // More phases than a sweep holds: the ops of the excess phases go back
       // to the queue (every op they precede is among them).
       std::vector<size_t> back_idx;
