@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--tile-bits", type=int, default=0, help="override the engine's tile size")
     p.add_argument("--low-bits", type=int, default=0,
                    help="override the contiguous low bits of every tile")
+    p.add_argument("--op-cost", action="store_true",
+                   help="print the per-gate cost inside one fused sweep for each sweep-op kind "
+                        "(--qubits, default 27) instead of the benchmark line")
     return p.parse_args()
 
 
@@ -222,9 +225,71 @@ def config(n, args):
 # ---------------------------------------------------------------------------
 # Our engine
 # ---------------------------------------------------------------------------
+def op_cost(args):
+    """Marginal cost of one gate inside a fused sweep, per sweep-op kind: a
+    sweep of 1 and of 31 gates of one kind on the same 4 qubits (one register
+    phase), CUDA-event timed over 5 repetitions each; the slope over 30 gates
+    is the cost of one gate (an odd count, so that products of self-inverse
+    gates do not cancel to the identity).  One JSON line per kind."""
+    import torch
+
+    from snuqs_b200 import capi, circuits
+
+    n = args.qubits if args.qubits != N_QUBITS else 27
+    dtype = capi.SQ_C128 if args.precision == "complex128" else capi.SQ_C64
+    amp = 16 if dtype == capi.SQ_C128 else 8
+    rng = np.random.default_rng(SEED)
+    a, b, c, d = n - 8, n - 9, n - 10, n - 11  # four qubits on high index bits 7..10
+    u2 = circuits.haar_unitary(4, rng)
+    kinds = [
+        ("PhaseShift", "conditional phase", lambda i: ("PhaseShift", ((a, b, c, d)[i % 4],), (0.3,))),
+        ("RotZ", "diagonal", lambda i: ("RotZ", ((a, b, c, d)[i % 4],), (0.3,))),
+        ("PauliX", "anti-diagonal, pure", lambda i: ("PauliX", ((a, b, c, d)[i % 4],), ())),
+        ("PauliY", "anti-diagonal", lambda i: ("PauliY", ((a, b, c, d)[i % 4],), ())),
+        ("RotX", "rotation form, imaginary", lambda i: ("RotX", ((a, b, c, d)[i % 4],), (0.3,))),
+        ("RotY", "rotation form, real", lambda i: ("RotY", ((a, b, c, d)[i % 4],), (0.3,))),
+        ("XX", "2-qubit rotation form", lambda i: ("XX", ((a, b), (c, d))[i % 2], (0.3,))),
+        ("Swap", "middle swap, pure", lambda i: ("Swap", ((a, b), (c, d))[i % 2], ())),
+        ("ISwap", "middle swap", lambda i: ("ISwap", ((a, b), (c, d))[i % 2], ())),
+        ("U", "dense 1q", lambda i: ("U", ((a, b, c, d)[i % 4],), (0.1, 0.2, 0.3))),
+        ("CX", "control in registers", lambda i: ("CX", ((a, b), (c, d))[i % 2], ())),
+        ("CX", "control outside the tile", lambda i: ("CX", (0, (a, b, c, d)[i % 4]), ())),
+        ("ZZ", "diagonal", lambda i: ("ZZ", ((a, b), (c, d))[i % 2], (0.3,))),
+        ("Unitary", "dense 2q", lambda i: ("Unitary", ((a, b), (c, d))[i % 2], (), u2)),
+    ]
+    st = capi.State(n, dtype)
+    st.init_basis(0)
+    floor_ms = 2 * amp * (1 << n) / (measured_peak()[0] * 1e9) * 1e3
+    for name, kind, mk in kinds:
+        times = {}
+        for count in (1, 31):
+            ops = [mk(i) for i in range(count)]
+            st.apply_ops(ops)  # warm-up (and JIT compile)
+            st.flush()
+            torch.cuda.synchronize()
+            st.sweep_timing()
+            st.set_option(capi.SQ_OPT_TIMING, 1)
+            for _ in range(5):
+                st.apply_ops(ops)
+                st.flush()
+            st.set_option(capi.SQ_OPT_TIMING, 0)
+            ms, launches = st.sweep_timing()
+            times[count] = (ms / max(1, launches), launches / 5)
+        slope = (times[31][0] - times[1][0]) / 30
+        print(json.dumps({"gate": name, "kind": kind, "qubits": n, "precision": args.precision,
+                          "sweep_ms_1": round(times[1][0], 4), "sweep_ms_31": round(times[31][0], 4),
+                          "sweeps_per_flush": times[31][1],
+                          "ps_per_amp_per_gate": round(slope * 1e-3 / (1 << n) * 1e12, 4),
+                          "hbm_floor_ms": round(floor_ms, 4)}))
+    st.close()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.op_cost:
+        op_cost(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

