@@ -406,6 +406,12 @@ size_t jit_smem(const PlannedSweep &ps, bool c64) {
 }
 
 int jit_minb(bool c64, uint32_t m) {
+  // SQ_JIT_MINB overrides the CTAs per SM for every tile size (tuning).
+  static const int env = [] {
+    const char *e = std::getenv("SQ_JIT_MINB");
+    return e && *e ? std::atoi(e) : 0;
+  }();
+  if (env > 0 && env <= 16) return env;
   // Register budgets of the precompiled sweep instantiations.
   if (c64) return m == 10 ? 8 : m == 12 ? 2 : 1;
   return m == 10 ? 6 : m == 11 ? 3 : 1;
