@@ -40,6 +40,11 @@ N_GATES = 400
 SEED = 1234
 AMP_BYTES = 16
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per amplitude of one JIT sweep launch, from one ncu
+# capture of the same random-mix generator at 26 qubits complex128 (2.0917 GB
+# per launch / 2^26 amplitudes; profiles/sq_jit_sweep_random_mix_26q_c128_ncu_full.md),
+# scaled to the benchmark's 2^n amplitudes.
+NCU_DRAM_BYTES_PER_AMP = {"complex128": 2.0917e9 / (1 << 26)}
 
 
 def parse():
@@ -367,7 +372,11 @@ def _run_ours(args, rank, world, local):
         "fused_sweeps_per_step": sweeps_per_step,
         "gates_per_sweep": round(args.gates / max(1e-9, sweeps_per_step), 2),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": (round(NCU_DRAM_BYTES_PER_AMP[args.precision] * (1 << n))
+                                 if args.precision in NCU_DRAM_BYTES_PER_AMP and jit_sweeps == sweeps
+                                 else None),
+                     "traffic_note": "ncu dram read+write bytes per launch at 26 qubits, scaled by 2^(n-26)",
                      "kernel": ("sq_jit_sweep (NVRTC-specialised sweep, " if jit_sweeps == sweeps
                                 else "sq::sweep_kernel (") +
                                ("double)" if dtype == capi.SQ_C128 else "float)"),
