@@ -401,6 +401,10 @@ def _run_ours(args, rank, world, local):
             out["batch"] = batch_metric(args.precision)
         except Exception as e:
             out["batch"] = {"note": f"batch failed: {e}"}
+        try:
+            out["qaoa_batch"] = qaoa_batch_metric(args.precision)
+        except Exception as e:
+            out["qaoa_batch"] = {"note": f"qaoa batch failed: {e}"}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(n, ops)
@@ -468,6 +472,61 @@ def adjoint_metric(precision: str):
             "speedup_vs_param_shift": round(t_eval * evals / t_adj, 1),
             "timing": "host wall clock around synchronous calls; parameter shift extrapolated "
                       f"from {done} evaluations"}
+
+
+def qaoa_batch_metric(precision: str, sets: int = 512, n: int = 16, p: int = 8):
+    """Adjoint gradients of `sets` QAOA MaxCut parameter sets (n qubits, p
+    layers, 2p parameters) in one batched launch, against the same gradients
+    one circuit at a time (sq_adjoint_gradient) and the parameter-shift rule,
+    on the same GPU."""
+    import torch
+
+    from snuqs_b200 import adjoint, capi
+
+    dtype = capi.SQ_C128 if precision == "complex128" else capi.SQ_C64
+    ops, terms, _ = qaoa_workload(n, p)
+    thetas = np.random.default_rng(SEED + 1).uniform(0, np.pi, (sets, 2 * p))
+    b = capi.Batch(dtype)
+    hid = b.add_hamiltonian(n, terms)
+    for th in thetas:
+        b.add_circuit(n, adjoint.bind(ops, th), hid)
+    b.run_gradients(2 * p)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e, g = b.run_gradients(2 * p)
+    t_batch = time.perf_counter() - t0
+    kernel_ms, ctas = b.last_timing()
+    b.close()
+    # One circuit at a time, on a sample of the parameter sets.
+    ws = adjoint.Workspace(n, dtype)
+    adjoint.adjoint_gradient(ws, ops, thetas[0], terms, 2 * p)
+    sample = 16
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    worst = 0.0
+    for k in range(sample):
+        _, gk = adjoint.adjoint_gradient(ws, ops, thetas[k], terms, 2 * p)
+        worst = max(worst, float(np.abs(gk - g[k]).max()))
+    t_single = (time.perf_counter() - t0) / sample
+    adjoint.parameter_shift_gradient(ws.psi, ops, thetas[0], terms, 2 * p, max_evals=4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, done = adjoint.parameter_shift_gradient(ws.psi, ops, thetas[0], terms, 2 * p, max_evals=40)
+    t_eval = (time.perf_counter() - t0) / done
+    evals = adjoint.count_shift_evaluations(ops)
+    ws.close()
+    return {"workload": f"qaoa_maxcut_{n}q_p{p}_{sets}sets_{precision}", "params": 2 * p,
+            "batch_ms": round(t_batch * 1e3, 3), "batch_kernel_ms": round(kernel_ms, 3), "ctas": ctas,
+            "batch_grads_per_s": round(sets / t_batch, 1),
+            "single_adjoint_ms_per_grad": round(t_single * 1e3, 3),
+            "single_adjoint_grads_per_s": round(1.0 / t_single, 1),
+            "param_shift_grads_per_s": round(1.0 / (t_eval * evals), 3),
+            "batch_vs_single_adjoint": round(t_single * sets / t_batch, 1),
+            "batch_vs_param_shift": round(t_eval * evals * sets / t_batch, 1),
+            "max_abs_diff_vs_single_adjoint": worst,
+            "timing": "host wall clock around synchronous calls (batch: planning + upload + one "
+                      f"launch); single-circuit adjoint over {sample} sets; parameter shift "
+                      f"extrapolated from {done} evaluations"}
 
 
 def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED):

@@ -275,6 +275,15 @@ int sq_batch_num_circuits(const sq_batch *b, uint32_t *count);
 /* Plan, upload and run every circuit in one launch; energies (host,
  * one double per circuit, in circuit-id order).  Synchronous. */
 int sq_batch_run(sq_batch *b, double *energies, void *stream);
+/* Energies and adjoint gradients of every circuit in one persistent launch
+ * (no counterpart in the reference): per circuit a forward pass, lambda = H psi
+ * and a reverse two-state pass, with the circuit's psi and lambda in shared
+ * memory when it fits one tile and in a device pool otherwise.  Circuits
+ * declare their parametrised angles with sq_circuit_op.param/scale as for
+ * sq_adjoint_gradient; grads is a host array of ncircuits x n_params doubles
+ * (row = circuit id), energies one double per circuit.  Synchronous. */
+int sq_batch_run_gradients(sq_batch *b, uint32_t n_params, double *energies, double *grads,
+                           void *stream);
 /* Final state of a circuit (needs SQ_BOPT_KEEP_STATES before sq_batch_run);
  * host_dst receives 2^n amplitudes of the batch's precision. */
 int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream);

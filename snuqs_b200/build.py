@@ -121,13 +121,25 @@ def build(force: bool = False, verbose: bool = False) -> None:
         objs.append(obj)
     bat_src = os.path.join(CSRC, "batch_inst.cu")
     bat_deps = inst_deps + [bat_src, os.path.join(CSRC, "batch_kernels.cuh"),
-                            os.path.join(CSRC, "reduce_kernels.cuh")]
+                            os.path.join(CSRC, "reduce_kernels.cuh"),
+                            os.path.join(CSRC, "adjoint_kernels.cuh")]
     for real, m in BATCH_INSTANCES:
         obj = os.path.join(BUILD, f"batch_{real}_{m}.o")
         if force or _stale(obj, bat_deps):
             cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
                    f"-DSQ_REAL={real}", f"-DSQ_M={m}",
                    "-Xptxas", "-warn-spills", "-c", bat_src, "-o", obj]
+            jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                               stderr=subprocess.STDOUT, text=True)))
+        objs.append(obj)
+    badj_src = os.path.join(CSRC, "batch_adj_inst.cu")
+    badj_deps = bat_deps + [badj_src]
+    for real, m in BATCH_INSTANCES:
+        obj = os.path.join(BUILD, f"batch_adj_{real}_{m}.o")
+        if force or _stale(obj, badj_deps):
+            cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",
+                   f"-DSQ_REAL={real}", f"-DSQ_M={m}",
+                   "-Xptxas", "-warn-spills", "-c", badj_src, "-o", obj]
             jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
                                                stderr=subprocess.STDOUT, text=True)))
         objs.append(obj)

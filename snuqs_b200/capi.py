@@ -91,6 +91,7 @@ SIGNATURES = {
     "sq_batch_set_angles": (_I, [_P, _U32, _PD, _U32]),
     "sq_batch_num_circuits": (_I, [_P, _PU32]),
     "sq_batch_run": (_I, [_P, _PD, _P]),
+    "sq_batch_run_gradients": (_I, [_P, _U32, _PD, _PD, _P]),
     "sq_batch_state": (_I, [_P, _U32, _P, _P]),
     "sq_batch_last_timing": (_I, [_P, _PD, _PU32]),
 }
@@ -217,6 +218,14 @@ class Batch:
         out = np.zeros(max(1, len(self._n)), dtype=np.float64)
         check(lib().sq_batch_run(self.h, _dp(out), stream))
         return out[: len(self._n)]
+
+    def run_gradients(self, n_params: int, stream=None):
+        """(energies[ncircuits], grads[ncircuits, n_params]) in one launch."""
+        nc = len(self._n)
+        e = np.zeros(max(1, nc), dtype=np.float64)
+        g = np.zeros((max(1, nc), max(1, n_params)), dtype=np.float64)
+        check(lib().sq_batch_run_gradients(self.h, n_params, _dp(e), _dp(g), stream))
+        return e[:nc], g[:nc, :n_params]
 
     def state(self, circuit: int) -> np.ndarray:
         a = np.empty(1 << self._n[circuit],

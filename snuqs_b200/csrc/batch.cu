@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/snuqs_b200.h"
+#include "adjoint_plan.h"
 #include "batch_kernels.cuh"
 #include "host_ops.h"
 #include "sweep_registry.h"
@@ -93,8 +94,8 @@ struct sq_batch {
   std::vector<sq::PauliParams> hams;
   std::vector<uint32_t> ham_n;
   std::vector<Circ> circs;
-  DevBuf d_pool, d_plans, d_table, d_hams, d_energy, d_counter;
-  HostBuf h_plans, h_table, h_energy;
+  DevBuf d_pool, d_plans, d_table, d_hams, d_energy, d_counter, d_occ;
+  HostBuf h_plans, h_table, h_energy, h_occ;
   size_t hams_uploaded = 0;
   std::vector<uint64_t> state_off;  // per circuit id; ~0 when not kept
   std::vector<uint32_t> order;      // sorted position -> circuit id
@@ -166,6 +167,10 @@ void pack_sweep(const sq::PlannedSweep &ps, std::vector<unsigned char> &out) {
   hdr.op_off = uint32_t(align16(hdr.phase_off + ps.ph.size() * sizeof(sq::SweepPhase)));
   hdr.coef_off = uint32_t(align16(hdr.op_off + ps.op.size() * sizeof(sq::SweepOp)));
   hdr.bytes = uint32_t(align16(hdr.coef_off + ps.coef.size() * sizeof(C2)));
+  if (!ps.inner_global.empty()) {
+    hdr.inner_off = hdr.bytes;
+    hdr.bytes = uint32_t(align16(hdr.inner_off + (1 + ps.inner_global.size()) * sizeof(uint32_t)));
+  }
   const size_t base = out.size();
   out.resize(base + hdr.bytes, 0);
   unsigned char *r = out.data() + base;
@@ -176,6 +181,11 @@ void pack_sweep(const sq::PlannedSweep &ps, std::vector<unsigned char> &out) {
   for (size_t i = 0; i < ps.coef.size(); ++i) {
     c[i].x = Real(ps.coef[i].real());
     c[i].y = Real(ps.coef[i].imag());
+  }
+  if (hdr.inner_off) {
+    uint32_t *g = reinterpret_cast<uint32_t *>(r + hdr.inner_off);
+    g[0] = uint32_t(ps.inner_global.size());
+    for (size_t i = 0; i < ps.inner_global.size(); ++i) g[1 + i] = ps.inner_global[i];
   }
 }
 
@@ -362,6 +372,192 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   return SQ_OK;
 }
 
+// Plans one circuit of a gradient run: forward sweeps then reverse two-state
+// sweeps (adjoint_plan.cc), packed back to back.  Returns false with `err`.
+template <typename Real>
+bool plan_gradient_circuit(const Circ &c, uint32_t m, std::vector<unsigned char> &out, uint32_t &nfwd,
+                           uint32_t &nrev, std::vector<std::pair<int32_t, double>> &occ, std::string &err) {
+  try {
+    sq::AdjointPlan ap;
+    sq::build_adjoint(c.ops.data(), uint32_t(c.ops.size()), c.n, ap);
+    sq::PlanOptions fopt;
+    fopt.tile_bits = m;
+    fopt.max_dense_k = sizeof(Real) == 4 ? 4 : 3;
+    sq::PlanOptions ropt;
+    ropt.tile_bits = m;
+    ropt.reg_bits = sq::kAdjRegBits;
+    ropt.max_dense_k = sq::kAdjRegBits;
+    const auto fplan = sq::plan_sweeps(ap.forward, c.n, fopt);
+    const auto rplan = sq::plan_sweeps(ap.reverse, c.n, ropt);
+    nfwd = nrev = 0;
+    for (const auto &pl : fplan) {
+      if (!pl.is_sweep) {
+        err = "batch: a gate wider than a sweep's registers (use the single-state API)";
+        return false;
+      }
+      pack_sweep<Real>(pl.sweep, out);
+      ++nfwd;
+    }
+    for (const auto &pl : rplan) {
+      if (!pl.is_sweep) {
+        err = "batch: a gate wider than a reverse sweep's registers (use sq_adjoint_gradient)";
+        return false;
+      }
+      pack_sweep<Real>(pl.sweep, out);
+      ++nrev;
+    }
+    occ = ap.occurrences;
+    return true;
+  } catch (const std::exception &e) {
+    err = std::string("batch gradient planner: ") + e.what();
+    return false;
+  }
+}
+
+template <typename Real>
+int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *grads, cudaStream_t st) {
+  using C2 = typename sq::Vec2<Real>::T;
+  const uint32_t M = sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128;
+  const size_t nc = b->circs.size();
+  if (nc == 0) return SQ_OK;
+  std::vector<std::vector<unsigned char>> packed(nc);
+  std::vector<uint32_t> nfwd(nc, 0), nrev(nc, 0);
+  std::vector<std::vector<std::pair<int32_t, double>>> occs(nc);
+  std::vector<std::string> errs(nc);
+  std::vector<char> ok(nc, 0);
+  std::atomic<size_t> next{0};
+  const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> workers;
+  for (unsigned t = 0; t < nth; ++t)
+    workers.emplace_back([&]() {
+      for (size_t i = next++; i < nc; i = next++)
+        ok[i] = plan_gradient_circuit<Real>(b->circs[i], M, packed[i], nfwd[i], nrev[i], occs[i], errs[i]);
+    });
+  for (auto &th : workers) th.join();
+  for (size_t i = 0; i < nc; ++i) {
+    if (!ok[i]) return fail(SQ_ERR_UNSUPPORTED, errs[i]);
+    for (const auto &o : occs[i])
+      if (o.first >= int32_t(n_params))
+        return fail(SQ_ERR_INVALID, "batch gradient: parameter index " + std::to_string(o.first) +
+                                        " >= n_params " + std::to_string(n_params));
+  }
+  // Largest work first.
+  b->order.resize(nc);
+  for (size_t i = 0; i < nc; ++i) b->order[i] = uint32_t(i);
+  std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) {
+    const uint64_t cx = (uint64_t(1) << b->circs[x].n) * (uint64_t(nfwd[x]) + 2 * nrev[x] + 2);
+    const uint64_t cy = (uint64_t(1) << b->circs[y].n) * (uint64_t(nfwd[y]) + 2 * nrev[y] + 2);
+    return cx > cy;
+  });
+  // psi and lambda of every circuit larger than a tile live in the pool.
+  uint64_t pool_amps = 0, nocc = 0;
+  std::vector<uint64_t> psi_off(nc, 0), lam_off(nc, 0), occ_off(nc, 0);
+  for (uint32_t id : b->order) {
+    const Circ &c = b->circs[id];
+    if (c.n > M) {
+      psi_off[id] = pool_amps;
+      lam_off[id] = pool_amps + (uint64_t(1) << c.n);
+      pool_amps += uint64_t(2) << c.n;
+    }
+    occ_off[id] = nocc;
+    nocc += occs[id].size();
+  }
+  size_t plan_bytes = 0;
+  for (size_t i = 0; i < nc; ++i) plan_bytes += packed[i].size();
+  SQB_CUDA(cudaSetDevice(b->device));
+  if (int s = b->d_pool.ensure(std::max<uint64_t>(pool_amps, 1) * sizeof(C2))) return s;
+  if (int s = b->d_plans.ensure(plan_bytes + 16)) return s;
+  if (int s = b->h_plans.ensure(plan_bytes + 16)) return s;
+  if (int s = b->d_table.ensure(nc * sizeof(sq::BatchCircuit))) return s;
+  if (int s = b->h_table.ensure(nc * sizeof(sq::BatchCircuit))) return s;
+  if (int s = b->d_energy.ensure(nc * sizeof(double))) return s;
+  if (int s = b->h_energy.ensure(nc * sizeof(double))) return s;
+  if (int s = b->d_counter.ensure(sizeof(unsigned))) return s;
+  if (int s = b->d_occ.ensure(std::max<uint64_t>(nocc, 1) * sizeof(double2))) return s;
+  if (int s = b->h_occ.ensure(std::max<uint64_t>(nocc, 1) * sizeof(double2))) return s;
+  if (b->hams_uploaded != b->hams.size()) {
+    if (int s = b->d_hams.ensure(b->hams.size() * sizeof(sq::PauliParams))) return s;
+    SQB_CUDA(cudaMemcpy(b->d_hams.p, b->hams.data(), b->hams.size() * sizeof(sq::PauliParams),
+                        cudaMemcpyHostToDevice));
+    b->hams_uploaded = b->hams.size();
+  }
+  auto *tab = static_cast<sq::BatchCircuit *>(b->h_table.p);
+  unsigned char *hp = static_cast<unsigned char *>(b->h_plans.p);
+  size_t off = 0;
+  for (size_t pos = 0; pos < nc; ++pos) {
+    const uint32_t id = b->order[pos];
+    const Circ &c = b->circs[id];
+    std::memcpy(hp + off, packed[id].data(), packed[id].size());
+    sq::BatchCircuit &t = tab[pos];
+    std::memset(&t, 0, sizeof(t));
+    t.n = c.n;
+    t.nsweeps = nfwd[id];
+    t.nrev = nrev[id];
+    t.ham = c.ham;
+    t.state_off = psi_off[id];
+    t.lam_off = lam_off[id];
+    t.occ_off = occ_off[id];
+    t.plan_off = off;
+    off += packed[id].size();
+  }
+  const void *fn = sizeof(Real) == 4 ? SQ_BATCH_ADJ_PTR_NAME(float, 12)() : SQ_BATCH_ADJ_PTR_NAME(double, 11)();
+  const uint32_t L = uint32_t(sq::sweep_low_bits(int(M)));
+  const int threads = 1 << (M - sq::kAdjRegBits);
+  const size_t nw = size_t(threads + 31) / 32;
+  const size_t smem = 2 * (size_t(1) << M) * sizeof(C2) + size_t(sq::kMaxCoef) * sizeof(C2) +
+                      (size_t(1) << (M - L)) * sizeof(uint64_t) + nw * sq::kMaxInner * sizeof(double2);
+  SQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int per_sm = 0, sms = 0;
+  SQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  SQB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  const uint32_t grid = uint32_t(std::max<uint64_t>(
+      1, std::min<uint64_t>(nc, uint64_t(std::max(per_sm, 1)) * uint64_t(sms))));
+  if (!b->ev0) {
+    SQB_CUDA(cudaEventCreate(&b->ev0));
+    SQB_CUDA(cudaEventCreate(&b->ev1));
+  }
+  sq::BatchParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.circuits = static_cast<const sq::BatchCircuit *>(b->d_table.p);
+  P.plans = static_cast<const unsigned char *>(b->d_plans.p);
+  P.hams = static_cast<const sq::PauliParams *>(b->d_hams.p);
+  P.ncircuits = uint32_t(nc);
+  P.counter = static_cast<unsigned *>(b->d_counter.p);
+  P.energies = static_cast<double *>(b->d_energy.p);
+  C2 *poolp = static_cast<C2 *>(b->d_pool.p);
+  double2 *occp = static_cast<double2 *>(b->d_occ.p);
+  void *args[] = {&poolp, &P, &occp};
+  SQB_CUDA(cudaMemcpyAsync(b->d_plans.p, b->h_plans.p, plan_bytes, cudaMemcpyHostToDevice, st));
+  SQB_CUDA(cudaMemcpyAsync(b->d_table.p, b->h_table.p, nc * sizeof(sq::BatchCircuit),
+                           cudaMemcpyHostToDevice, st));
+  SQB_CUDA(cudaMemsetAsync(b->d_counter.p, 0, sizeof(unsigned), st));
+  SQB_CUDA(cudaMemsetAsync(b->d_occ.p, 0, std::max<uint64_t>(nocc, 1) * sizeof(double2), st));
+  SQB_CUDA(cudaEventRecord(b->ev0, st));
+  SQB_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, st));
+  SQB_CUDA(cudaGetLastError());
+  SQB_CUDA(cudaEventRecord(b->ev1, st));
+  SQB_CUDA(cudaMemcpyAsync(b->h_energy.p, b->d_energy.p, nc * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SQB_CUDA(cudaMemcpyAsync(b->h_occ.p, b->d_occ.p, std::max<uint64_t>(nocc, 1) * sizeof(double2),
+                           cudaMemcpyDeviceToHost, st));
+  SQB_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  SQB_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  b->last_ms = ms;
+  b->last_ctas = grid;
+  const double *he = static_cast<const double *>(b->h_energy.p);
+  const double2 *ho = static_cast<const double2 *>(b->h_occ.p);
+  for (size_t pos = 0; pos < nc; ++pos) energies[b->order[pos]] = he[pos];
+  for (size_t id = 0; id < nc; ++id) {
+    double *g = grads + id * n_params;
+    for (uint32_t p = 0; p < n_params; ++p) g[p] = 0.0;
+    for (size_t s = 0; s < occs[id].size(); ++s) {
+      const auto &o = occs[id][s];
+      if (o.first >= 0) g[o.first] += 2.0 * ho[occ_off[id] + s].x * o.second;
+    }
+  }
+  return SQ_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -389,6 +585,8 @@ int sq_batch_destroy(sq_batch *b) {
   b->d_hams.release();
   b->d_energy.release();
   b->d_counter.release();
+  b->d_occ.release();
+  b->h_occ.release();
   b->h_plans.release();
   b->h_table.release();
   b->h_energy.release();
@@ -471,6 +669,14 @@ int sq_batch_run(sq_batch *b, double *energies, void *stream) {
   if (!b || (!energies && !b->circs.empty())) return fail(SQ_ERR_INVALID, "null pointer");
   auto st = static_cast<cudaStream_t>(stream);
   return b->dtype == SQ_C64 ? run_impl<float>(b, energies, st) : run_impl<double>(b, energies, st);
+}
+
+int sq_batch_run_gradients(sq_batch *b, uint32_t n_params, double *energies, double *grads,
+                           void *stream) {
+  if (!b || !energies || (n_params && !grads)) return fail(SQ_ERR_INVALID, "null pointer");
+  auto st = static_cast<cudaStream_t>(stream);
+  return b->dtype == SQ_C64 ? run_gradient_impl<float>(b, n_params, energies, grads, st)
+                            : run_gradient_impl<double>(b, n_params, energies, grads, st);
 }
 
 int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream) {

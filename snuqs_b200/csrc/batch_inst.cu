@@ -10,3 +10,4 @@
 const void *SQ_BATCH_PTR_NAME(SQ_REAL, SQ_M)() {
   return reinterpret_cast<const void *>(&sq::batch_kernel<SQ_REAL, SQ_M>);
 }
+

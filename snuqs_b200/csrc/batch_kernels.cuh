@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "adjoint_kernels.cuh"
 #include "reduce_kernels.cuh"
 #include "sweep_kernels.cuh"
 
@@ -20,11 +21,18 @@ namespace sq {
 // Device table entry of one circuit.
 struct BatchCircuit {
   uint32_t n;          // qubits (>= 4)
-  uint32_t nsweeps;
+  uint32_t nsweeps;    // forward sweeps
   uint32_t ham;        // Hamiltonian index
   uint32_t keep;       // 1: leave the final state in the state pool
   uint64_t state_off;  // amplitude offset of its state in the pool
   uint64_t plan_off;   // byte offset of its first packed sweep in the plan pool
+  // Gradient runs only: the reverse (two-state) sweeps follow the forward
+  // ones in the plan pool; lambda's pool offset (n > tile bits); offset of the
+  // circuit's parameter-occurrence inner products in the output array.
+  uint32_t nrev;
+  uint32_t pad;
+  uint64_t lam_off;
+  uint64_t occ_off;
 };
 
 // A packed sweep: this header, then nphases SweepPhase, then nops SweepOp,
@@ -35,7 +43,9 @@ struct PackedSweep {
   uint32_t nops;
   uint32_t bytes;
   uint32_t phase_off, op_off, coef_off;  // byte offsets from the record start
-  uint32_t pad;
+  // Reverse sweeps of a gradient run: byte offset of a uint32 array
+  // [nslots, occurrence of slot 0, ...] (0 when the sweep has no inner ops).
+  uint32_t inner_off;
 };
 
 struct BatchParams {
@@ -208,6 +218,265 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 1)
     if (resident && C.keep)
       for (uint32_t j = tid; j < uint32_t(N); j += NT) psi[j] = tile[swz<Real>(j)];
     __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched adjoint gradients: one circuit per CTA (work queue as above).  For
+// each circuit: forward sweeps on psi, lambda = H psi with E = Re <psi|lambda>,
+// then the reverse two-state sweeps that un-compute both states and
+// accumulate <lambda| K |phi> for every parametrised angle occurrence
+// (adjoint_kernels.cuh).  A circuit of n <= M qubits keeps psi and lambda in
+// shared memory throughout; a larger one keeps them in the state pool and
+// streams tiles.  Inner products are summed per warp (shuffles), then over
+// warps in a fixed order, into occ[occ_off + occurrence] (one CTA owns a
+// circuit: no atomics).
+// ---------------------------------------------------------------------------
+
+// Two-state phases of one packed reverse sweep on a (phi, lambda) tile pair
+// in shared memory.  2^(m-3) threads take part; the others only meet the
+// barriers.
+template <typename Real>
+__device__ __forceinline__ void batch_adjoint_phases(typename Vec2<Real>::T *ft, typename Vec2<Real>::T *lt,
+                                                     const PackedSweep &ps, const SweepPhase *ph,
+                                                     const SweepOp *ops, const typename Vec2<Real>::T *coef,
+                                                     uint64_t gbase, double2 *acc) {
+  using C2 = typename Vec2<Real>::T;
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t nthr = 1u << (ps.h.m - kAdjRegBits);
+  const unsigned mask = nthr >= 32 ? 0xffffffffu : ((1u << nthr) - 1u);
+  for (uint32_t p = 0; p < ps.h.nphases; ++p) {
+    if (tid < nthr) {
+      const SweepPhase P = ph[p];
+      uint32_t jb = tid;
+#pragma unroll
+      for (int b = 0; b < kAdjRegBits; ++b) jb = uint32_t(insert_zero(jb, P.reg[b]));
+      const uint32_t sb = swz<Real>(jb);
+      const uint32_t w0 = swz<Real>(1u << P.reg[0]), w1 = swz<Real>(1u << P.reg[1]);
+      const uint32_t w2 = swz<Real>(1u << P.reg[2]);
+      Amps<Real, kAdjAmps> F, G;
+#pragma unroll
+      for (int ri = 0; ri < kAdjAmps; ++ri) {
+        const uint32_t s = sb ^ ((ri & 1) ? w0 : 0) ^ ((ri & 2) ? w1 : 0) ^ ((ri & 4) ? w2 : 0);
+        const C2 a = ft[s], b = lt[s];
+        F.re[ri] = a.x;
+        F.im[ri] = a.y;
+        G.re[ri] = b.x;
+        G.im[ri] = b.y;
+      }
+      for (uint32_t o = P.op_begin; o < P.op_end; ++o) {
+        const SweepOp &op = ops[o];
+        if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
+          double sr = 0.0, si = 0.0;
+          inner_op<Real>(F, G, coef, op, gbase, jb, sr, si);
+          for (uint32_t off = (nthr >= 32 ? 16u : nthr / 2); off > 0; off >>= 1) {
+            sr += __shfl_xor_sync(mask, sr, off);
+            si += __shfl_xor_sync(mask, si, off);
+          }
+          if (lane == 0) {
+            double2 &a = acc[warp * kMaxInner + op.slot];
+            a.x += sr;
+            a.y += si;
+          }
+        } else {
+          apply_op<Real, kAdjAmps>(F, coef, op, gbase, jb);
+          apply_op<Real, kAdjAmps>(G, coef, op, gbase, jb);
+        }
+      }
+#pragma unroll
+      for (int ri = 0; ri < kAdjAmps; ++ri) {
+        const uint32_t s = sb ^ ((ri & 1) ? w0 : 0) ^ ((ri & 2) ? w1 : 0) ^ ((ri & 4) ? w2 : 0);
+        C2 a, b;
+        a.x = F.re[ri];
+        a.y = F.im[ri];
+        b.x = G.re[ri];
+        b.y = G.im[ri];
+        ft[s] = a;
+        lt[s] = b;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// lambda = H psi over a state read through psi_at(i) and written through
+// lam_set(i, v); returns this thread's share of Re <psi|lambda>.  Group g
+// contributes (sum_t f_t (-1)^popc(i & zy_t)) * (odd_g ? -i : 1) * psi[i ^ x_g]
+// (PauliParams stores w_t (-1)^(ny_t / 2) in f and ny_t mod 2 in odd).
+template <typename Real, class PsiAt, class LamSet>
+__device__ __forceinline__ double batch_pauli_apply(const PauliParams &H, uint32_t n, PsiAt psi_at,
+                                                    LamSet lam_set) {
+  using C2 = typename Vec2<Real>::T;
+  double e = 0.0;
+  for (uint64_t i = threadIdx.x; i < (uint64_t(1) << n); i += blockDim.x) {
+    double ar = 0.0, ai = 0.0;
+    for (uint32_t gi = 0; gi < H.ngroups; ++gi) {
+      const PauliGroup &G = H.g[gi];
+      double c = 0.0;
+      for (uint32_t t = G.t0; t < G.t1; ++t) c += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
+      const C2 b = psi_at(i ^ G.x);
+      if (G.odd) {  // c * (-i) * b
+        ar += c * double(b.y);
+        ai -= c * double(b.x);
+      } else {
+        ar += c * double(b.x);
+        ai += c * double(b.y);
+      }
+    }
+    C2 o;
+    o.x = Real(ar);
+    o.y = Real(ai);
+    lam_set(i, o);
+    const C2 a = psi_at(i);
+    e += double(a.x) * ar + double(a.y) * ai;
+  }
+  return e;
+}
+
+// Dynamic shared memory: phi tile | lambda tile (2^M amplitudes each) |
+// coefficients (kMaxCoef) | high-bit table (2^(M-L) u64) | inner-product
+// slots (warps x kMaxInner double2).  2^(M-3) threads.
+template <typename Real, int M>
+__global__ void __launch_bounds__(1 << (M - kAdjRegBits), 1)
+    batch_adjoint_kernel(typename Vec2<Real>::T *__restrict__ pool, const __grid_constant__ BatchParams B,
+                         double2 *__restrict__ occ) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr uint32_t TS = 1u << M;
+  constexpr int NT = 1 << (M - kAdjRegBits);
+  constexpr int NW = (NT + 31) / 32;
+  constexpr int L = sweep_low_bits(M);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *ft = reinterpret_cast<C2 *>(smem_raw);
+  C2 *lt = ft + TS;
+  C2 *coef = lt + TS;
+  uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + kMaxCoef);
+  double2 *acc = reinterpret_cast<double2 *>(hitab + (1u << (M - L)));
+  __shared__ uint32_t s_next;
+  const uint32_t tid = threadIdx.x;
+
+  for (;;) {
+    if (tid == 0) s_next = atomicAdd(B.counter, 1u);
+    __syncthreads();
+    const uint32_t c = s_next;
+    __syncthreads();
+    if (c >= B.ncircuits) break;
+    const BatchCircuit C = B.circuits[c];
+    const uint32_t n = C.n;
+    C2 *psi = pool + C.state_off;
+    C2 *lam = pool + C.lam_off;
+    const bool resident = n <= uint32_t(M);
+    const uint64_t N = uint64_t(1) << n;
+    // |0...0>
+    for (uint64_t j = tid; j < N; j += NT) {
+      C2 v;
+      v.x = Real(j == 0 ? 1 : 0);
+      v.y = Real(0);
+      if (resident)
+        ft[swz<Real>(uint32_t(j))] = v;
+      else
+        psi[j] = v;
+    }
+    __syncthreads();
+    const unsigned char *rec = B.plans + C.plan_off;
+    // Forward sweeps (one state).
+    for (uint32_t s = 0; s < C.nsweeps; ++s) {
+      const PackedSweep &ps = *reinterpret_cast<const PackedSweep *>(rec);
+      const SweepPhase *ph = reinterpret_cast<const SweepPhase *>(rec + ps.phase_off);
+      const SweepOp *ops = reinterpret_cast<const SweepOp *>(rec + ps.op_off);
+      const C2 *gcoef = reinterpret_cast<const C2 *>(rec + ps.coef_off);
+      for (uint32_t i = tid; i < ps.h.ncoef; i += NT) coef[i] = gcoef[i];
+      const uint32_t m = ps.h.m, l = ps.h.l;
+      if (!resident)
+        for (uint32_t cc = tid; cc < (1u << (m - l)); cc += NT) {
+          uint64_t a = 0;
+          for (uint32_t i = 0; i < m - l; ++i)
+            if ((cc >> i) & 1) a |= uint64_t(1) << ps.h.hi[i];
+          hitab[cc] = a;
+        }
+      __syncthreads();
+      // One call site per phase routine (a resident state is one tile at base 0).
+      const uint32_t lowmask = (1u << l) - 1u, tsize = 1u << m;
+      const uint64_t ntiles = resident ? 1 : ps.h.num_tiles;
+      for (uint64_t t = 0; t < ntiles; ++t) {
+        const uint64_t gbase = resident ? 0 : tile_base(t, ps.h);
+        if (!resident) {
+          for (uint32_t j = tid; j < tsize; j += NT) ft[swz<Real>(j)] = psi[gbase | hitab[j >> l] | (j & lowmask)];
+          __syncthreads();
+        }
+        batch_tile_phases<Real>(ft, ps, ph, ops, coef, gbase);
+        if (!resident) {
+          for (uint32_t j = tid; j < tsize; j += NT) psi[gbase | hitab[j >> l] | (j & lowmask)] = ft[swz<Real>(j)];
+          __syncthreads();
+        }
+      }
+      rec += ps.bytes;
+    }
+    // lambda = H psi, E = Re <psi|lambda>.
+    const PauliParams &H = B.hams[C.ham];
+    double e;
+    if (resident)
+      e = batch_pauli_apply<Real>(
+          H, n, [&](uint64_t i) { return ft[swz<Real>(uint32_t(i))]; },
+          [&](uint64_t i, const C2 &v) { lt[swz<Real>(uint32_t(i))] = v; });
+    else
+      e = batch_pauli_apply<Real>(
+          H, n, [&](uint64_t i) { return psi[i]; }, [&](uint64_t i, const C2 &v) { lam[i] = v; });
+    e = block_sum(e);
+    if (tid == 0) B.energies[c] = e;
+    __syncthreads();
+    // Reverse two-state sweeps.
+    for (uint32_t s = 0; s < C.nrev; ++s) {
+      const PackedSweep &ps = *reinterpret_cast<const PackedSweep *>(rec);
+      const SweepPhase *ph = reinterpret_cast<const SweepPhase *>(rec + ps.phase_off);
+      const SweepOp *ops = reinterpret_cast<const SweepOp *>(rec + ps.op_off);
+      const C2 *gcoef = reinterpret_cast<const C2 *>(rec + ps.coef_off);
+      const uint32_t *inner = ps.inner_off ? reinterpret_cast<const uint32_t *>(rec + ps.inner_off) : nullptr;
+      for (uint32_t i = tid; i < ps.h.ncoef; i += NT) coef[i] = gcoef[i];
+      for (uint32_t i = tid; i < NW * kMaxInner; i += NT) acc[i] = make_double2(0.0, 0.0);
+      const uint32_t m = ps.h.m, l = ps.h.l;
+      if (!resident)
+        for (uint32_t cc = tid; cc < (1u << (m - l)); cc += NT) {
+          uint64_t a = 0;
+          for (uint32_t i = 0; i < m - l; ++i)
+            if ((cc >> i) & 1) a |= uint64_t(1) << ps.h.hi[i];
+          hitab[cc] = a;
+        }
+      __syncthreads();
+      const uint32_t lowmask = (1u << l) - 1u, tsize = 1u << m;
+      const uint64_t ntiles = resident ? 1 : ps.h.num_tiles;
+      for (uint64_t t = 0; t < ntiles; ++t) {
+        const uint64_t gbase = resident ? 0 : tile_base(t, ps.h);
+        if (!resident) {
+          for (uint32_t j = tid; j < tsize; j += NT) {
+            const uint64_t g = gbase | hitab[j >> l] | (j & lowmask);
+            ft[swz<Real>(j)] = psi[g];
+            lt[swz<Real>(j)] = lam[g];
+          }
+          __syncthreads();
+        }
+        batch_adjoint_phases<Real>(ft, lt, ps, ph, ops, coef, gbase, acc);
+        if (!resident) {
+          for (uint32_t j = tid; j < tsize; j += NT) {
+            const uint64_t g = gbase | hitab[j >> l] | (j & lowmask);
+            psi[g] = ft[swz<Real>(j)];
+            lam[g] = lt[swz<Real>(j)];
+          }
+          __syncthreads();
+        }
+      }
+      if (inner && tid < inner[0]) {
+        double r = 0.0, i = 0.0;
+        for (int w = 0; w < NW; ++w) {
+          r += acc[w * kMaxInner + tid].x;
+          i += acc[w * kMaxInner + tid].y;
+        }
+        double2 &o = occ[C.occ_off + inner[1 + tid]];
+        o.x += r;
+        o.y += i;
+      }
+      __syncthreads();
+      rec += ps.bytes;
+    }
   }
 }
 
