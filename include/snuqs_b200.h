@@ -256,7 +256,13 @@ int sq_expect_pauli_noalloc(const void *state, uint32_t num_qubits, int dtype,
  * tile (<= 11 qubits complex128, <= 12 complex64) never touches HBM. */
 typedef struct sq_batch sq_batch;
 typedef enum {
-  SQ_BOPT_KEEP_STATES = 0  /* 1: keep every final state for sq_batch_state */
+  SQ_BOPT_KEEP_STATES = 0, /* 1: keep every final state for sq_batch_state */
+  SQ_BOPT_TILE_BITS = 1,   /* log2 amplitudes per shared-memory tile (10..12; 0 = 11 for
+                              complex128, 12 for complex64): the fusion block and, for
+                              circuits of at most that many qubits, the resident state */
+  SQ_BOPT_LOW_BITS = 2,    /* contiguous low bits of a streamed tile (0 = planner default) */
+  SQ_BOPT_MAX_OPS = 3,     /* most gates one fused sweep carries (0 = 64) */
+  SQ_BOPT_CTAS_PER_SM = 4  /* persistent CTAs per SM (0 = the occupancy limit) */
 } sq_batch_option;
 int sq_batch_create(int dtype, sq_batch **out);
 int sq_batch_destroy(sq_batch *b);
@@ -275,6 +281,18 @@ int sq_batch_num_circuits(const sq_batch *b, uint32_t *count);
 /* Plan, upload and run every circuit in one launch; energies (host,
  * one double per circuit, in circuit-id order).  Synchronous. */
 int sq_batch_run(sq_batch *b, double *energies, void *stream);
+/* Launch configuration of the energy kernel, as the autotuner reports it. */
+typedef struct {
+  uint32_t tile_bits, low_bits, max_ops, ctas_per_sm;
+  double kernel_ms; /* best kernel time measured for it */
+} sq_batch_config;
+/* Autotuner (no counterpart in the reference): runs the batch's energy
+ * kernel for every tile size (10..12 bits), low-bit count (default / 3),
+ * fusion width (32 / 64 gates per sweep) and CTAs per SM (1 .. occupancy
+ * limit, at most 4), `reps` times each, times each run with CUDA events,
+ * keeps the fastest configuration on the batch (later sq_batch_run calls use
+ * it) and reports it in *best.  Synchronous; runs the circuits many times. */
+int sq_batch_autotune(sq_batch *b, uint32_t reps, sq_batch_config *best, void *stream);
 /* Energies and adjoint gradients of every circuit in one persistent launch
  * (no counterpart in the reference): per circuit a forward pass, lambda = H psi
  * and a reverse two-state pass, with the circuit's psi and lambda in shared

@@ -36,8 +36,12 @@ SWEEP_INSTANCES = [
 # Two-state adjoint kernels: (precision, tile bits); must match kAdjTileBits*.
 ADJOINT_INSTANCES = [("double", 4), ("double", 7), ("double", 10),
                      ("float", 4), ("float", 7), ("float", 11)]
-# Batched-circuit kernels: (precision, tile bits); must match kBatchTileBits*.
-BATCH_INSTANCES = [("double", 11), ("float", 12)]
+# Batched-circuit energy kernels: (precision, tile bits) for every tile size the
+# batch autotuner tries.
+BATCH_INSTANCES = [("double", 10), ("double", 11), ("double", 12),
+                   ("float", 10), ("float", 11), ("float", 12)]
+# Batched adjoint-gradient kernels: (precision, tile bits); must match kBatchTileBits*.
+BATCH_ADJ_INSTANCES = [("double", 11), ("float", 12)]
 LIB = os.path.join(HERE, "libsnuqs_b200.so")
 
 
@@ -134,7 +138,7 @@ def build(force: bool = False, verbose: bool = False) -> None:
         objs.append(obj)
     badj_src = os.path.join(CSRC, "batch_adj_inst.cu")
     badj_deps = bat_deps + [badj_src]
-    for real, m in BATCH_INSTANCES:
+    for real, m in BATCH_ADJ_INSTANCES:
         obj = os.path.join(BUILD, f"batch_adj_{real}_{m}.o")
         if force or _stale(obj, badj_deps):
             cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC",

@@ -92,9 +92,20 @@ SIGNATURES = {
     "sq_batch_num_circuits": (_I, [_P, _PU32]),
     "sq_batch_run": (_I, [_P, _PD, _P]),
     "sq_batch_run_gradients": (_I, [_P, _U32, _PD, _PD, _P]),
+    "sq_batch_autotune": (_I, [_P, _U32, _P, _P]),
     "sq_batch_state": (_I, [_P, _U32, _P, _P]),
     "sq_batch_last_timing": (_I, [_P, _PD, _PU32]),
 }
+
+
+class SqBatchConfig(ctypes.Structure):
+    """sq_batch_config (include/snuqs_b200.h)."""
+    _fields_ = [("tile_bits", ctypes.c_uint32), ("low_bits", ctypes.c_uint32),
+                ("max_ops", ctypes.c_uint32), ("ctas_per_sm", ctypes.c_uint32),
+                ("kernel_ms", ctypes.c_double)]
+
+
+SQ_BOPT_KEEP_STATES, SQ_BOPT_TILE_BITS, SQ_BOPT_LOW_BITS, SQ_BOPT_MAX_OPS, SQ_BOPT_CTAS_PER_SM = range(5)
 
 
 class SqCircuitOp(ctypes.Structure):
@@ -168,7 +179,6 @@ def circuit_ops(ops):
     return arr, keep
 
 
-SQ_BOPT_KEEP_STATES = 0
 
 
 class Batch:
@@ -218,6 +228,62 @@ class Batch:
         out = np.zeros(max(1, len(self._n)), dtype=np.float64)
         check(lib().sq_batch_run(self.h, _dp(out), stream))
         return out[: len(self._n)]
+
+    def set_option(self, option: int, value: int) -> None:
+        check(lib().sq_batch_set_option(self.h, option, value))
+
+    def configure(self, config: dict) -> None:
+        """Applies a launch configuration (the dict autotune() returns)."""
+        for key, opt in (("tile_bits", SQ_BOPT_TILE_BITS), ("low_bits", SQ_BOPT_LOW_BITS),
+                         ("max_ops", SQ_BOPT_MAX_OPS), ("ctas_per_sm", SQ_BOPT_CTAS_PER_SM)):
+            self.set_option(opt, int(config.get(key, 0)))
+
+    def signature(self) -> str:
+        """Workload key of the autotuner cache: device, precision and the
+        circuits' qubit-count histogram."""
+        import hashlib
+
+        dev = "unknown"
+        try:
+            import torch
+
+            dev = torch.cuda.get_device_name()
+        except Exception:
+            pass
+        hist = {}
+        for n in self._n:
+            hist[n] = hist.get(n, 0) + 1
+        text = f"{dev}|{self.dtype}|{sorted(hist.items())}"
+        return hashlib.sha1(text.encode()).hexdigest()[:16]
+
+    def autotune(self, reps: int = 2, cache: str | None = None, stream=None) -> dict:
+        """Picks tile size, low bits, fusion width and CTAs per SM by timing
+        the energy kernel (sq_batch_autotune) and applies the fastest.  With
+        `cache` (a JSON file), a result stored for the same signature() is
+        applied without timing, and new results are stored there."""
+        import json
+
+        key = self.signature()
+        store = {}
+        if cache and os.path.exists(cache):
+            try:
+                with open(cache) as f:
+                    store = json.load(f)
+            except Exception:
+                store = {}
+        if key in store:
+            self.configure(store[key])
+            return dict(store[key], cached=True)
+        c = SqBatchConfig()
+        check(lib().sq_batch_autotune(self.h, reps, ctypes.byref(c), stream))
+        out = {"tile_bits": c.tile_bits, "low_bits": c.low_bits, "max_ops": c.max_ops,
+               "ctas_per_sm": c.ctas_per_sm, "kernel_ms": c.kernel_ms}
+        if cache:
+            store[key] = out
+            os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+            with open(cache, "w") as f:
+                json.dump(store, f, indent=1)
+        return dict(out, cached=False)
 
     def run_gradients(self, n_params: int, stream=None):
         """(energies[ncircuits], grads[ncircuits, n_params]) in one launch."""

@@ -106,6 +106,15 @@ struct sq_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   uint32_t last_ctas = 0;
+  const void *graph_fn = nullptr;
+  // Launch configuration (0 = default): tile bits, low bits of a streamed
+  // tile, ops per sweep, CTAs per SM.
+  uint32_t tile_bits = 0, low_bits = 0, max_ops = 0, ctas_per_sm = 0;
+  // Energy-run plan cache: valid while the circuits and the plan settings
+  // are those it was made for.
+  uint64_t version = 0, planned_version = ~uint64_t(0);
+  uint32_t planned_m = 0, planned_l = 0, planned_ops = 0;
+  size_t planned_bytes = 0;
 };
 
 namespace {
@@ -191,7 +200,8 @@ void pack_sweep(const sq::PlannedSweep &ps, std::vector<unsigned char> &out) {
 
 // Plans one circuit into packed sweeps; returns the sweep count or < 0.
 template <typename Real>
-int plan_circuit(const Circ &c, uint32_t m, std::vector<unsigned char> &out, std::string &err) {
+int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
+                 std::vector<unsigned char> &out, std::string &err) {
   try {
     std::vector<sq::HostOp> ops;
     for (const auto &op : c.ops) {
@@ -212,6 +222,9 @@ int plan_circuit(const Circ &c, uint32_t m, std::vector<unsigned char> &out, std
     sq::PlanOptions opt;
     opt.tile_bits = m;
     opt.max_dense_k = sizeof(Real) == 4 ? 4 : 3;
+    opt.max_ops = max_ops;
+    // Low bits matter only for a state streamed through tiles (n > m).
+    if (low_bits && c.n > m && low_bits + uint32_t(sq::kRegBits) <= m) opt.low_bits = low_bits;
     const auto plan = sq::plan_sweeps(ops, c.n, opt);
     int sweeps = 0;
     for (const auto &pl : plan) {
@@ -229,12 +242,62 @@ int plan_circuit(const Circ &c, uint32_t m, std::vector<unsigned char> &out, std
   }
 }
 
+// Energy kernel of (precision, tile bits); nullptr when not compiled.
+template <typename Real>
+const void *batch_fn(uint32_t m) {
+  if constexpr (sizeof(Real) == 8) {
+    switch (m) {
+      case 10: return SQ_BATCH_PTR_NAME(double, 10)();
+      case 11: return SQ_BATCH_PTR_NAME(double, 11)();
+      case 12: return SQ_BATCH_PTR_NAME(double, 12)();
+    }
+  } else {
+    switch (m) {
+      case 10: return SQ_BATCH_PTR_NAME(float, 10)();
+      case 11: return SQ_BATCH_PTR_NAME(float, 11)();
+      case 12: return SQ_BATCH_PTR_NAME(float, 12)();
+    }
+  }
+  return nullptr;
+}
+
+template <typename Real>
+uint32_t batch_tile_bits(const sq_batch *b) {
+  return b->tile_bits ? b->tile_bits : uint32_t(sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128);
+}
+
+// Threads, dynamic shared memory and resident CTAs per SM of the energy
+// kernel for tile bits m.
+template <typename Real>
+int batch_shape(uint32_t m, const void *&fn, int &threads, size_t &smem, int &per_sm) {
+  using C2 = typename sq::Vec2<Real>::T;
+  fn = batch_fn<Real>(m);
+  if (!fn) return fail(SQ_ERR_INVALID, "batch: no kernel for " + std::to_string(m) + " tile bits");
+  const uint32_t L = uint32_t(sq::sweep_low_bits(int(m)));
+  // The high-bit table is sized for the smallest low-bit count a plan may use (3).
+  smem = 2 * (size_t(1) << m) * sizeof(C2) + size_t(sq::kMaxCoef) * sizeof(C2) +
+         (size_t(1) << (m - std::min<uint32_t>(L, 3))) * sizeof(uint64_t);
+  threads = 1 << (m - sq::kRegBits);
+  SQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  SQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  per_sm = std::max(per_sm, 1);
+  return SQ_OK;
+}
+
 template <typename Real>
 int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   using C2 = typename sq::Vec2<Real>::T;
-  const uint32_t M = sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128;
+  const uint32_t M = batch_tile_bits<Real>(b);
   const size_t nc = b->circs.size();
   if (nc == 0) return SQ_OK;
+  const void *fn = nullptr;
+  int threads = 0, per_sm = 0;
+  size_t smem = 0;
+  if (int s = batch_shape<Real>(M, fn, threads, smem, per_sm)) return s;
+  const bool replan = b->planned_version != b->version || b->planned_m != M ||
+                      b->planned_l != b->low_bits || b->planned_ops != b->max_ops;
+  size_t plan_bytes = b->planned_bytes;
+  if (replan) {
   // Plan all circuits in parallel.
   std::vector<std::vector<unsigned char>> packed(nc);
   std::vector<int> nsweeps(nc, 0);
@@ -245,7 +308,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   for (unsigned t = 0; t < nth; ++t)
     pool.emplace_back([&]() {
       for (size_t i = next++; i < nc; i = next++)
-        nsweeps[i] = plan_circuit<Real>(b->circs[i], M, packed[i], errs[i]);
+        nsweeps[i] = plan_circuit<Real>(b->circs[i], M, b->low_bits, b->max_ops, packed[i], errs[i]);
     });
   for (auto &th : pool) th.join();
   for (size_t i = 0; i < nc; ++i)
@@ -268,7 +331,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
       pool_amps += uint64_t(1) << c.n;
     }
   }
-  size_t plan_bytes = 0;
+  plan_bytes = 0;
   for (size_t i = 0; i < nc; ++i) plan_bytes += packed[i].size();
   SQB_CUDA(cudaSetDevice(b->device));
   if (int s = b->d_pool.ensure(std::max<uint64_t>(pool_amps, 1) * sizeof(C2))) return s;
@@ -302,25 +365,27 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     t.plan_off = off;
     off += packed[id].size();
   }
+    // Staging buffers may have moved: the graph is captured again.
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->planned_version = b->version;
+    b->planned_m = M;
+    b->planned_l = b->low_bits;
+    b->planned_ops = b->max_ops;
+    b->planned_bytes = plan_bytes;
+  }  // replan
   // Kernel configuration.
-  const void *fn = sizeof(Real) == 4 ? SQ_BATCH_PTR_NAME(float, 12)() : SQ_BATCH_PTR_NAME(double, 11)();
-  const uint32_t L = uint32_t(sq::sweep_low_bits(int(M)));
-  const size_t smem = (size_t(1) << M) * sizeof(C2) + size_t(sq::kMaxCoef) * sizeof(C2) +
-                      (size_t(1) << (M - L)) * sizeof(uint64_t);
-  SQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  const int threads = 1 << (M - sq::kRegBits);
-  int per_sm = 0, sms = 0;
-  SQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  int sms = 0;
   SQB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-  const uint32_t grid = uint32_t(std::max<uint64_t>(
-      1, std::min<uint64_t>(nc, uint64_t(std::max(per_sm, 1)) * uint64_t(sms))));
+  const int cps = b->ctas_per_sm ? std::min<int>(per_sm, int(b->ctas_per_sm)) : per_sm;
+  const uint32_t grid = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(nc, uint64_t(cps) * uint64_t(sms))));
   if (!b->ev0) {
     SQB_CUDA(cudaEventCreate(&b->ev0));
     SQB_CUDA(cudaEventCreate(&b->ev1));
   }
   // (Re)capture the graph when sizes or the stream changed.
   if (!b->graph || b->graph_plan_bytes != plan_bytes || b->graph_ncirc != nc ||
-      b->graph_stream != st || b->graph_grid != grid) {
+      b->graph_stream != st || b->graph_grid != grid || b->graph_fn != fn) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
     cudaStream_t cs;
@@ -360,6 +425,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     b->graph_ncirc = nc;
     b->graph_stream = st;
     b->graph_grid = grid;
+    b->graph_fn = fn;
   }
   SQB_CUDA(cudaGraphLaunch(b->graph, st));
   SQB_CUDA(cudaStreamSynchronize(st));
@@ -420,6 +486,11 @@ int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *
   const uint32_t M = sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128;
   const size_t nc = b->circs.size();
   if (nc == 0) return SQ_OK;
+  // This run restages the shared buffers: the energy run's plan cache and
+  // graph are no longer valid.
+  b->planned_version = ~uint64_t(0);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
   std::vector<std::vector<unsigned char>> packed(nc);
   std::vector<uint32_t> nfwd(nc, 0), nrev(nc, 0);
   std::vector<std::vector<std::pair<int32_t, double>>> occs(nc);
@@ -595,9 +666,29 @@ int sq_batch_destroy(sq_batch *b) {
 
 int sq_batch_set_option(sq_batch *b, int option, int64_t value) {
   if (!b) return fail(SQ_ERR_INVALID, "null batch");
-  if (option == SQ_BOPT_KEEP_STATES) {
-    b->keep = value != 0;
-    return SQ_OK;
+  switch (option) {
+    case SQ_BOPT_KEEP_STATES:
+      b->keep = value != 0;
+      b->version++;
+      return SQ_OK;
+    case SQ_BOPT_TILE_BITS:
+      if (value != 0 && (value < 10 || value > 12))
+        return fail(SQ_ERR_INVALID, "SQ_BOPT_TILE_BITS takes 0 or 10..12");
+      b->tile_bits = uint32_t(value);
+      return SQ_OK;
+    case SQ_BOPT_LOW_BITS:
+      if (value < 0 || value > 8) return fail(SQ_ERR_INVALID, "SQ_BOPT_LOW_BITS takes 0..8");
+      b->low_bits = uint32_t(value);
+      return SQ_OK;
+    case SQ_BOPT_MAX_OPS:
+      if (value < 0 || value > sq::kMaxOps)
+        return fail(SQ_ERR_INVALID, "SQ_BOPT_MAX_OPS takes 0.." + std::to_string(sq::kMaxOps));
+      b->max_ops = uint32_t(value);
+      return SQ_OK;
+    case SQ_BOPT_CTAS_PER_SM:
+      if (value < 0 || value > 32) return fail(SQ_ERR_INVALID, "SQ_BOPT_CTAS_PER_SM takes 0..32");
+      b->ctas_per_sm = uint32_t(value);
+      return SQ_OK;
   }
   return fail(SQ_ERR_INVALID, "unknown batch option");
 }
@@ -642,6 +733,7 @@ int sq_batch_add_circuit(sq_batch *b, uint32_t num_qubits, const sq_circuit_op *
     }
   }
   b->circs.push_back(std::move(c));
+  b->version++;
   *circuit_id = uint32_t(b->circs.size() - 1);
   return SQ_OK;
 }
@@ -656,6 +748,7 @@ int sq_batch_set_angles(sq_batch *b, uint32_t circuit, const double *angles, uin
       op.angles[j] = angles[k++];
     }
   if (k != count) return fail(SQ_ERR_INVALID, "batch: angle count mismatch");
+  b->version++;
   return SQ_OK;
 }
 
@@ -669,6 +762,63 @@ int sq_batch_run(sq_batch *b, double *energies, void *stream) {
   if (!b || (!energies && !b->circs.empty())) return fail(SQ_ERR_INVALID, "null pointer");
   auto st = static_cast<cudaStream_t>(stream);
   return b->dtype == SQ_C64 ? run_impl<float>(b, energies, st) : run_impl<double>(b, energies, st);
+}
+
+int sq_batch_autotune(sq_batch *b, uint32_t reps, sq_batch_config *best, void *stream) {
+  if (!b) return fail(SQ_ERR_INVALID, "null batch");
+  if (b->circs.empty()) return fail(SQ_ERR_INVALID, "batch autotune: no circuits");
+  auto st = static_cast<cudaStream_t>(stream);
+  reps = std::max<uint32_t>(1, std::min<uint32_t>(reps, 16));
+  std::vector<double> e(b->circs.size());
+  const uint32_t saved[4] = {b->tile_bits, b->low_bits, b->max_ops, b->ctas_per_sm};
+  sq_batch_config bc{};
+  bc.kernel_ms = -1.0;
+  int status = SQ_OK;
+  const bool c64 = b->dtype == SQ_C64;
+  for (uint32_t m : {10u, 11u, 12u}) {
+    const void *fn = nullptr;
+    int threads = 0, per_sm = 0;
+    size_t smem = 0;
+    status = c64 ? batch_shape<float>(m, fn, threads, smem, per_sm)
+                 : batch_shape<double>(m, fn, threads, smem, per_sm);
+    if (status != SQ_OK) break;
+    for (uint32_t l : {0u, 3u})
+      for (uint32_t ops : {32u, 64u}) {
+        // CTAs per SM from 1 up to the occupancy limit (at most 4 candidates).
+        for (int cps = 1; cps <= std::min(per_sm, 4) && status == SQ_OK; ++cps) {
+          b->tile_bits = m;
+          b->low_bits = l;
+          b->max_ops = ops;
+          b->ctas_per_sm = uint32_t(cps);
+          double t = 1e30;
+          for (uint32_t r = 0; r < reps && status == SQ_OK; ++r) {
+            status = c64 ? run_impl<float>(b, e.data(), st) : run_impl<double>(b, e.data(), st);
+            t = std::min(t, double(b->last_ms));
+          }
+          if (status == SQ_OK && (bc.kernel_ms < 0 || t < bc.kernel_ms)) {
+            bc.tile_bits = m;
+            bc.low_bits = l;
+            bc.max_ops = ops;
+            bc.ctas_per_sm = uint32_t(cps);
+            bc.kernel_ms = t;
+          }
+        }
+      }
+    if (status != SQ_OK) break;
+  }
+  if (status != SQ_OK) {
+    b->tile_bits = saved[0];
+    b->low_bits = saved[1];
+    b->max_ops = saved[2];
+    b->ctas_per_sm = saved[3];
+    return status;
+  }
+  b->tile_bits = bc.tile_bits;
+  b->low_bits = bc.low_bits;
+  b->max_ops = bc.max_ops;
+  b->ctas_per_sm = bc.ctas_per_sm;
+  if (best) *best = bc;
+  return SQ_OK;
 }
 
 int sq_batch_run_gradients(sq_batch *b, uint32_t n_params, double *energies, double *grads,

@@ -100,39 +100,69 @@ __device__ __forceinline__ void batch_tile_phases(typename Vec2<Real>::T *tile, 
 }
 
 // sum_groups sum_pairs of the Pauli expectation (reduce_kernels.cuh) over a
-// state read through `amp(i)`; result valid in thread 0.
+// state read through `amp(i)`; result valid in thread 0.  Each thread issues
+// the loads of U pairs before using any of them, so a state streamed from
+// HBM by one CTA keeps U times more reads in flight.
 template <typename Real, class AmpFn>
 __device__ __forceinline__ double batch_energy(const PauliParams &H, uint32_t n, AmpFn amp) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int U = 4;
   double acc = 0.0;
+  const uint64_t step = uint64_t(blockDim.x) * U;
   for (uint32_t gi = 0; gi < H.ngroups; ++gi) {
     const PauliGroup &G = H.g[gi];
     if (G.x == 0) {
-      for (uint64_t i = threadIdx.x; i < (uint64_t(1) << n); i += blockDim.x) {
-        const auto a = amp(i);
-        const double q = double(a.x) * double(a.x) + double(a.y) * double(a.y);
-        double w = 0.0;
-        for (uint32_t t = G.t0; t < G.t1; ++t) w += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
-        acc = fma(q, w, acc);
+      const uint64_t N = uint64_t(1) << n;
+      for (uint64_t i0 = threadIdx.x; i0 < N; i0 += step) {
+        C2 a[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const uint64_t i = i0 + uint64_t(u) * blockDim.x;
+          a[u] = amp(i < N ? i : 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const uint64_t i = i0 + uint64_t(u) * blockDim.x;
+          if (i >= N) continue;
+          const double q = double(a[u].x) * double(a[u].x) + double(a[u].y) * double(a[u].y);
+          double w = 0.0;
+          for (uint32_t t = G.t0; t < G.t1; ++t) w += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
+          acc = fma(q, w, acc);
+        }
       }
     } else {
       const uint32_t hb = 63 - __clzll(G.x);
-      for (uint64_t hh = threadIdx.x; hh < (uint64_t(1) << (n - 1)); hh += blockDim.x) {
-        const uint64_t i = insert_zero(hh, hb), j = i ^ G.x;
-        const auto a = amp(i), b = amp(j);
-        const double zr = double(a.x) * double(b.x) + double(a.y) * double(b.y);
-        const double zi = double(a.x) * double(b.y) - double(a.y) * double(b.x);
-        const double q = 2.0 * (G.odd ? zi : zr);
-        double w = 0.0;
-        for (uint32_t t = G.t0; t < G.t1; ++t) w += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
-        acc = fma(q, w, acc);
+      const uint64_t NP = uint64_t(1) << (n - 1);
+      for (uint64_t h0 = threadIdx.x; h0 < NP; h0 += step) {
+        C2 a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const uint64_t hh = h0 + uint64_t(u) * blockDim.x;
+          const uint64_t i = insert_zero(hh < NP ? hh : 0, hb);
+          a[u] = amp(i);
+          b[u] = amp(i ^ G.x);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const uint64_t hh = h0 + uint64_t(u) * blockDim.x;
+          if (hh >= NP) continue;
+          const uint64_t i = insert_zero(hh, hb);
+          const double zr = double(a[u].x) * double(b[u].x) + double(a[u].y) * double(b[u].y);
+          const double zi = double(a[u].x) * double(b[u].y) - double(a[u].y) * double(b[u].x);
+          const double q = 2.0 * (G.odd ? zi : zr);
+          double w = 0.0;
+          for (uint32_t t = G.t0; t < G.t1; ++t) w += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
+          acc = fma(q, w, acc);
+        }
       }
     }
   }
   return block_sum(acc);
 }
 
-// Dynamic shared memory: tile (2^M amplitudes) | coefficients (kMaxCoef) |
-// high-bit table (2^(M-L) u64).
+// Dynamic shared memory: two tiles (2 x 2^M amplitudes) | coefficients
+// (kMaxCoef) | high-bit table (2^(M-3) u64).  A state streamed through tiles
+// double-buffers them: tile t+1 arrives by cp.async while tile t is worked.
 template <typename Real, int M>
 __global__ void __launch_bounds__(1 << (M - kRegBits), 1)
     batch_kernel(typename Vec2<Real>::T *__restrict__ pool, const __grid_constant__ BatchParams B) {
@@ -141,7 +171,7 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 1)
   constexpr int NT = 1 << (M - kRegBits);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2 *tile = reinterpret_cast<C2 *>(smem_raw);
-  C2 *coef = tile + TS;
+  C2 *coef = tile + 2 * TS;
   uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + kMaxCoef);
   __shared__ uint32_t s_next;
   const uint32_t tid = threadIdx.x;
@@ -195,16 +225,28 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 1)
         batch_tile_phases<Real>(tile, ps, ph, ops, coef, 0);
       } else {
         const uint32_t lowmask = (1u << l) - 1u, tsize = 1u << m;
+        auto prefetch = [&](uint64_t t, C2 *dst) {
+          const uint64_t gb = tile_base(t, ps.h);
+          for (uint32_t j = tid; j < tsize; j += NT)
+            cp_async<sizeof(C2)>(dst + swz<Real>(j), psi + (gb | hitab[j >> l] | (j & lowmask)));
+        };
+        prefetch(0, tile);
+        cp_async_commit();
         for (uint64_t t = 0; t < ps.h.num_tiles; ++t) {
-          const uint64_t gbase = tile_base(t, ps.h);
-          for (uint32_t j = tid; j < tsize; j += NT)
-            tile[swz<Real>(j)] = psi[gbase | hitab[j >> l] | (j & lowmask)];
+          C2 *cur = tile + (t & 1) * TS;
+          // The other buffer's previous tile was written back before the
+          // barrier that ended the last iteration.
+          if (t + 1 < ps.h.num_tiles) prefetch(t + 1, tile + ((t + 1) & 1) * TS);
+          cp_async_commit();
+          cp_async_wait_prev();
           __syncthreads();
-          batch_tile_phases<Real>(tile, ps, ph, ops, coef, gbase);
+          const uint64_t gbase = tile_base(t, ps.h);
+          batch_tile_phases<Real>(cur, ps, ph, ops, coef, gbase);
           for (uint32_t j = tid; j < tsize; j += NT)
-            psi[gbase | hitab[j >> l] | (j & lowmask)] = tile[swz<Real>(j)];
+            psi[gbase | hitab[j >> l] | (j & lowmask)] = cur[swz<Real>(j)];
           __syncthreads();
         }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
       }
       rec += ps.bytes;
     }

@@ -78,6 +78,8 @@ struct PlanOptions {
   // Low index bits every tile contains (contiguous runs of 2^low_bits
   // amplitudes per global access); 0: sweep_low_bits(tile bits).
   uint32_t low_bits = 0;
+  // Most ops one sweep carries (fusion width in gates); 0: kMaxOps.
+  uint32_t max_ops = 0;
   // Tile selection and phase scheduling (needs reorder): 1 = choose each
   // sweep's tile bits to absorb the most upcoming gates and order the gates
   // of a sweep into the fewest register phases; 0 = take gates first come

@@ -24,7 +24,7 @@ namespace {
 int popc64(uint64_t x) { return __builtin_popcountll(x); }
 
 struct SweepBuilder {
-  uint32_t n, m, l, max_dense_k = 3, reg_bits = kRegBits;
+  uint32_t n, m, l, max_dense_k = 3, reg_bits = kRegBits, max_ops = kMaxOps;
   uint64_t S;  // tile bits (global index bits)
   std::vector<const HostOp *> ops;
   std::vector<uint64_t> phase_regs;  // register bits (global) of each phase
@@ -44,7 +44,7 @@ struct SweepBuilder {
 
   // Would `op` fit (tile, register, budget)?  If so, add it.
   bool try_add(const HostOp &op) {
-    if (ops.size() >= size_t(kMaxOps)) return false;
+    if (ops.size() >= size_t(max_ops)) return false;
     if (ncoef + coef_count(op) > uint32_t(kMaxCoef)) return false;
     if (op.kind == kOpInner && ninner >= uint32_t(kMaxInner)) return false;
     if (is_diag(op)) {
@@ -326,11 +326,17 @@ bool fusable_size(const HostOp &op, const PlanOptions &opt) {
   return op.tbits.size() <= size_t(kmax);
 }
 
+// Op budget of one sweep: opt.max_ops, capped by what SweepParams holds.
+uint32_t op_budget(const PlanOptions &opt) {
+  return opt.max_ops ? std::min<uint32_t>(opt.max_ops, kMaxOps) : uint32_t(kMaxOps);
+}
+
 // Gates from rem[head..] that a sweep with tile bits S takes (same rules as
 // the collection below, without growing S).
 uint32_t absorbed(const std::vector<const HostOp *> &rem, size_t head, uint64_t S, uint32_t n,
                   const PlanOptions &opt, size_t window) {
   uint32_t cnt = 0, ncoef = 0, ninner = 0;
+  const uint32_t max_ops = op_budget(opt);
   uint64_t blockT = 0, blockA = 0;
   size_t skipped = 0;
   for (size_t i = head; i < rem.size(); ++i) {
@@ -340,13 +346,13 @@ uint32_t absorbed(const std::vector<const HostOp *> &rem, size_t head, uint64_t 
     const bool diag = SweepBuilder::is_diag(op);
     const uint32_t c = SweepBuilder::coef_count(op);
     const bool fits = fusable_size(op, opt) && (diag || (op.target_mask() & ~S) == 0) &&
-                      cnt < uint32_t(kMaxOps) && ncoef + c <= uint32_t(kMaxCoef) &&
+                      cnt < max_ops && ncoef + c <= uint32_t(kMaxCoef) &&
                       !(op.kind == kOpInner && ninner >= uint32_t(kMaxInner));
     if (commutes && fits) {
       ++cnt;
       ncoef += c;
       if (op.kind == kOpInner) ++ninner;
-      if (cnt >= uint32_t(kMaxOps)) break;
+      if (cnt >= max_ops) break;
       continue;
     }
     blockT |= T;
@@ -496,6 +502,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       continue;
     }
     SweepBuilder sb(n, m, l);
+    sb.max_ops = op_budget(opt);
     sb.reg_bits = opt.reg_bits;
     sb.max_dense_k = std::min<uint32_t>(opt.max_dense_k, opt.reg_bits);
     if (select) {
@@ -516,7 +523,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
         const uint32_t c = SweepBuilder::coef_count(op);
         const bool fits = fusable_size(op, opt) &&
                           (diag || uint32_t(popc64(S | op.target_mask())) <= m) &&
-                          chosen.size() < size_t(kMaxOps) && ncoef + c <= uint32_t(kMaxCoef) &&
+                          chosen.size() < size_t(sb.max_ops) && ncoef + c <= uint32_t(kMaxCoef) &&
                           !(op.kind == kOpInner && ninner >= uint32_t(kMaxInner));
         if (commutes && fits) {
           if (!diag) S |= op.target_mask();
@@ -524,7 +531,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
           chosen_idx.push_back(i);
           ncoef += c;
           if (op.kind == kOpInner) ++ninner;
-          if (chosen.size() >= size_t(kMaxOps)) {
+          if (chosen.size() >= size_t(sb.max_ops)) {
             ++i;
             break;
           }

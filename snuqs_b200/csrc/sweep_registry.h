@@ -28,7 +28,11 @@ SQ_DECLARE_ADJOINT(float, 11)
 #undef SQ_DECLARE_ADJOINT
 
 #define SQ_BATCH_PTR_NAME(real, m) SQ_SWEEP_CAT(sq_batch_kernel_ptr, real, m)
+const void *SQ_BATCH_PTR_NAME(double, 10)();
 const void *SQ_BATCH_PTR_NAME(double, 11)();
+const void *SQ_BATCH_PTR_NAME(double, 12)();
+const void *SQ_BATCH_PTR_NAME(float, 10)();
+const void *SQ_BATCH_PTR_NAME(float, 11)();
 const void *SQ_BATCH_PTR_NAME(float, 12)();
 #define SQ_BATCH_ADJ_PTR_NAME(real, m) SQ_SWEEP_CAT(sq_batch_adjoint_kernel_ptr, real, m)
 const void *SQ_BATCH_ADJ_PTR_NAME(double, 11)();

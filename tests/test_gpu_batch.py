@@ -73,3 +73,40 @@ def test_batch_rejects_mismatched_hamiltonian():
     with pytest.raises(capi.SqError):
         b.add_circuit(7, [("Hadamard", (0,), ())], hid)
     b.close()
+
+
+@pytest.mark.parametrize("dtype,tol", [(capi.SQ_C128, 1e-11), (capi.SQ_C64, 2e-5)])
+def test_batch_launch_configurations_agree(dtype, tol):
+    sizes = [5, 9, 10, 11, 12, 13, 14, 8]
+    b, cases = make_batch(dtype, sizes, seed=21, keep=False, gates=60)
+    want = {cid: oracle.expectation(oracle.run_ops(ops, n), n, terms) for cid, n, ops, terms in cases}
+    for cfg in ({"tile_bits": 10, "low_bits": 3, "max_ops": 8, "ctas_per_sm": 1},
+                {"tile_bits": 11, "low_bits": 0, "max_ops": 64, "ctas_per_sm": 0},
+                {"tile_bits": 12, "low_bits": 3, "max_ops": 32, "ctas_per_sm": 2}):
+        b.configure(cfg)
+        e = b.run()
+        for cid, w in want.items():
+            assert abs(e[cid] - w) <= tol * max(1.0, abs(w)), (cfg, cid)
+    b.close()
+
+
+def test_batch_autotune_picks_a_candidate_and_keeps_results(tmp_path):
+    b, cases = make_batch(capi.SQ_C128, [6, 10, 12, 13, 9, 11], seed=22, keep=False, gates=40)
+    e0 = b.run()
+    cache = str(tmp_path / "tune.json")
+    cfg = b.autotune(reps=1, cache=cache)
+    assert cfg["tile_bits"] in (10, 11, 12) and cfg["low_bits"] in (0, 3)
+    assert cfg["max_ops"] in (32, 64) and 1 <= cfg["ctas_per_sm"] <= 4 and not cfg["cached"]
+    e1 = b.run()
+    assert np.abs(e1 - e0).max() <= 1e-11
+    assert b.autotune(cache=cache)["cached"]
+    b.close()
+
+
+def test_batch_option_validation():
+    b = capi.Batch(capi.SQ_C128)
+    with pytest.raises(capi.SqError):
+        b.set_option(capi.SQ_BOPT_TILE_BITS, 9)
+    with pytest.raises(capi.SqError):
+        b.set_option(capi.SQ_BOPT_MAX_OPS, 65)
+    b.close()
