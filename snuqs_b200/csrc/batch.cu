@@ -575,7 +575,7 @@ int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *
   const uint32_t L = uint32_t(sq::sweep_low_bits(int(M)));
   const int threads = 1 << (M - sq::kAdjRegBits);
   const size_t nw = size_t(threads + 31) / 32;
-  const size_t smem = 2 * (size_t(1) << M) * sizeof(C2) + size_t(sq::kMaxCoef) * sizeof(C2) +
+  const size_t smem = 4 * (size_t(1) << M) * sizeof(C2) + size_t(sq::kMaxCoef) * sizeof(C2) +
                       (size_t(1) << (M - L)) * sizeof(uint64_t) + nw * sq::kMaxInner * sizeof(double2);
   SQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   int per_sm = 0, sms = 0;

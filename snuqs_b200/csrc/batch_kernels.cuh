@@ -375,9 +375,11 @@ __device__ __forceinline__ double batch_pauli_apply(const PauliParams &H, uint32
   return e;
 }
 
-// Dynamic shared memory: phi tile | lambda tile (2^M amplitudes each) |
-// coefficients (kMaxCoef) | high-bit table (2^(M-L) u64) | inner-product
-// slots (warps x kMaxInner double2).  2^(M-3) threads.
+// Dynamic shared memory: two (phi tile | lambda tile) buffers (2^M amplitudes
+// each) | coefficients (kMaxCoef) | high-bit table (2^(M-L) u64) |
+// inner-product slots (warps x kMaxInner double2).  2^(M-3) threads.  States
+// streamed from the pool double-buffer their tiles: tile t+1 arrives by
+// cp.async while tile t is worked.
 template <typename Real, int M>
 __global__ void __launch_bounds__(1 << (M - kAdjRegBits), 1)
     batch_adjoint_kernel(typename Vec2<Real>::T *__restrict__ pool, const __grid_constant__ BatchParams B,
@@ -388,9 +390,9 @@ __global__ void __launch_bounds__(1 << (M - kAdjRegBits), 1)
   constexpr int NW = (NT + 31) / 32;
   constexpr int L = sweep_low_bits(M);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2 *ft = reinterpret_cast<C2 *>(smem_raw);
+  C2 *ft = reinterpret_cast<C2 *>(smem_raw);  // buffer b: phi at ft + 2 b TS, lambda after it
   C2 *lt = ft + TS;
-  C2 *coef = lt + TS;
+  C2 *coef = ft + 4 * TS;
   uint64_t *hitab = reinterpret_cast<uint64_t *>(coef + kMaxCoef);
   double2 *acc = reinterpret_cast<double2 *>(hitab + (1u << (M - L)));
   __shared__ uint32_t s_next;
@@ -439,18 +441,31 @@ __global__ void __launch_bounds__(1 << (M - kAdjRegBits), 1)
       // One call site per phase routine (a resident state is one tile at base 0).
       const uint32_t lowmask = (1u << l) - 1u, tsize = 1u << m;
       const uint64_t ntiles = resident ? 1 : ps.h.num_tiles;
+      auto prefetch1 = [&](uint64_t t, C2 *dst) {
+        const uint64_t gb = tile_base(t, ps.h);
+        for (uint32_t j = tid; j < tsize; j += NT)
+          cp_async<sizeof(C2)>(dst + swz<Real>(j), psi + (gb | hitab[j >> l] | (j & lowmask)));
+      };
+      if (!resident) {
+        prefetch1(0, ft);
+        cp_async_commit();
+      }
       for (uint64_t t = 0; t < ntiles; ++t) {
+        C2 *cur = ft + (t & 1) * 2 * TS;
         const uint64_t gbase = resident ? 0 : tile_base(t, ps.h);
         if (!resident) {
-          for (uint32_t j = tid; j < tsize; j += NT) ft[swz<Real>(j)] = psi[gbase | hitab[j >> l] | (j & lowmask)];
+          if (t + 1 < ntiles) prefetch1(t + 1, ft + ((t + 1) & 1) * 2 * TS);
+          cp_async_commit();
+          cp_async_wait_prev();
           __syncthreads();
         }
-        batch_tile_phases<Real>(ft, ps, ph, ops, coef, gbase);
+        batch_tile_phases<Real>(cur, ps, ph, ops, coef, gbase);
         if (!resident) {
-          for (uint32_t j = tid; j < tsize; j += NT) psi[gbase | hitab[j >> l] | (j & lowmask)] = ft[swz<Real>(j)];
+          for (uint32_t j = tid; j < tsize; j += NT) psi[gbase | hitab[j >> l] | (j & lowmask)] = cur[swz<Real>(j)];
           __syncthreads();
         }
       }
+      if (!resident) asm volatile("cp.async.wait_all;\n" ::: "memory");
       rec += ps.bytes;
     }
     // lambda = H psi, E = Re <psi|lambda>.
@@ -486,26 +501,38 @@ __global__ void __launch_bounds__(1 << (M - kAdjRegBits), 1)
       __syncthreads();
       const uint32_t lowmask = (1u << l) - 1u, tsize = 1u << m;
       const uint64_t ntiles = resident ? 1 : ps.h.num_tiles;
+      auto prefetch2 = [&](uint64_t t, C2 *dst) {
+        const uint64_t gb = tile_base(t, ps.h);
+        for (uint32_t j = tid; j < tsize; j += NT) {
+          const uint64_t g = gb | hitab[j >> l] | (j & lowmask);
+          cp_async<sizeof(C2)>(dst + swz<Real>(j), psi + g);
+          cp_async<sizeof(C2)>(dst + TS + swz<Real>(j), lam + g);
+        }
+      };
+      if (!resident) {
+        prefetch2(0, ft);
+        cp_async_commit();
+      }
       for (uint64_t t = 0; t < ntiles; ++t) {
+        C2 *cf = ft + (t & 1) * 2 * TS, *cl = cf + TS;
         const uint64_t gbase = resident ? 0 : tile_base(t, ps.h);
         if (!resident) {
-          for (uint32_t j = tid; j < tsize; j += NT) {
-            const uint64_t g = gbase | hitab[j >> l] | (j & lowmask);
-            ft[swz<Real>(j)] = psi[g];
-            lt[swz<Real>(j)] = lam[g];
-          }
+          if (t + 1 < ntiles) prefetch2(t + 1, ft + ((t + 1) & 1) * 2 * TS);
+          cp_async_commit();
+          cp_async_wait_prev();
           __syncthreads();
         }
-        batch_adjoint_phases<Real>(ft, lt, ps, ph, ops, coef, gbase, acc);
+        batch_adjoint_phases<Real>(cf, cl, ps, ph, ops, coef, gbase, acc);
         if (!resident) {
           for (uint32_t j = tid; j < tsize; j += NT) {
             const uint64_t g = gbase | hitab[j >> l] | (j & lowmask);
-            psi[g] = ft[swz<Real>(j)];
-            lam[g] = lt[swz<Real>(j)];
+            psi[g] = cf[swz<Real>(j)];
+            lam[g] = cl[swz<Real>(j)];
           }
           __syncthreads();
         }
       }
+      if (!resident) asm volatile("cp.async.wait_all;\n" ::: "memory");
       if (inner && tid < inner[0]) {
         double r = 0.0, i = 0.0;
         for (int w = 0; w < NW; ++w) {
