@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--tile-bits", type=int, default=0, help="override the engine's tile size")
     p.add_argument("--low-bits", type=int, default=0,
                    help="override the contiguous low bits of every tile")
+    p.add_argument("--kernel-tour", action="store_true",
+                   help="run each kernel family once on a small case (for ncu captures) "
+                        "instead of the benchmark line")
     p.add_argument("--op-cost", action="store_true",
                    help="print the per-gate cost inside one fused sweep for each sweep-op kind "
                         "(--qubits, default 27) instead of the benchmark line")
@@ -289,9 +292,54 @@ def op_cost(args):
     st.close()
 
 
+def kernel_tour():
+    """Each kernel family once, on cases sized for an ncu capture (states of
+    2^22-2^24 amplitudes, above the 126 MB L2 where it matters): unfused gate
+    kernel, Pauli expectation, single-circuit adjoint (Pauli apply, two-state
+    sweeps, inner-product reduction), batched energies, batched gradients."""
+    import torch
+
+    from snuqs_b200 import adjoint, capi, circuits
+
+    n = 24
+    st = capi.State(n)
+    st.set_option(capi.SQ_OPT_FUSION, 0)
+    st.init_basis(0)
+    st.apply_ops(circuits.random_mix(n, 8, seed=SEED))  # gate_kernel, one launch per gate
+    st.flush()
+    terms = circuits.random_pauli_hamiltonian(n, 16, seed=SEED)
+    e = st.expectation(terms)  # pauli_expect_kernel
+    st.close()
+    ops, qterms, theta = qaoa_workload(22, 2)
+    ws = adjoint.Workspace(22)
+    e2, g = adjoint.adjoint_gradient(ws, ops, theta, qterms, 4)  # adjoint kernels
+    ws.close()
+    rng = np.random.default_rng(SEED)
+    b = capi.Batch(capi.SQ_C128)
+    hams = {k: b.add_hamiltonian(k, circuits.random_pauli_hamiltonian(k, 16, seed=k)) for k in range(8, 17)}
+    for _ in range(256):
+        k = int(rng.integers(8, 17))
+        b.add_circuit(k, circuits.vqe_ansatz(k, rng.uniform(0, 2 * np.pi, 12 * k)), hams[k])
+    eb = b.run()  # batch_kernel
+    b.close()
+    ops16, t16, _ = qaoa_workload(16, 4)
+    b = capi.Batch(capi.SQ_C128)
+    h16 = b.add_hamiltonian(16, t16)
+    for th in rng.uniform(0, np.pi, (64, 8)):
+        b.add_circuit(16, adjoint.bind(ops16, th), h16)
+    eg, gg = b.run_gradients(8)  # batch_adjoint_kernel
+    b.close()
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_tour": "ok", "expectation": e, "adjoint_energy": e2,
+                      "batch_energy_0": float(eb[0]), "batch_grad_00": float(gg[0, 0])}))
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.kernel_tour:
+        kernel_tour()
+        return
     if args.op_cost:
         op_cost(args)
         return
