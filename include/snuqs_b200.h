@@ -216,6 +216,12 @@ typedef struct {
 int sq_jit_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
                   uint32_t sweep_index, char *buf, uint64_t cap, uint64_t *len,
                   uint32_t *nsweeps);
+/* Test hook: as sq_jit_source, for reverse sweep `sweep_index` of the
+ * circuit's adjoint-gradient plan (two-state JIT kernel; *len = 0 when that
+ * sweep runs on the generic adjoint kernel).  Needs no GPU. */
+int sq_jit_adjoint_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
+                          uint32_t sweep_index, char *buf, uint64_t cap, uint64_t *len,
+                          uint32_t *nsweeps);
 
 /* Energy E = <psi|H|psi> of psi = U(theta)|0...0> for H = sum_t w_t P_t, and
  * dE/dtheta for n_params parameters, by one forward pass and one reverse

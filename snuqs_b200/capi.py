@@ -74,6 +74,7 @@ SIGNATURES = {
     "sq_jit_info": (_I, [ctypes.POINTER(_I), _PU64, _PU64]),
     "sq_jit_compile": (_I, [ctypes.c_char_p]),
     "sq_jit_source": (_I, [_U32, _I, _P, _U32, _U32, ctypes.c_char_p, _U64, _PU64, _PU32]),
+    "sq_jit_adjoint_source": (_I, [_U32, _I, _P, _U32, _U32, ctypes.c_char_p, _U64, _PU64, _PU32]),
     "sq_apply_gate_buffer": (_I, [_P, _P, _PU64, _U32, _U32, _U64, _P]),
     "sq_copy_to_host": (_I, [_P, _P, _P]),
     "sq_copy_from_host": (_I, [_P, _P, _P]),
@@ -123,19 +124,20 @@ def jit_info():
     return bool(av.value), a.value, b.value
 
 
-def jit_sources(n: int, ops, dtype: int = SQ_C128, limit: int | None = None):
-    """CUDA sources of the JIT kernels of the fused sweeps of a circuit."""
+def jit_sources(n: int, ops, dtype: int = SQ_C128, limit: int | None = None, adjoint: bool = False):
+    """CUDA sources of the JIT kernels of the fused sweeps of a circuit (with
+    adjoint=True: of the reverse sweeps of its adjoint-gradient plan; "" for
+    a sweep the generic kernel runs)."""
+    fn = lib().sq_jit_adjoint_source if adjoint else lib().sq_jit_source
     arr, keep = circuit_ops(ops)
     ln, ns = _U64(0), _U32(0)
-    check(lib().sq_jit_source(n, dtype, ctypes.cast(arr, _P), len(ops), 0, None, 0,
-                              ctypes.byref(ln), ctypes.byref(ns)))
+    check(fn(n, dtype, ctypes.cast(arr, _P), len(ops), 0, None, 0, ctypes.byref(ln), ctypes.byref(ns)))
     out = []
     for i in range(ns.value if limit is None else min(limit, ns.value)):
-        check(lib().sq_jit_source(n, dtype, ctypes.cast(arr, _P), len(ops), i, None, 0,
-                                  ctypes.byref(ln), ctypes.byref(ns)))
+        check(fn(n, dtype, ctypes.cast(arr, _P), len(ops), i, None, 0, ctypes.byref(ln), ctypes.byref(ns)))
         buf = ctypes.create_string_buffer(ln.value + 1)
-        check(lib().sq_jit_source(n, dtype, ctypes.cast(arr, _P), len(ops), i, buf, ln.value + 1,
-                                  ctypes.byref(ln), ctypes.byref(ns)))
+        check(fn(n, dtype, ctypes.cast(arr, _P), len(ops), i, buf, ln.value + 1,
+                 ctypes.byref(ln), ctypes.byref(ns)))
         out.append(buf.value.decode())
     del keep
     return out

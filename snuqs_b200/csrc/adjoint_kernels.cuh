@@ -18,9 +18,6 @@
 
 namespace sq {
 
-constexpr int kAdjRegBits = 3;
-constexpr int kAdjAmps = 1 << kAdjRegBits;
-
 struct PauliApplyGroup {
   uint64_t x;        // flip mask
   uint32_t t0, t1;   // term range
@@ -67,51 +64,6 @@ __global__ void __launch_bounds__(kReduceThreads)
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
-}
-
-// Inner-product contribution of one thread for a kSwInnerDiag op.
-template <typename Real, int V>
-__device__ __forceinline__ void inner_diag(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
-                                           const typename Vec2<Real>::T *__restrict__ c,
-                                           uint32_t base, double &sr, double &si) {
-  const auto *cb = c + (base << ct_popc<V>());
-#pragma unroll
-  for (int ri = 0; ri < kAdjAmps; ++ri) {
-    const auto d = cb[ct_ext<V>(ri)];
-    // K phi
-    const double kr = double(d.x) * double(F.re[ri]) - double(d.y) * double(F.im[ri]);
-    const double ki = double(d.x) * double(F.im[ri]) + double(d.y) * double(F.re[ri]);
-    // conj(lambda) * (K phi)
-    sr += double(G.re[ri]) * kr + double(G.im[ri]) * ki;
-    si += double(G.re[ri]) * ki - double(G.im[ri]) * kr;
-  }
-}
-
-// Inner-product contribution of one thread for a kSwInnerDense op on
-// register positions V (canonical coefficient order).
-template <typename Real, int V>
-__device__ __forceinline__ void inner_dense(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
-                                            const typename Vec2<Real>::T *__restrict__ c, double &sr,
-                                            double &si) {
-  constexpr int D = 1 << ct_popc<V>();
-#pragma unroll
-  for (int g = 0; g < kAdjAmps; ++g) {
-    if (g & V) continue;
-#pragma unroll
-    for (int r = 0; r < D; ++r) {
-      double kr = 0.0, ki = 0.0;
-#pragma unroll
-      for (int x = 0; x < D; ++x) {
-        const auto m = c[r * D + x];
-        const int ix = g | ct_dep<V>(x);
-        kr += double(m.x) * double(F.re[ix]) - double(m.y) * double(F.im[ix]);
-        ki += double(m.x) * double(F.im[ix]) + double(m.y) * double(F.re[ix]);
-      }
-      const int ir = g | ct_dep<V>(r);
-      sr += double(G.re[ir]) * kr + double(G.im[ir]) * ki;
-      si += double(G.re[ir]) * ki - double(G.im[ir]) * kr;
-    }
-  }
 }
 
 template <typename Real>

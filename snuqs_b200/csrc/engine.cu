@@ -1026,13 +1026,31 @@ int adjoint_sweep(sq_state *psi, sq_state *lam, const sq::PlannedSweep &ps, doub
     P->coef[2 * i + 1] = Real(ps.coef[i].imag());
   }
   const uint32_t m = ps.h.m;
-  const void *fn = adjoint_fn<Real>(m);
-  if (!fn) return fail(SQ_ERR_INVALID, "internal: no adjoint kernel for %u tile bits", m);
   const int threads = 1 << (m - sq::kAdjRegBits);
   const int nw = (threads + 31) / 32;
-  const size_t smem = adjoint_smem<Real>(m, ps.h.ncoef);
+  const void *fn = nullptr;
+  size_t smem = 0;
   int per_sm = 0;
-  SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  if (use_jit(psi)) {
+    std::string err;
+    fn = sq::jit_adjoint_kernel(ps, sizeof(Real) == 4, err);
+    smem = sq::jit_adjoint_smem(ps, sizeof(Real) == 4);
+    if (fn && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
+      cudaGetLastError();
+      fn = nullptr;
+    }
+    if (fn && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    sq::jit_note_launch(fn != nullptr);
+  }
+  if (!fn) {
+    fn = adjoint_fn<Real>(m);
+    if (!fn) return fail(SQ_ERR_INVALID, "internal: no adjoint kernel for %u tile bits", m);
+    smem = adjoint_smem<Real>(m, ps.h.ncoef);
+    SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  }
   if (per_sm < 1) per_sm = 1;
   const uint64_t grid = std::min<uint64_t>(
       std::min<uint64_t>(ps.h.num_tiles, uint64_t(per_sm) * sms), partial_rows / uint64_t(nw));
@@ -1099,6 +1117,12 @@ int adjoint_impl(sq_state *psi, sq_state *lam, const sq::AdjointPlan &ap, const 
       (reinterpret_cast<uintptr_t>(e_dev + 2) + 15) & ~uintptr_t(15));
   auto *partials = ipvals + nip;
   int status = SQ_OK;
+  if (use_jit(psi)) {
+    std::vector<const sq::PlannedSweep *> sweeps;
+    for (const auto &pl : rplan)
+      if (pl.is_sweep) sweeps.push_back(&pl.sweep);
+    sq::jit_prepare_adjoint(sweeps, sizeof(Real) == 4);
+  }
   auto run = [&]() -> int {
     SQ_CUDA(cudaMemsetAsync(ipvals, 0, nip * sizeof(double2), st));
     SQ_TRY(pauli_apply<Real>(psi, lam, paulis, w, nt, red, red_blocks, e_dev, st));

@@ -165,7 +165,7 @@ const std::string &prelude() {
 }
 
 // Loads (compiling when not cached) the kernel whose generated part is `body`.
-Entry &get_entry(const std::string &body) {
+Entry &get_entry(const std::string &body, const char *name = "sq_jit_sweep") {
   static const uint64_t prelude_hash = fnv1a(prelude());
   const uint64_t key = fnv1a(body) ^ (prelude_hash * 0x9e3779b97f4a7c15ull);
   {
@@ -200,7 +200,7 @@ Entry &get_entry(const std::string &body) {
   }
   if (!e.failed) {
     cudaError_t ce = cudaLibraryLoadData(&e.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-    if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&e.kernel, e.lib, "sq_jit_sweep");
+    if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&e.kernel, e.lib, name);
     if (ce != cudaSuccess) {
       e.failed = true;
       e.kernel = nullptr;
@@ -215,30 +215,30 @@ Entry &get_entry(const std::string &body) {
   return slot;
 }
 
-const char *op_routine(const SweepOp &op, bool c64, std::string &tmpl) {
+const char *op_routine(const SweepOp &op, bool c64, std::string &tmpl, int na = 16) {
   const char *R = c64 ? "float" : "double";
   const int V = op.vmask;
   std::ostringstream o;
   const bool pure = op.aux & kAuxPure;
   switch (op.kind) {
     case kSwPhase:
-      o << "op_phase<" << R << ", 16, " << (pure ? "true" : "false") << ">";
+      o << "op_phase<" << R << ", " << na << ", " << (pure ? "true" : "false") << ">";
       break;
     case kSwDiag:
-      o << "op_diag<" << R << ", 16, " << V << ">";
+      o << "op_diag<" << R << ", " << na << ", " << V << ">";
       break;
     case kSwAnti1:
-      o << "op_anti1<" << R << ", 16, " << V << ", " << (pure ? "true" : "false") << ">";
+      o << "op_anti1<" << R << ", " << na << ", " << V << ", " << (pure ? "true" : "false") << ">";
       break;
     case kSwSwap2:
-      o << "op_swap2<" << R << ", 16, " << V << ", " << (pure ? "true" : "false") << ">";
+      o << "op_swap2<" << R << ", " << na << ", " << V << ", " << (pure ? "true" : "false") << ">";
       break;
     case kSwXRot:
-      o << "op_xrot<" << R << ", 16, " << V << ", " << int(op.aux & kAuxXMask) << ", "
+      o << "op_xrot<" << R << ", " << na << ", " << V << ", " << int(op.aux & kAuxXMask) << ", "
         << ((op.aux & kAuxImag) ? "true" : "false") << ">";
       break;
     default:
-      o << "op_dense<" << R << ", 16, " << V << ">";
+      o << "op_dense<" << R << ", " << na << ", " << V << ">";
       break;
   }
   tmpl = o.str();
@@ -258,11 +258,12 @@ void jit_note_launch(bool jit) { (jit ? g_launches : g_fallbacks)++; }
 // swizzle images are linearly independent, the rest ascending.  A phase that
 // stores straight to HBM keeps all thread bits ascending (the lanes then
 // cover contiguous amplitudes).
-std::vector<int> thread_positions(const SweepPhase &ph, int m, bool c64, bool direct_store) {
+std::vector<int> thread_positions(const SweepPhase &ph, int m, bool c64, bool direct_store,
+                                  int nreg = kRegBits) {
   const int W = c64 ? Swz<float>::W : Swz<double>::W;
   const uint8_t *img = c64 ? Swz<float>::kImage : Swz<double>::kImage;
   uint32_t regs = 0;
-  for (int b = 0; b < kRegBits; ++b) regs |= 1u << ph.reg[b];
+  for (int b = 0; b < nreg; ++b) regs |= 1u << ph.reg[b];
   std::vector<int> nonreg;
   for (int p = 0; p < m; ++p)
     if (!((regs >> p) & 1)) nonreg.push_back(p);
@@ -400,6 +401,122 @@ std::string jit_source(const PlannedSweep &ps, bool c64, int minb) {
   return prelude() + jit_body(ps, c64, minb);
 }
 
+// Source of the JIT kernel of one reverse (two-state) adjoint sweep; empty
+// when the sweep holds an op the generated form does not cover (the generic
+// adjoint kernel then runs it).
+std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb) {
+  const char *R = c64 ? "float" : "double";
+  const int M = int(ps.h.m);
+  const int NT = 1 << (M - kAdjRegBits);
+  std::ostringstream s;
+  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << minb
+    << ")\nsq_jit_adjoint(Vec2<" << R << ">::T *__restrict__ psi, Vec2<" << R
+    << ">::T *__restrict__ lam, const __grid_constant__ SweepParams<" << R
+    << "> P, double2 *__restrict__ partials) {\n";
+  s << "  using C2 = Vec2<" << R << ">::T;\n";
+  s << "  using Tile = JitTile<" << M << ", " << ps.h.l;
+  for (uint32_t i = 0; i < ps.h.m - ps.h.l; ++i) s << ", " << int(ps.h.hi[i]);
+  s << ">;\n";
+  s << "  jit_adjoint_sweep<" << R << ", " << M
+    << ", Tile>(psi, lam, P, partials, [&](C2 *ft, C2 *lt, const C2 *coef, uint64_t gbase, double2 *acc) {\n";
+  auto diag_bits = [&](const SweepOp &op) {
+    std::ostringstream b;
+    b << "uint32_t b = 0;";
+    for (int t = 0; t < op.ndt; ++t) {
+      if (op.dsrc[t] == kSrcGlobal)
+        b << " b = (b << 1) | (uint32_t(gbase >> " << int(op.dpos[t]) << ") & 1u);";
+      else
+        b << " b = (b << 1) | ((jb >> " << int(op.dpos[t]) << ") & 1u);";
+    }
+    return b.str();
+  };
+  for (uint32_t p = 0; p < ps.h.nphases; ++p) {
+    const SweepPhase &ph = ps.ph[p];
+    s << "    {\n      using Ph = JitPhase2<" << R << ", " << M << ", Tile, " << int(ph.reg[0]) << ", "
+      << int(ph.reg[1]) << ", " << int(ph.reg[2]);
+    for (int t : thread_positions(ph, M, c64, false, kAdjRegBits)) s << ", " << t;
+    s << ">;\n";
+    s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << ", " << kAdjAmps
+      << "> F, G;\n      Ph::gather(F, G, ft, lt, jb);\n";
+    for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
+      const SweepOp &op = ps.op[oi];
+      if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
+        // Inner products carry no conditions (as in the generic kernel).
+        if (op.gmask || op.lmask || op.rmask || op.slot >= uint32_t(kMaxInner)) return std::string();
+        s << "      { double sr = 0.0, si = 0.0; ";
+        if (op.kind == kSwInnerDiag)
+          s << diag_bits(op) << " inner_diag<" << R << ", " << int(op.vmask) << ">(F, G, coef + " << op.coef
+            << ", b, sr, si); ";
+        else
+          s << "inner_dense<" << R << ", " << int(op.vmask) << ">(F, G, coef + " << op.coef << ", sr, si); ";
+        s << "jit_inner_acc<" << NT << ", " << op.slot << ">(acc, sr, si); }\n";
+        continue;
+      }
+      s << "      ";
+      if (op.gmask || op.lmask) {
+        s << "if (";
+        if (op.gmask)
+          s << "(gbase & 0x" << std::hex << op.gmask << "ull) == 0x" << op.gval << "ull" << std::dec;
+        if (op.gmask && op.lmask) s << " && ";
+        if (op.lmask) s << "(jb & 0x" << std::hex << op.lmask << "u) == 0x" << op.lval << "u" << std::dec;
+        s << ") ";
+      }
+      std::string tmpl;
+      op_routine(op, c64, tmpl, kAdjAmps);
+      std::ostringstream cexpr;
+      if (lane_indexed(op))
+        cexpr << "coef + " << op.coef;
+      else
+        cexpr << "ParamCoef<" << R << ", " << op.coef << ">{P.coef}";
+      if (op.kind == kSwDiag) {
+        s << "{ " << diag_bits(op) << " " << tmpl << "(F, " << cexpr.str() << ", b); " << tmpl << "(G, "
+          << cexpr.str() << ", b); }\n";
+      } else {
+        s << "{ " << tmpl << "(F, " << cexpr.str() << ", " << int(op.rmask) << ", " << int(op.rval) << "); "
+          << tmpl << "(G, " << cexpr.str() << ", " << int(op.rmask) << ", " << int(op.rval) << "); }\n";
+      }
+    }
+    s << "      Ph::scatter(F, G, ft, lt, jb);\n      __syncthreads();\n    }\n";
+  }
+  s << "  });\n}\n";
+  return s.str();
+}
+
+size_t jit_adjoint_smem(const PlannedSweep &ps, bool c64) {
+  return jit_adjoint_smem_bytes(int(ps.h.m), c64 ? 8 : 16, ps.h.ncoef);
+}
+
+const void *jit_adjoint_kernel(const PlannedSweep &ps, bool c64, std::string &err) {
+  const std::string body = jit_adjoint_body(ps, c64, 2);
+  if (body.empty()) {
+    err = "sweep not covered by the JIT adjoint form";
+    return nullptr;
+  }
+  Entry &e = get_entry(body, "sq_jit_adjoint");
+  if (e.failed) {
+    err = e.err;
+    return nullptr;
+  }
+  return reinterpret_cast<const void *>(e.kernel);
+}
+
+void jit_prepare_adjoint(const std::vector<const PlannedSweep *> &sweeps, bool c64) {
+  if (!jit_available() || sweeps.empty()) return;
+  std::vector<std::string> bodies;
+  for (const auto *ps : sweeps) {
+    std::string b = jit_adjoint_body(*ps, c64, 2);
+    if (!b.empty()) bodies.push_back(std::move(b));
+  }
+  std::atomic<size_t> next{0};
+  const unsigned nth = std::max(1u, std::min<unsigned>(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < std::min<size_t>(nth, bodies.size()); ++t)
+    pool.emplace_back([&] {
+      for (size_t i = next++; i < bodies.size(); i = next++) get_entry(bodies[i], "sq_jit_adjoint");
+    });
+  for (auto &th : pool) th.join();
+}
+
 size_t jit_smem(const PlannedSweep &ps, bool c64) {
   const JitShape js = jit_shape(ps, c64);
   return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload, js.smem_coef ? (ps.h.ncoef + 1) & ~1u : 0u);
@@ -486,6 +603,45 @@ extern "C" int sq_jit_source(uint32_t num_qubits, int dtype, const sq_circuit_op
   if (sweep_index >= sweeps.size()) return sq_detail_fail(SQ_ERR_INVALID, "no such sweep");
   const sq::PlannedSweep &ps = *sweeps[sweep_index];
   const std::string src = sq::jit_source(ps, c64, sq::jit_minb(c64, ps.h.m));
+  *len = src.size();
+  if (buf && cap) {
+    const size_t n = std::min<size_t>(cap - 1, src.size());
+    std::memcpy(buf, src.data(), n);
+    buf[n] = '\0';
+  }
+  return SQ_OK;
+}
+
+extern "C" int sq_jit_adjoint_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops,
+                                     uint32_t nops, uint32_t sweep_index, char *buf, uint64_t cap,
+                                     uint64_t *len, uint32_t *nsweeps) {
+  if ((nops && !ops) || !len) return sq_detail_fail(SQ_ERR_INVALID, "null pointer");
+  if (dtype != SQ_C128 && dtype != SQ_C64) return sq_detail_fail(SQ_ERR_INVALID, "bad dtype");
+  if (num_qubits < uint32_t(sq::kRegBits) || num_qubits > 40)
+    return sq_detail_fail(SQ_ERR_INVALID, "num_qubits out of range");
+  const bool c64 = dtype == SQ_C64;
+  std::vector<sq::PlannedLaunch> plan;
+  try {
+    sq::AdjointPlan ap;
+    sq::build_adjoint(ops, nops, num_qubits, ap);
+    sq::PlanOptions opt;
+    opt.tile_bits = 0;
+    const auto &tb = c64 ? sq::kAdjTileBitsC64 : sq::kAdjTileBitsC128;
+    for (int m : tb)
+      if (uint32_t(m) <= num_qubits) opt.tile_bits = uint32_t(m);
+    opt.reg_bits = sq::kAdjRegBits;
+    opt.max_dense_k = sq::kAdjRegBits;
+    plan = sq::plan_sweeps(ap.reverse, num_qubits, opt);
+  } catch (const std::exception &e) {
+    return sq_detail_fail(SQ_ERR_INVALID, e.what());
+  }
+  std::vector<const sq::PlannedSweep *> sweeps;
+  for (const auto &pl : plan)
+    if (pl.is_sweep) sweeps.push_back(&pl.sweep);
+  if (nsweeps) *nsweeps = uint32_t(sweeps.size());
+  if (sweep_index >= sweeps.size()) return sq_detail_fail(SQ_ERR_INVALID, "no such sweep");
+  const std::string body = sq::jit_adjoint_body(*sweeps[sweep_index], c64, 2);
+  const std::string src = body.empty() ? std::string() : sq::prelude() + body;
   *len = src.size();
   if (buf && cap) {
     const size_t n = std::min<size_t>(cap - 1, src.size());

@@ -21,6 +21,13 @@ int jit_minb(bool c64, uint32_t m);
 // Launchable kernel (a cudaKernel_t as const void*) for `ps`, compiling and
 // caching it on first use; nullptr with `err` set when it cannot be built.
 const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err);
+// Two-state (adjoint reverse) sweeps: the JIT kernel (cudaKernel_t as const
+// void*, or nullptr with `err`), its dynamic shared memory, its source, and
+// a parallel pre-compile of several sweeps.
+const void *jit_adjoint_kernel(const PlannedSweep &ps, bool c64, std::string &err);
+size_t jit_adjoint_smem(const PlannedSweep &ps, bool c64);
+std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb);
+void jit_prepare_adjoint(const std::vector<const PlannedSweep *> &sweeps, bool c64);
 // Compiles the kernels of several sweeps in parallel (fills the cache).
 void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64);
 

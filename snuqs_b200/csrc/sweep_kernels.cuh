@@ -516,6 +516,59 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
 // each phase compiles to straight-line code: no op dispatch, and no register
 // shuffling back to fixed registers between gates.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Two-state (adjoint) building blocks shared by the generic adjoint kernel
+// (adjoint_kernels.cuh) and the JIT-specialised one: 8 amplitudes of phi and
+// the same 8 of lambda per thread (3 register bits).
+// ---------------------------------------------------------------------------
+constexpr int kAdjRegBits = 3;
+constexpr int kAdjAmps = 1 << kAdjRegBits;
+
+// Inner-product contribution of one thread for a kSwInnerDiag op.
+template <typename Real, int V>
+__device__ __forceinline__ void inner_diag(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                           const typename Vec2<Real>::T *__restrict__ c,
+                                           uint32_t base, double &sr, double &si) {
+  const auto *cb = c + (base << ct_popc<V>());
+#pragma unroll
+  for (int ri = 0; ri < kAdjAmps; ++ri) {
+    const auto d = cb[ct_ext<V>(ri)];
+    // K phi
+    const double kr = double(d.x) * double(F.re[ri]) - double(d.y) * double(F.im[ri]);
+    const double ki = double(d.x) * double(F.im[ri]) + double(d.y) * double(F.re[ri]);
+    // conj(lambda) * (K phi)
+    sr += double(G.re[ri]) * kr + double(G.im[ri]) * ki;
+    si += double(G.re[ri]) * ki - double(G.im[ri]) * kr;
+  }
+}
+
+// Inner-product contribution of one thread for a kSwInnerDense op on
+// register positions V (canonical coefficient order).
+template <typename Real, int V>
+__device__ __forceinline__ void inner_dense(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                            const typename Vec2<Real>::T *__restrict__ c, double &sr,
+                                            double &si) {
+  constexpr int D = 1 << ct_popc<V>();
+#pragma unroll
+  for (int g = 0; g < kAdjAmps; ++g) {
+    if (g & V) continue;
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+      double kr = 0.0, ki = 0.0;
+#pragma unroll
+      for (int x = 0; x < D; ++x) {
+        const auto m = c[r * D + x];
+        const int ix = g | ct_dep<V>(x);
+        kr += double(m.x) * double(F.re[ix]) - double(m.y) * double(F.im[ix]);
+        ki += double(m.x) * double(F.im[ix]) + double(m.y) * double(F.re[ix]);
+      }
+      const int ir = g | ct_dep<V>(r);
+      sr += double(G.re[ir]) * kr + double(G.im[ir]) * ki;
+      si += double(G.re[ir]) * ki - double(G.im[ir]) * kr;
+    }
+  }
+}
+
 // Coefficients read straight from the kernel's parameter block (constant
 // bank) at compile-time offsets: no shared-memory load per coefficient, and
 // one compiled kernel still serves every coefficient value.
@@ -701,6 +754,155 @@ __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ p
     cp_async_wait_prev();
     asm volatile("cp.async.wait_all;\n" ::: "memory");
   }
+}
+
+// ---------------------------------------------------------------------------
+// JIT-specialised two-state (adjoint reverse) sweeps: the generated kernel
+// un-computes phi and lambda together and accumulates <lambda| K |phi> for
+// each inner-product op, with the same plan, shared-memory layout and
+// per-warp partial sums as adjoint_sweep_kernel (adjoint_kernels.cuh).
+// ---------------------------------------------------------------------------
+template <typename Real, int M, class Tile, int R0, int R1, int R2, int... T>
+struct JitPhase2 {
+  using C2 = typename Vec2<Real>::T;
+  static_assert(sizeof...(T) == M - kAdjRegBits, "one tile position per thread bit");
+  __device__ __forceinline__ static uint32_t jb(uint32_t tid) {
+    uint32_t x = 0;
+    int i = 0;
+    ((x |= ((tid >> i++) & 1u) << T), ...);
+    return x;
+  }
+  __device__ __forceinline__ static uint32_t slot(uint32_t sb, int ri) {
+    constexpr uint32_t W0 = swz_c<Real>(1u << R0), W1 = swz_c<Real>(1u << R1);
+    constexpr uint32_t W2 = swz_c<Real>(1u << R2);
+    return sb ^ ((ri & 1) ? W0 : 0u) ^ ((ri & 2) ? W1 : 0u) ^ ((ri & 4) ? W2 : 0u);
+  }
+  __device__ __forceinline__ static void gather(Amps<Real, kAdjAmps> &F, Amps<Real, kAdjAmps> &G,
+                                                const C2 *ft, const C2 *lt, uint32_t jbv) {
+    const uint32_t sb = swz<Real>(jbv);
+#pragma unroll
+    for (int ri = 0; ri < kAdjAmps; ++ri) {
+      const C2 a = ft[slot(sb, ri)], b = lt[slot(sb, ri)];
+      F.re[ri] = a.x;
+      F.im[ri] = a.y;
+      G.re[ri] = b.x;
+      G.im[ri] = b.y;
+    }
+  }
+  __device__ __forceinline__ static void scatter(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                                 C2 *ft, C2 *lt, uint32_t jbv) {
+    const uint32_t sb = swz<Real>(jbv);
+#pragma unroll
+    for (int ri = 0; ri < kAdjAmps; ++ri) {
+      C2 a, b;
+      a.x = F.re[ri];
+      a.y = F.im[ri];
+      b.x = G.re[ri];
+      b.y = G.im[ri];
+      ft[slot(sb, ri)] = a;
+      lt[slot(sb, ri)] = b;
+    }
+  }
+};
+
+// Adds one thread's inner-product share to its warp's slot (warp shuffle,
+// then lane 0 adds to acc[warp * kMaxInner + SLOT]).
+template <int NT, int SLOT>
+__device__ __forceinline__ void jit_inner_acc(double2 *acc, double sr, double si) {
+  constexpr unsigned kMask = NT >= 32 ? 0xffffffffu : ((1u << NT) - 1u);
+#pragma unroll
+  for (int off = (NT >= 32 ? 16 : NT / 2); off > 0; off >>= 1) {
+    sr += __shfl_xor_sync(kMask, sr, off);
+    si += __shfl_xor_sync(kMask, si, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    double2 &a = acc[(threadIdx.x >> 5) * kMaxInner + SLOT];
+    a.x += sr;
+    a.y += si;
+  }
+}
+
+// Dynamic shared memory of a JIT adjoint sweep: phi tiles (2 buffers) |
+// lambda tiles (2 buffers) | coefficients | per-warp inner-product slots.
+__host__ __device__ constexpr size_t jit_adjoint_smem_bytes(int m, size_t amp_bytes, uint32_t ncoef) {
+  return 4 * (size_t(1) << m) * amp_bytes + size_t((ncoef + 1) & ~1u) * amp_bytes +
+         size_t(((1 << (m - kAdjRegBits)) + 31) / 32) * kMaxInner * 16;
+}
+
+// The two-state tile loop with the phases supplied by the generated kernel:
+// phases(ft, lt, coef, gbase, acc) runs every phase of one tile pair.
+// partials[(block * warps + warp) * kMaxInner + slot] receives each warp's
+// sums at the end (as adjoint_sweep_kernel).
+template <typename Real, int M, class Tile, class Phases>
+__device__ __forceinline__ void jit_adjoint_sweep(typename Vec2<Real>::T *__restrict__ psi,
+                                                  typename Vec2<Real>::T *__restrict__ lam,
+                                                  const SweepParams<Real> &P, double2 *__restrict__ partials,
+                                                  Phases phases) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int NT = 1 << (M - kAdjRegBits);
+  constexpr int NW = (NT + 31) / 32;
+  constexpr uint32_t TS = 1u << M;
+  constexpr uint32_t PER = TS / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const SweepHeader &h = P.h;
+  C2 *fbufs = reinterpret_cast<C2 *>(smem_raw);
+  C2 *lbufs = fbufs + 2 * TS;
+  C2 *coef = lbufs + 2 * TS;
+  double2 *acc = reinterpret_cast<double2 *>(coef + ((h.ncoef + 1) & ~1u));
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t i = tid; i < h.ncoef; i += NT) {
+    C2 v;
+    v.x = P.coef[2 * i];
+    v.y = P.coef[2 * i + 1];
+    coef[i] = v;
+  }
+  for (uint32_t i = tid; i < NW * kMaxInner; i += NT) {
+    double2 z;
+    z.x = 0.0;
+    z.y = 0.0;
+    acc[i] = z;
+  }
+  __syncthreads();
+  const uint32_t s_tid = swz<Real>(tid);
+  const uint64_t toff = Tile::off(tid);
+  auto prefetch = [&](uint64_t t, C2 *fdst, C2 *ldst) {
+    const uint64_t g0 = Tile::base(t) | toff;
+#pragma unroll
+    for (uint32_t it = 0; it < PER; ++it) {
+      const uint64_t g = g0 | Tile::off(it * NT);
+      const uint32_t s = s_tid ^ swz<Real>(it * NT);
+      cp_async<sizeof(C2)>(fdst + s, psi + g);
+      cp_async<sizeof(C2)>(ldst + s, lam + g);
+    }
+  };
+  uint32_t cur = 0;
+  if (blockIdx.x < h.num_tiles) prefetch(blockIdx.x, fbufs, lbufs);
+  cp_async_commit();
+  for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
+    C2 *ft = fbufs + cur * TS, *lt = lbufs + cur * TS;
+    const uint64_t tn = t + gridDim.x;
+    if (tn < h.num_tiles) prefetch(tn, fbufs + (cur ^ 1) * TS, lbufs + (cur ^ 1) * TS);
+    cp_async_commit();
+    cp_async_wait_prev();
+    __syncthreads();
+    const uint64_t gbase = Tile::base(t);
+    phases(ft, lt, coef, gbase, acc);
+    const uint64_t g0 = gbase | toff;
+#pragma unroll
+    for (uint32_t it = 0; it < PER; ++it) {
+      const uint64_t g = g0 | Tile::off(it * NT);
+      const uint32_t s = s_tid ^ swz<Real>(it * NT);
+      psi[g] = ft[s];
+      lam[g] = lt[s];
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  cp_async_wait_prev();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  for (uint32_t i = tid; i < NW * kMaxInner; i += NT)
+    partials[size_t(blockIdx.x) * NW * kMaxInner + i] = acc[i];
 }
 
 // ---------------------------------------------------------------------------

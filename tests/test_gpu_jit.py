@@ -107,3 +107,31 @@ def test_low_bits_large_state_matches_default(dtype):
     a = run(ops, n, dtype, jit=1, low_bits=5)
     b = run(ops, n, dtype, jit=0)
     assert np.abs(a - b).max() <= (1e-13 if dtype == capi.SQ_C128 else 1e-6)
+
+
+@pytest.mark.parametrize("dtype", [capi.SQ_C128, capi.SQ_C64])
+def test_jit_adjoint_matches_generic_adjoint(dtype):
+    from snuqs_b200 import adjoint
+    from tests.test_adjoint_cpu import random_param_circuit
+
+    edges = circuits.random_regular_graph(20, 3, seed=2)
+    qaoa = [("Hadamard", (q,), ()) for q in range(20)]
+    for l in range(2):
+        qaoa += [("ZZ", (i, j), (0.0,), (l,)) for i, j in edges]
+        qaoa += [("RotX", (q,), (0.0,), (2 + l,)) for q in range(20)]
+    cases = [(20, qaoa, circuits.maxcut_hamiltonian(20, edges), 4),
+             (14, random_param_circuit(14, 40, 6, 5), circuits.random_pauli_hamiltonian(14, 12, seed=5), 6)]
+    for n, ops, terms, npar in cases:
+        theta = np.random.default_rng(n).uniform(-3, 3, npar)
+        res = {}
+        for jit in (0, 1):
+            ws = adjoint.Workspace(n, dtype)
+            ws.psi.set_option(capi.SQ_OPT_JIT, jit)
+            before = capi.jit_info()[1]
+            res[jit] = adjoint.adjoint_gradient(ws, ops, theta, terms, npar)
+            if jit:
+                assert capi.jit_info()[1] > before, "the JIT kernels did not run"
+            ws.close()
+        tol = 1e-10 if dtype == capi.SQ_C128 else 1e-4
+        assert abs(res[0][0] - res[1][0]) <= tol
+        assert np.abs(res[0][1] - res[1][1]).max() <= tol * max(1.0, np.abs(res[0][1]).max())

@@ -101,3 +101,29 @@ def test_lane_placement_is_a_permutation_and_conflict_free(dtype):
     # Every phase except the direct-store ones (ascending lanes from tile
     # position 0, also conflict-free) gets independent lane images.
     assert conflict_free == phases
+
+
+def _qaoa(n, p, seed):
+    edges = circuits.random_regular_graph(n, 3, seed=seed)
+    ops = [("Hadamard", (q,), ()) for q in range(n)]
+    for l in range(p):
+        ops += [("ZZ", (i, j), (0.3,), (l,)) for i, j in edges]
+        ops += [("RotX", (q,), (0.7,), (p + l,)) for q in range(n)]
+    return ops
+
+
+@pytest.mark.parametrize("dtype", [capi.SQ_C128, capi.SQ_C64])
+def test_adjoint_sources_compile(dtype):
+    from tests.test_adjoint_cpu import random_param_circuit
+
+    cases = [(20, _qaoa(20, 2, seed=1)), (14, random_param_circuit(14, 40, 6, 3))]
+    compiled = 0
+    for n, ops in cases:
+        srcs = capi.jit_sources(n, ops, dtype, adjoint=True)
+        assert srcs
+        for src in srcs[:6]:
+            if src:
+                assert "sq_jit_adjoint" in src
+                capi.jit_compile(src)
+                compiled += 1
+    assert compiled > 0
