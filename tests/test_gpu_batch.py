@@ -110,3 +110,16 @@ def test_batch_option_validation():
     with pytest.raises(capi.SqError):
         b.set_option(capi.SQ_BOPT_MAX_OPS, 65)
     b.close()
+
+
+def test_sharded_runner_on_one_rank_matches_batch():
+    from snuqs_b200 import sharding
+
+    sizes = [6, 9, 12, 13, 8]
+    cs = {}
+    for i, n in enumerate(sizes):
+        cs[i] = (n, circuits.random_all_gates(n, 40, seed=300 + i), circuits.random_pauli_hamiltonian(n, 8, seed=i))
+    got = sharding.run_sharded(sizes, sharding.batch_runner(capi.SQ_C128, lambda i: cs[i]), 0, 1)
+    for i, (n, ops, terms) in cs.items():
+        want = oracle.expectation(oracle.run_ops(ops, n), n, terms)
+        assert abs(got[i] - want) <= 1e-11
