@@ -556,13 +556,15 @@ def batch_metric_sharded(precision: str, rank: int, world: int, ncirc: int = 409
             hams[n] = b.add_hamiltonian(n, terms)
         b.add_circuit(n, ops, hams[n])
     b.run()  # plan, allocate, capture
-    dist.barrier()
+    if world > 1:
+        dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e = b.run()
     t = torch.tensor([time.perf_counter() - t0, b.last_timing()[0] * 1e-3], device="cuda",
                      dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
     energies = sharding.gather_results(e, share, len(sizes), rank, world)
     b.close()
     return {"workload": f"vqe_batch_{ncirc}x_8to20q_{precision}", "circuits": ncirc,

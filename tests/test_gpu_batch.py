@@ -123,3 +123,17 @@ def test_sharded_runner_on_one_rank_matches_batch():
     for i, (n, ops, terms) in cs.items():
         want = oracle.expectation(oracle.run_ops(ops, n), n, terms)
         assert abs(got[i] - want) <= 1e-11
+
+
+def test_bench_sharded_batch_metric_one_rank():
+    import bench
+
+    out = bench.batch_metric_sharded("complex128", 0, 1, ncirc=64)
+    assert out["circuits"] == 64 and out["energies_per_s"] > 0
+    sizes, circuit_of = bench.vqe_batch_circuits(64)
+    b = capi.Batch(capi.SQ_C128)
+    for i in range(64):
+        n, ops, terms = circuit_of(i)
+        b.add_circuit(n, ops, b.add_hamiltonian(n, terms))
+    assert abs(float(np.sum(b.run())) - out["energy_checksum"]) <= 1e-9
+    b.close()
