@@ -41,7 +41,7 @@ ADJOINT_INSTANCES = [("double", 4), ("double", 7), ("double", 10),
 BATCH_INSTANCES = [("double", 10), ("double", 11), ("double", 12),
                    ("float", 10), ("float", 11), ("float", 12)]
 # Batched adjoint-gradient kernels: (precision, tile bits); must match kBatchTileBits*.
-BATCH_ADJ_INSTANCES = [("double", 11), ("float", 12)]
+BATCH_ADJ_INSTANCES = [("double", 10), ("double", 11), ("float", 11), ("float", 12)]
 LIB = os.path.join(HERE, "libsnuqs_b200.so")
 
 

@@ -261,6 +261,28 @@ const void *batch_fn(uint32_t m) {
   return nullptr;
 }
 
+// Gradient kernel of (precision, tile bits); nullptr when not compiled.
+template <typename Real>
+const void *batch_adj_fn(uint32_t m) {
+  if constexpr (sizeof(Real) == 8) {
+    switch (m) {
+      case 10: return SQ_BATCH_ADJ_PTR_NAME(double, 10)();
+      case 11: return SQ_BATCH_ADJ_PTR_NAME(double, 11)();
+    }
+  } else {
+    switch (m) {
+      case 11: return SQ_BATCH_ADJ_PTR_NAME(float, 11)();
+      case 12: return SQ_BATCH_ADJ_PTR_NAME(float, 12)();
+    }
+  }
+  return nullptr;
+}
+
+template <typename Real>
+uint32_t batch_default_bits() {
+  return uint32_t(sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128);
+}
+
 template <typename Real>
 uint32_t batch_tile_bits(const sq_batch *b) {
   return b->tile_bits ? b->tile_bits : uint32_t(sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128);
@@ -483,7 +505,9 @@ bool plan_gradient_circuit(const Circ &c, uint32_t m, std::vector<unsigned char>
 template <typename Real>
 int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *grads, cudaStream_t st) {
   using C2 = typename sq::Vec2<Real>::T;
-  const uint32_t M = sizeof(Real) == 4 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128;
+  // Tile bits of the gradient kernel: the batch's SQ_BOPT_TILE_BITS when a
+  // gradient kernel of that size exists, else the precision's default.
+  const uint32_t M = batch_adj_fn<Real>(b->tile_bits) ? b->tile_bits : batch_default_bits<Real>();
   const size_t nc = b->circs.size();
   if (nc == 0) return SQ_OK;
   // This run restages the shared buffers: the energy run's plan cache and
@@ -571,7 +595,7 @@ int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *
     t.plan_off = off;
     off += packed[id].size();
   }
-  const void *fn = sizeof(Real) == 4 ? SQ_BATCH_ADJ_PTR_NAME(float, 12)() : SQ_BATCH_ADJ_PTR_NAME(double, 11)();
+  const void *fn = batch_adj_fn<Real>(M);
   const uint32_t L = uint32_t(sq::sweep_low_bits(int(M)));
   const int threads = 1 << (M - sq::kAdjRegBits);
   const size_t nw = size_t(threads + 31) / 32;

@@ -35,5 +35,7 @@ const void *SQ_BATCH_PTR_NAME(float, 10)();
 const void *SQ_BATCH_PTR_NAME(float, 11)();
 const void *SQ_BATCH_PTR_NAME(float, 12)();
 #define SQ_BATCH_ADJ_PTR_NAME(real, m) SQ_SWEEP_CAT(sq_batch_adjoint_kernel_ptr, real, m)
+const void *SQ_BATCH_ADJ_PTR_NAME(double, 10)();
 const void *SQ_BATCH_ADJ_PTR_NAME(double, 11)();
+const void *SQ_BATCH_ADJ_PTR_NAME(float, 11)();
 const void *SQ_BATCH_ADJ_PTR_NAME(float, 12)();

@@ -93,3 +93,19 @@ def test_batch_gradient_parameter_index_checked():
     with pytest.raises(capi.SqError, match="n_params"):
         b.run_gradients(npar - 1)
     b.close()
+
+
+@pytest.mark.parametrize("dtype,tiles,tol", [(capi.SQ_C128, (10, 11), 1e-10), (capi.SQ_C64, (11, 12), 1e-4)])
+def test_batch_gradient_tile_sizes_agree(dtype, tiles, tol):
+    cs = cases(11)
+    n_params = max(c[4] for c in cs)
+    b = capi.Batch(dtype)
+    for n, ops, theta, terms, _ in cs:
+        b.add_circuit(n, adjoint.bind(ops, theta), b.add_hamiltonian(n, terms))
+    res = []
+    for tb in tiles:
+        b.set_option(capi.SQ_BOPT_TILE_BITS, tb)
+        res.append(b.run_gradients(n_params))
+    assert np.abs(res[0][0] - res[1][0]).max() <= tol
+    assert np.abs(res[0][1] - res[1][1]).max() <= tol * max(1.0, np.abs(res[0][1]).max())
+    b.close()
