@@ -308,6 +308,12 @@ int sq_batch_autotune(sq_batch *b, uint32_t reps, sq_batch_config *best, void *s
  * (row = circuit id), energies one double per circuit.  Synchronous. */
 int sq_batch_run_gradients(sq_batch *b, uint32_t n_params, double *energies, double *grads,
                            void *stream);
+/* Test hook: CUDA source of the JIT batched-gradient kernel that
+ * sq_batch_run_gradients uses when every circuit of a batch shares this
+ * circuit's plan structure (num_qubits above the batch tile bits); *len = 0
+ * when the plan is not covered.  Needs no GPU. */
+int sq_jit_batch_adjoint_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
+                                char *buf, uint64_t cap, uint64_t *len);
 /* Final state of a circuit (needs SQ_BOPT_KEEP_STATES before sq_batch_run);
  * host_dst receives 2^n amplitudes of the batch's precision. */
 int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream);

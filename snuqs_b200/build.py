@@ -75,7 +75,8 @@ def _write_jit_sources() -> None:
     """Embeds the sweep headers in the library (NVRTC compiles them at run time)."""
     out = os.path.join(BUILD, "jit_sources.inc")
     parts = []
-    for var, fname in (("kJitPlanSource", "sq_plan.h"), ("kJitSweepSource", "sweep_kernels.cuh")):
+    for var, fname in (("kJitPlanSource", "sq_plan.h"), ("kJitSweepSource", "sweep_kernels.cuh"),
+                       ("kJitReduceSource", "reduce_kernels.cuh"), ("kJitBatchSource", "jit_batch.cuh")):
         text = open(os.path.join(CSRC, fname)).read()
         assert ")SQJIT\"" not in text
         parts.append(f'static const char {var}[] = R"SQJIT({text})SQJIT";\n')

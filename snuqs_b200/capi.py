@@ -75,6 +75,7 @@ SIGNATURES = {
     "sq_jit_compile": (_I, [ctypes.c_char_p]),
     "sq_jit_source": (_I, [_U32, _I, _P, _U32, _U32, ctypes.c_char_p, _U64, _PU64, _PU32]),
     "sq_jit_adjoint_source": (_I, [_U32, _I, _P, _U32, _U32, ctypes.c_char_p, _U64, _PU64, _PU32]),
+    "sq_jit_batch_adjoint_source": (_I, [_U32, _I, _P, _U32, ctypes.c_char_p, _U64, _PU64]),
     "sq_apply_gate_buffer": (_I, [_P, _P, _PU64, _U32, _U32, _U64, _P]),
     "sq_copy_to_host": (_I, [_P, _P, _P]),
     "sq_copy_from_host": (_I, [_P, _P, _P]),
@@ -141,6 +142,19 @@ def jit_sources(n: int, ops, dtype: int = SQ_C128, limit: int | None = None, adj
         out.append(buf.value.decode())
     del keep
     return out
+
+
+def jit_batch_adjoint_source(n: int, ops, dtype: int = SQ_C128) -> str:
+    """Source of the JIT batched-gradient kernel for batches of circuits
+    sharing the structure of `ops` ("" when not covered)."""
+    arr, keep = circuit_ops(ops)
+    ln = _U64(0)
+    check(lib().sq_jit_batch_adjoint_source(n, dtype, ctypes.cast(arr, _P), len(ops), None, 0, ctypes.byref(ln)))
+    buf = ctypes.create_string_buffer(ln.value + 1)
+    check(lib().sq_jit_batch_adjoint_source(n, dtype, ctypes.cast(arr, _P), len(ops), buf, ln.value + 1,
+                                            ctypes.byref(ln)))
+    del keep
+    return buf.value.decode()
 
 
 def jit_compile(source: str) -> None:

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -20,6 +21,7 @@
 #include "adjoint_plan.h"
 #include "batch_kernels.cuh"
 #include "host_ops.h"
+#include "jit.h"
 #include "sweep_registry.h"
 
 int sq_detail_fail(int code, const char *msg);
@@ -107,6 +109,7 @@ struct sq_batch {
   float last_ms = 0.f;
   uint32_t last_ctas = 0;
   const void *graph_fn = nullptr;
+  bool last_jit = false;  // the last gradient run used the JIT kernel
   // Launch configuration (0 = default): tile bits, low bits of a streamed
   // tile, ops per sweep, CTAs per SM.
   uint32_t tile_bits = 0, low_bits = 0, max_ops = 0, ctas_per_sm = 0;
@@ -502,6 +505,41 @@ bool plan_gradient_circuit(const Circ &c, uint32_t m, std::vector<unsigned char>
   }
 }
 
+// True when every circuit streams its states (n > M) and all packed plans are
+// identical except for their coefficient values (SQ_JIT=0 turns the JIT path
+// off).
+template <typename Real>
+bool uniform_plans(const sq_batch *b, const std::vector<std::vector<unsigned char>> &packed,
+                   const std::vector<uint32_t> &nfwd, const std::vector<uint32_t> &nrev,
+                   const std::vector<std::vector<std::pair<int32_t, double>>> &occs, uint32_t M) {
+  using C2 = typename sq::Vec2<Real>::T;
+  const char *env = std::getenv("SQ_JIT");
+  if ((env && env[0] == '0') || !sq::jit_available() || b->circs.empty()) return false;
+  const size_t nc = b->circs.size();
+  const uint32_t n = b->circs[0].n;
+  if (n <= M) return false;
+  const std::vector<unsigned char> &p0 = packed[0];
+  // Coefficient byte ranges of circuit 0's records.
+  std::vector<std::pair<size_t, size_t>> holes;
+  for (size_t off = 0; off < p0.size();) {
+    const auto &ps = *reinterpret_cast<const sq::PackedSweep *>(p0.data() + off);
+    holes.emplace_back(off + ps.coef_off, off + ps.coef_off + size_t(ps.h.ncoef) * sizeof(C2));
+    off += ps.bytes;
+  }
+  for (size_t i = 1; i < nc; ++i) {
+    if (b->circs[i].n != n || nfwd[i] != nfwd[0] || nrev[i] != nrev[0] || packed[i].size() != p0.size() ||
+        occs[i] != occs[0])
+      return false;
+    size_t pos = 0;
+    for (const auto &h : holes) {
+      if (std::memcmp(packed[i].data() + pos, p0.data() + pos, h.first - pos) != 0) return false;
+      pos = h.second;
+    }
+    if (std::memcmp(packed[i].data() + pos, p0.data() + pos, p0.size() - pos) != 0) return false;
+  }
+  return true;
+}
+
 template <typename Real>
 int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *grads, cudaStream_t st) {
   using C2 = typename sq::Vec2<Real>::T;
@@ -535,6 +573,14 @@ int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *
       if (o.first >= int32_t(n_params))
         return fail(SQ_ERR_INVALID, "batch gradient: parameter index " + std::to_string(o.first) +
                                         " >= n_params " + std::to_string(n_params));
+  }
+  // Circuits that all share one plan structure (many parameter sets of one
+  // circuit) and stream their states get a JIT-specialised kernel.
+  const void *jit_fn = nullptr;
+  if (uniform_plans<Real>(b, packed, nfwd, nrev, occs, M)) {
+    std::string err;
+    jit_fn = sq::jit_batch_adjoint_kernel(packed[0].data(), nfwd[0], nrev[0], b->circs[0].n, M,
+                                          sizeof(Real) == 4, err);
   }
   // Largest work first.
   b->order.resize(nc);
@@ -595,12 +641,15 @@ int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *
     t.plan_off = off;
     off += packed[id].size();
   }
-  const void *fn = batch_adj_fn<Real>(M);
+  const void *fn = jit_fn ? jit_fn : batch_adj_fn<Real>(M);
   const uint32_t L = uint32_t(sq::sweep_low_bits(int(M)));
   const int threads = 1 << (M - sq::kAdjRegBits);
   const size_t nw = size_t(threads + 31) / 32;
   const size_t smem = 4 * (size_t(1) << M) * sizeof(C2) + size_t(sq::kMaxCoef) * sizeof(C2) +
-                      (size_t(1) << (M - L)) * sizeof(uint64_t) + nw * sq::kMaxInner * sizeof(double2);
+                      (jit_fn ? 0 : (size_t(1) << (M - L)) * sizeof(uint64_t)) +
+                      nw * sq::kMaxInner * sizeof(double2);
+  b->last_jit = jit_fn != nullptr;
+  if (jit_fn) sq::jit_note_launch(true);
   SQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   int per_sm = 0, sms = 0;
   SQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
@@ -851,6 +900,34 @@ int sq_batch_run_gradients(sq_batch *b, uint32_t n_params, double *energies, dou
   auto st = static_cast<cudaStream_t>(stream);
   return b->dtype == SQ_C64 ? run_gradient_impl<float>(b, n_params, energies, grads, st)
                             : run_gradient_impl<double>(b, n_params, energies, grads, st);
+}
+
+int sq_jit_batch_adjoint_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
+                                char *buf, uint64_t cap, uint64_t *len) {
+  if ((nops && !ops) || !len) return fail(SQ_ERR_INVALID, "null pointer");
+  if (dtype != SQ_C128 && dtype != SQ_C64) return fail(SQ_ERR_INVALID, "bad dtype");
+  const bool c64 = dtype == SQ_C64;
+  const uint32_t M = c64 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128;
+  if (num_qubits <= M || num_qubits > 30) return fail(SQ_ERR_INVALID, "num_qubits must exceed the tile bits");
+  Circ c;
+  c.n = num_qubits;
+  c.ops.assign(ops, ops + nops);
+  std::vector<unsigned char> packed;
+  uint32_t nf = 0, nr = 0;
+  std::vector<std::pair<int32_t, double>> occ;
+  std::string err;
+  const bool ok = c64 ? plan_gradient_circuit<float>(c, M, packed, nf, nr, occ, err)
+                      : plan_gradient_circuit<double>(c, M, packed, nf, nr, occ, err);
+  if (!ok) return fail(SQ_ERR_UNSUPPORTED, err);
+  const std::string body = sq::jit_batch_adjoint_body(packed.data(), nf, nr, num_qubits, M, c64);
+  const std::string src = body.empty() ? std::string() : sq::jit_batch_source(body);
+  *len = src.size();
+  if (buf && cap) {
+    const size_t n = std::min<size_t>(cap - 1, src.size());
+    std::memcpy(buf, src.data(), n);
+    buf[n] = '\0';
+  }
+  return SQ_OK;
 }
 
 int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream) {

@@ -13,50 +13,11 @@
 #include <stdint.h>
 
 #include "adjoint_kernels.cuh"
+#include "jit_batch.cuh"
 #include "reduce_kernels.cuh"
 #include "sweep_kernels.cuh"
 
 namespace sq {
-
-// Device table entry of one circuit.
-struct BatchCircuit {
-  uint32_t n;          // qubits (>= 4)
-  uint32_t nsweeps;    // forward sweeps
-  uint32_t ham;        // Hamiltonian index
-  uint32_t keep;       // 1: leave the final state in the state pool
-  uint64_t state_off;  // amplitude offset of its state in the pool
-  uint64_t plan_off;   // byte offset of its first packed sweep in the plan pool
-  // Gradient runs only: the reverse (two-state) sweeps follow the forward
-  // ones in the plan pool; lambda's pool offset (n > tile bits); offset of the
-  // circuit's parameter-occurrence inner products in the output array.
-  uint32_t nrev;
-  uint32_t pad;
-  uint64_t lam_off;
-  uint64_t occ_off;
-};
-
-// A packed sweep: this header, then nphases SweepPhase, then nops SweepOp,
-// then ncoef complex coefficients of the state's precision; `bytes` is the
-// 16-byte-aligned size of the whole record.
-struct PackedSweep {
-  SweepHeader h;
-  uint32_t nops;
-  uint32_t bytes;
-  uint32_t phase_off, op_off, coef_off;  // byte offsets from the record start
-  // Reverse sweeps of a gradient run: byte offset of a uint32 array
-  // [nslots, occurrence of slot 0, ...] (0 when the sweep has no inner ops).
-  uint32_t inner_off;
-};
-
-struct BatchParams {
-  const BatchCircuit *circuits;
-  const unsigned char *plans;
-  const PauliParams *hams;
-  uint32_t ncircuits;
-  uint32_t pad;
-  unsigned int *counter;  // work queue head (zeroed before the launch)
-  double *energies;       // one per circuit
-};
 
 // Phases of one packed sweep on one tile held in shared memory.  Threads
 // with tid >= 2^(m-4) only take part in the barriers.
@@ -339,40 +300,6 @@ __device__ __forceinline__ void batch_adjoint_phases(typename Vec2<Real>::T *ft,
     }
     __syncthreads();
   }
-}
-
-// lambda = H psi over a state read through psi_at(i) and written through
-// lam_set(i, v); returns this thread's share of Re <psi|lambda>.  Group g
-// contributes (sum_t f_t (-1)^popc(i & zy_t)) * (odd_g ? -i : 1) * psi[i ^ x_g]
-// (PauliParams stores w_t (-1)^(ny_t / 2) in f and ny_t mod 2 in odd).
-template <typename Real, class PsiAt, class LamSet>
-__device__ __forceinline__ double batch_pauli_apply(const PauliParams &H, uint32_t n, PsiAt psi_at,
-                                                    LamSet lam_set) {
-  using C2 = typename Vec2<Real>::T;
-  double e = 0.0;
-  for (uint64_t i = threadIdx.x; i < (uint64_t(1) << n); i += blockDim.x) {
-    double ar = 0.0, ai = 0.0;
-    for (uint32_t gi = 0; gi < H.ngroups; ++gi) {
-      const PauliGroup &G = H.g[gi];
-      double c = 0.0;
-      for (uint32_t t = G.t0; t < G.t1; ++t) c += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
-      const C2 b = psi_at(i ^ G.x);
-      if (G.odd) {  // c * (-i) * b
-        ar += c * double(b.y);
-        ai -= c * double(b.x);
-      } else {
-        ar += c * double(b.x);
-        ai += c * double(b.y);
-      }
-    }
-    C2 o;
-    o.x = Real(ar);
-    o.y = Real(ai);
-    lam_set(i, o);
-    const C2 a = psi_at(i);
-    e += double(a.x) * ar + double(a.y) * ai;
-  }
-  return e;
 }
 
 // Dynamic shared memory: two (phi tile | lambda tile) buffers (2^M amplitudes

@@ -34,6 +34,7 @@
 #include "adjoint_plan.h"
 #include "host_ops.h"
 #include "jit.h"
+#include "jit_batch.cuh"
 #include "sweep_kernels.cuh"
 
 int sq_detail_fail(int code, const char *msg);  // engine.cu: sets sq_last_error()
@@ -42,7 +43,7 @@ namespace sq {
 
 namespace {
 
-#include "jit_sources.inc"  // kJitPlanSource, kJitSweepSource (generated by build.py)
+#include "jit_sources.inc"  // kJit{Plan,Sweep,Reduce,Batch}Source (generated by build.py)
 
 // --- NVRTC through dlopen -------------------------------------------------
 typedef int nvrtcResult_t;
@@ -154,20 +155,42 @@ bool compile(const std::string &src, std::vector<char> &cubin, std::string &err)
   return true;
 }
 
-// Header sources every generated kernel is compiled with.
-const std::string &prelude() {
-  static const std::string p =
-      std::string("typedef unsigned char uint8_t;\ntypedef unsigned short uint16_t;\n"
-                  "typedef unsigned int uint32_t;\ntypedef unsigned long long uint64_t;\n"
-                  "typedef int int32_t;\ntypedef long long int64_t;\n") +
-      kJitPlanSource + "\n" + kJitSweepSource + "\nusing namespace sq;\n";
+// Header sources generated kernels are compiled with, and their hash.
+struct Prelude {
+  std::string text;
+  uint64_t hash;
+};
+
+Prelude make_prelude(bool batch) {
+  Prelude p;
+  p.text = std::string("typedef unsigned char uint8_t;\ntypedef unsigned short uint16_t;\n"
+                       "typedef unsigned int uint32_t;\ntypedef unsigned long long uint64_t;\n"
+                       "typedef int int32_t;\ntypedef long long int64_t;\n") +
+           kJitPlanSource + "\n" + kJitSweepSource + "\n";
+  if (batch) p.text += std::string(kJitReduceSource) + "\n" + kJitBatchSource + "\n";
+  p.text += "using namespace sq;\n";
+  p.hash = fnv1a(p.text);
   return p;
 }
 
+// Sweep kernels (single- and two-state).
+const Prelude &sweep_prelude() {
+  static const Prelude p = make_prelude(false);
+  return p;
+}
+
+// Batched-gradient kernels (also need the Pauli and batch types).
+const Prelude &batch_prelude() {
+  static const Prelude p = make_prelude(true);
+  return p;
+}
+
+const std::string &prelude() { return sweep_prelude().text; }
+
 // Loads (compiling when not cached) the kernel whose generated part is `body`.
-Entry &get_entry(const std::string &body, const char *name = "sq_jit_sweep") {
-  static const uint64_t prelude_hash = fnv1a(prelude());
-  const uint64_t key = fnv1a(body) ^ (prelude_hash * 0x9e3779b97f4a7c15ull);
+Entry &get_entry(const std::string &body, const char *name = "sq_jit_sweep",
+                 const Prelude &pre = sweep_prelude()) {
+  const uint64_t key = fnv1a(body) ^ (pre.hash * 0x9e3779b97f4a7c15ull);
   {
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_cache.find(key);
@@ -184,7 +207,7 @@ Entry &get_entry(const std::string &body, const char *name = "sq_jit_sweep") {
     if (in) cubin.assign(std::istreambuf_iterator<char>(in), std::istreambuf_iterator<char>());
   }
   if (cubin.empty()) {
-    if (compile(prelude() + body, cubin, e.err)) {
+    if (compile(pre.text + body, cubin, e.err)) {
       mkdirs(dir);
       const std::string tmp = file + "." + std::to_string(getpid()) + "." +
                               std::to_string(std::hash<std::thread::id>()(std::this_thread::get_id())) +
@@ -481,6 +504,197 @@ std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb) {
   s << "  });\n}\n";
   return s.str();
 }
+
+// ---------------------------------------------------------------------------
+// Batched gradients of circuits that share one plan structure: one kernel
+// whose every sweep is straight-line code (coefficients per circuit from its
+// packed plan, through shared memory).
+// ---------------------------------------------------------------------------
+namespace {
+
+std::string cond_prefix(const SweepOp &op) {
+  if (!op.gmask && !op.lmask) return std::string();
+  std::ostringstream s;
+  s << "if (";
+  if (op.gmask) s << "(gbase & 0x" << std::hex << op.gmask << "ull) == 0x" << op.gval << "ull" << std::dec;
+  if (op.gmask && op.lmask) s << " && ";
+  if (op.lmask) s << "(jb & 0x" << std::hex << op.lmask << "u) == 0x" << op.lval << "u" << std::dec;
+  s << ") ";
+  return s.str();
+}
+
+std::string diag_bits_src(const SweepOp &op) {
+  std::ostringstream b;
+  b << "uint32_t b = 0;";
+  for (int t = 0; t < op.ndt; ++t) {
+    if (op.dsrc[t] == kSrcGlobal)
+      b << " b = (b << 1) | (uint32_t(gbase >> " << int(op.dpos[t]) << ") & 1u);";
+    else
+      b << " b = (b << 1) | ((jb >> " << int(op.dpos[t]) << ") & 1u);";
+  }
+  return b.str();
+}
+
+std::string tile_type(const SweepHeader &h) {
+  std::ostringstream s;
+  s << "JitTile<" << h.m << ", " << h.l;
+  for (uint32_t i = 0; i < h.m - h.l; ++i) s << ", " << int(h.hi[i]);
+  s << ">";
+  return s.str();
+}
+
+}  // namespace
+
+std::string jit_batch_adjoint_body(const unsigned char *plan, uint32_t nfwd, uint32_t nrev, uint32_t n,
+                                   uint32_t M, bool c64) {
+  const char *R = c64 ? "float" : "double";
+  const int NT = 1 << (int(M) - kAdjRegBits), NT4 = 1 << (int(M) - kRegBits), NW = (NT + 31) / 32;
+  // One __noinline__ device function per sweep (the compiler then works on
+  // one sweep at a time), called in order by the kernel.
+  std::ostringstream fns, calls;
+  auto smem_ptrs = [&](std::ostringstream &o) {
+    o << "  extern __shared__ __align__(16) unsigned char smem_raw[];\n"
+      << "  C2 *bufs = reinterpret_cast<C2 *>(smem_raw);\n"
+      << "  C2 *coef = bufs + 4 * (1u << " << M << ");\n"
+      << "  double2 *acc = reinterpret_cast<double2 *>(coef + kMaxCoef);\n";
+  };
+  fns << "using C2 = Vec2<" << R << ">::T;\n";
+  size_t off = 0;
+  for (uint32_t k = 0; k < nfwd + nrev; ++k) {
+    const PackedSweep &ps = *reinterpret_cast<const PackedSweep *>(plan + off);
+    const SweepPhase *ph = reinterpret_cast<const SweepPhase *>(plan + off + ps.phase_off);
+    const SweepOp *ops = reinterpret_cast<const SweepOp *>(plan + off + ps.op_off);
+    const uint32_t *inner = ps.inner_off ? reinterpret_cast<const uint32_t *>(plan + off + ps.inner_off) : nullptr;
+    if (ps.h.m != M) return std::string();
+    const bool rev = k >= nfwd;
+    if (k == nfwd)
+      calls << "    sqb_energy(B, C, c, psi, lam);\n";
+    fns << "__device__ __noinline__ void sqb_sweep" << k << "(C2 *__restrict__ psi, C2 *__restrict__ lam, "
+        << "const unsigned char *rec, double2 *occc) {\n";
+    smem_ptrs(fns);
+    fns << "  using Tile = " << tile_type(ps.h) << ";\n"
+        << "  jit_batch_coef<" << R << ">(coef, rec, " << (off + ps.coef_off) << "u, " << ps.h.ncoef << "u);\n";
+    if (rev) fns << "  jit_batch_acc_zero(acc, " << NW << ");\n";
+    fns << "  __syncthreads();\n";
+    if (!rev)
+      fns << "  jit_batch_fwd<" << R << ", " << M << ", Tile>(psi, bufs, " << ps.h.num_tiles
+          << "ull, [&](C2 *tile, uint64_t gbase) {\n";
+    else
+      fns << "  jit_batch_rev<" << R << ", " << M << ", Tile>(psi, lam, bufs, " << ps.h.num_tiles
+          << "ull, [&](C2 *ft, C2 *lt, uint64_t gbase) {\n";
+    for (uint32_t p = 0; p < ps.h.nphases; ++p) {
+      const SweepPhase &P = ph[p];
+      if (!rev) {
+        fns << "    { using Ph = JitPhase<" << R << ", " << M << ", Tile, " << int(P.reg[0]) << ", "
+            << int(P.reg[1]) << ", " << int(P.reg[2]) << ", " << int(P.reg[3]);
+        for (int t : thread_positions(P, int(M), c64, false)) fns << ", " << t;
+        fns << ">;\n      if (threadIdx.x < " << NT4 << ") {\n"
+            << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R
+            << "> A;\n      Ph::gather(A, tile, jb);\n";
+        for (uint32_t oi = P.op_begin; oi < P.op_end; ++oi) {
+          const SweepOp &op = ops[oi];
+          if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) return std::string();
+          std::string tmpl;
+          op_routine(op, c64, tmpl, 16);
+          fns << "      " << cond_prefix(op);
+          if (op.kind == kSwDiag)
+            fns << "{ " << diag_bits_src(op) << " " << tmpl << "(A, coef + " << op.coef << ", b); }\n";
+          else
+            fns << tmpl << "(A, coef + " << op.coef << ", " << int(op.rmask) << ", " << int(op.rval) << ");\n";
+        }
+        fns << "      Ph::scatter(A, tile, jb);\n      }\n      __syncthreads(); }\n";
+      } else {
+        fns << "    { using Ph = JitPhase2<" << R << ", " << M << ", Tile, " << int(P.reg[0]) << ", "
+            << int(P.reg[1]) << ", " << int(P.reg[2]);
+        for (int t : thread_positions(P, int(M), c64, false, kAdjRegBits)) fns << ", " << t;
+        fns << ">;\n      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << ", " << kAdjAmps
+            << "> F, G;\n      Ph::gather(F, G, ft, lt, jb);\n";
+        for (uint32_t oi = P.op_begin; oi < P.op_end; ++oi) {
+          const SweepOp &op = ops[oi];
+          if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
+            if (op.gmask || op.lmask || op.rmask || op.slot >= uint32_t(kMaxInner)) return std::string();
+            fns << "      { double sr = 0.0, si = 0.0; ";
+            if (op.kind == kSwInnerDiag)
+              fns << diag_bits_src(op) << " inner_diag<" << R << ", " << int(op.vmask) << ">(F, G, coef + "
+                  << op.coef << ", b, sr, si); ";
+            else
+              fns << "inner_dense<" << R << ", " << int(op.vmask) << ">(F, G, coef + " << op.coef << ", sr, si); ";
+            fns << "jit_inner_acc<" << NT << ", " << op.slot << ">(acc, sr, si); }\n";
+            continue;
+          }
+          std::string tmpl;
+          op_routine(op, c64, tmpl, kAdjAmps);
+          fns << "      " << cond_prefix(op);
+          if (op.kind == kSwDiag)
+            fns << "{ " << diag_bits_src(op) << " " << tmpl << "(F, coef + " << op.coef << ", b); " << tmpl
+                << "(G, coef + " << op.coef << ", b); }\n";
+          else
+            fns << "{ " << tmpl << "(F, coef + " << op.coef << ", " << int(op.rmask) << ", " << int(op.rval)
+                << "); " << tmpl << "(G, coef + " << op.coef << ", " << int(op.rmask) << ", " << int(op.rval)
+                << "); }\n";
+        }
+        fns << "      Ph::scatter(F, G, ft, lt, jb);\n      __syncthreads(); }\n";
+      }
+    }
+    fns << "  });\n";
+    if (rev && inner) {
+      fns << "  if (threadIdx.x == 0) {\n";
+      for (uint32_t q = 0; q < inner[0]; ++q)
+        fns << "    jit_batch_slot_add(acc, " << NW << ", " << q << ", occc + " << inner[1 + q] << "u);\n";
+      fns << "  }\n  __syncthreads();\n";
+    }
+    fns << "}\n";
+    calls << "    sqb_sweep" << k << "(psi, lam, rec, occ + C.occ_off);\n";
+    off += ps.bytes;
+  }
+  if (nrev == 0) calls << "    sqb_energy(B, C, c, psi, lam);\n";
+  std::ostringstream s;
+  s << fns.str();
+  s << "__device__ __noinline__ void sqb_energy(const BatchParams &B, const BatchCircuit &C, uint32_t c, "
+       "C2 *psi, C2 *lam) {\n"
+    << "  double e = batch_pauli_apply<" << R << ">(B.hams[C.ham], " << n
+    << ", [&](uint64_t i) { return psi[i]; }, [&](uint64_t i, const C2 &v) { lam[i] = v; });\n"
+    << "  e = block_sum(e);\n  if (threadIdx.x == 0) B.energies[c] = e;\n  __syncthreads();\n}\n";
+  // sqb_energy is defined after its callers' definitions but before the kernel.
+  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", 1)\nsq_jit_batch_adjoint(C2 *__restrict__ pool, "
+    << "const __grid_constant__ BatchParams B, double2 *__restrict__ occ) {\n"
+    << "  __shared__ uint32_t s_next;\n"
+    << "  for (;;) {\n"
+    << "    if (threadIdx.x == 0) s_next = atomicAdd(B.counter, 1u);\n"
+    << "    __syncthreads();\n"
+    << "    const uint32_t c = s_next;\n"
+    << "    __syncthreads();\n"
+    << "    if (c >= B.ncircuits) break;\n"
+    << "    const BatchCircuit C = B.circuits[c];\n"
+    << "    C2 *psi = pool + C.state_off;\n"
+    << "    C2 *lam = pool + C.lam_off;\n"
+    << "    const unsigned char *rec = B.plans + C.plan_off;\n"
+    << "    jit_batch_init<" << R << ">(psi, " << n << ");\n"
+    << "    __syncthreads();\n"
+    << calls.str() << "  }\n}\n";
+  return s.str();
+}
+
+const void *jit_batch_adjoint_kernel(const unsigned char *plan, uint32_t nfwd, uint32_t nrev, uint32_t n,
+                                     uint32_t M, bool c64, std::string &err) {
+  if (!jit_available()) {
+    err = "NVRTC not available";
+    return nullptr;
+  }
+  const std::string body = jit_batch_adjoint_body(plan, nfwd, nrev, n, M, c64);
+  if (body.empty()) {
+    err = "plan not covered by the JIT batch form";
+    return nullptr;
+  }
+  Entry &e = get_entry(body, "sq_jit_batch_adjoint", batch_prelude());
+  if (e.failed) {
+    err = e.err;
+    return nullptr;
+  }
+  return reinterpret_cast<const void *>(e.kernel);
+}
+
+std::string jit_batch_source(const std::string &body) { return batch_prelude().text + body; }
 
 size_t jit_adjoint_smem(const PlannedSweep &ps, bool c64) {
   return jit_adjoint_smem_bytes(int(ps.h.m), c64 ? 8 : 16, ps.h.ncoef);

@@ -28,6 +28,15 @@ const void *jit_adjoint_kernel(const PlannedSweep &ps, bool c64, std::string &er
 size_t jit_adjoint_smem(const PlannedSweep &ps, bool c64);
 std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb);
 void jit_prepare_adjoint(const std::vector<const PlannedSweep *> &sweeps, bool c64);
+// Batched gradients of circuits that share one packed plan structure
+// (`plan`: one circuit's packed records, nfwd forward then nrev reverse
+// sweeps, every sweep of m == M): the kernel (or nullptr with `err`), its
+// generated body, and the full source of a body.
+const void *jit_batch_adjoint_kernel(const unsigned char *plan, uint32_t nfwd, uint32_t nrev, uint32_t n,
+                                     uint32_t M, bool c64, std::string &err);
+std::string jit_batch_adjoint_body(const unsigned char *plan, uint32_t nfwd, uint32_t nrev, uint32_t n,
+                                   uint32_t M, bool c64);
+std::string jit_batch_source(const std::string &body);
 // Compiles the kernels of several sweeps in parallel (fills the cache).
 void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64);
 

@@ -15,10 +15,12 @@
 // the weight and the (-i)^ny phase into one real factor per term, so a group
 // costs one read of the state and the kernel needs one FP64 accumulator.
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "sweep_kernels.cuh"
+#endif
 
 namespace sq {
 

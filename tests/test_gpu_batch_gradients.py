@@ -109,3 +109,27 @@ def test_batch_gradient_tile_sizes_agree(dtype, tiles, tol):
     assert np.abs(res[0][0] - res[1][0]).max() <= tol
     assert np.abs(res[0][1] - res[1][1]).max() <= tol * max(1.0, np.abs(res[0][1]).max())
     b.close()
+
+
+@pytest.mark.parametrize("dtype,n,tol", [(capi.SQ_C128, 14, 1e-10), (capi.SQ_C64, 14, 1e-4)])
+def test_uniform_batch_jit_kernel_matches_generic(dtype, n, tol, monkeypatch):
+    """Many parameter sets of one circuit (every plan has one structure): the
+    JIT-specialised batched-gradient kernel against the generic one."""
+    ops, terms, npar = qaoa(n, 2, seed=4)
+    thetas = np.random.default_rng(9).uniform(-3, 3, (24, npar))
+    res = {}
+    for jit in ("1", "0"):
+        monkeypatch.setenv("SQ_JIT", jit)
+        b = capi.Batch(dtype)
+        hid = b.add_hamiltonian(n, terms)
+        for th in thetas:
+            b.add_circuit(n, adjoint.bind(ops, th), hid)
+        before = capi.jit_info()[1]
+        res[jit] = b.run_gradients(npar)
+        if jit == "1":
+            assert capi.jit_info()[1] > before, "the JIT batched-gradient kernel did not run"
+        b.close()
+    assert np.abs(res["1"][0] - res["0"][0]).max() <= tol
+    assert np.abs(res["1"][1] - res["0"][1]).max() <= tol * max(1.0, np.abs(res["0"][1]).max())
+    e_ref, g_ref = reference(n, ops, thetas[5], terms, npar)
+    assert abs(res["1"][0][5] - e_ref) <= tol * max(1.0, abs(e_ref))

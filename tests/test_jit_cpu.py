@@ -127,3 +127,17 @@ def test_adjoint_sources_compile(dtype):
                 capi.jit_compile(src)
                 compiled += 1
     assert compiled > 0
+
+
+@pytest.mark.parametrize("dtype,n", [(capi.SQ_C128, 14), (capi.SQ_C64, 13)])
+def test_batch_adjoint_source_compiles(dtype, n):
+    from snuqs_b200 import adjoint
+
+    edges = circuits.random_regular_graph(n, 3, seed=3) if n % 2 == 0 else [(i, (i + 1) % n) for i in range(n)]
+    ops = [("Hadamard", (q,), ()) for q in range(n)]
+    for l in range(2):
+        ops += [("ZZ", (i, j), (0.0,), (l,)) for i, j in edges]
+        ops += [("RotX", (q,), (0.0,), (2 + l,)) for q in range(n)]
+    src = capi.jit_batch_adjoint_source(n, adjoint.bind(ops, [0.3, 0.5, 0.7, 0.9]), dtype)
+    assert "sq_jit_batch_adjoint" in src
+    capi.jit_compile(src)
