@@ -129,7 +129,7 @@ def test_adjoint_sources_compile(dtype):
     assert compiled > 0
 
 
-@pytest.mark.parametrize("dtype,n", [(capi.SQ_C128, 14), (capi.SQ_C64, 13)])
+@pytest.mark.parametrize("dtype,n", [(capi.SQ_C128, 14)])
 def test_batch_adjoint_source_compiles(dtype, n):
     from snuqs_b200 import adjoint
 
