@@ -96,8 +96,11 @@ struct sq_batch {
   std::vector<sq::PauliParams> hams;
   std::vector<uint32_t> ham_n;
   std::vector<Circ> circs;
-  DevBuf d_pool, d_plans, d_table, d_hams, d_energy, d_counter, d_occ;
-  HostBuf h_plans, h_table, h_energy, h_occ;
+  DevBuf d_pool, d_plans, d_table, d_hams, d_energy, d_counter, d_occ, d_def, d_part;
+  HostBuf h_plans, h_table, h_energy, h_occ, h_def;
+  std::vector<uint32_t> deferred;  // table positions whose energy the grid-wide pass computes
+  uint32_t nitems = 0;              // work items of that pass
+  size_t def_words = 0;             // staged words: deferred, item offsets, item circuits, chunks
   size_t hams_uploaded = 0;
   std::vector<uint64_t> state_off;  // per circuit id; ~0 when not kept
   std::vector<uint32_t> order;      // sorted position -> circuit id
@@ -323,6 +326,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
                       b->planned_l != b->low_bits || b->planned_ops != b->max_ops;
   size_t plan_bytes = b->planned_bytes;
   if (replan) {
+  b->deferred.clear();
   // Plan all circuits in parallel.
   std::vector<std::vector<unsigned char>> packed(nc);
   std::vector<int> nsweeps(nc, 0);
@@ -388,7 +392,35 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     t.keep = b->keep ? 1u : 0u;
     t.state_off = b->state_off[id] == ~uint64_t(0) ? 0 : b->state_off[id];
     t.plan_off = off;
+    t.nrev = 0;
+    t.lam_off = t.occ_off = 0;
+    // A streamed state (n > M) leaves its energy to the grid-wide pass.
+    t.defer = c.n > M ? 1u : 0u;
+    if (t.defer) b->deferred.push_back(uint32_t(pos));
     off += packed[id].size();
+  }
+  // Work items of the energy pass: chunks of 2^kEnergyChunkBits pairs.
+  // Staged as [deferred | item_off (ndef+1) | item_k | item_j].
+  {
+    std::vector<uint32_t> item_off{0}, item_k, item_j;
+    for (uint32_t k = 0; k < b->deferred.size(); ++k) {
+      const uint32_t n = tab[b->deferred[k]].n;
+      const uint32_t chunks = n - 1 > sq::kEnergyChunkBits ? 1u << (n - 1 - sq::kEnergyChunkBits) : 1u;
+      for (uint32_t j = 0; j < chunks; ++j) {
+        item_k.push_back(k);
+        item_j.push_back(j);
+      }
+      item_off.push_back(uint32_t(item_k.size()));
+    }
+    b->nitems = uint32_t(item_k.size());
+    std::vector<uint32_t> staged(b->deferred);
+    staged.insert(staged.end(), item_off.begin(), item_off.end());
+    staged.insert(staged.end(), item_k.begin(), item_k.end());
+    staged.insert(staged.end(), item_j.begin(), item_j.end());
+    b->def_words = staged.size();
+    if (int s = b->d_def.ensure(staged.size() * sizeof(uint32_t))) return s;
+    if (int s = b->h_def.ensure(staged.size() * sizeof(uint32_t))) return s;
+    std::memcpy(b->h_def.p, staged.data(), staged.size() * sizeof(uint32_t));
   }
     // Staging buffers may have moved: the graph is captured again.
     if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -408,6 +440,10 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     SQB_CUDA(cudaEventCreate(&b->ev0));
     SQB_CUDA(cudaEventCreate(&b->ev1));
   }
+  // Grid-wide energy pass over the streamed states: 4 blocks per SM.
+  uint32_t ndef = uint32_t(b->deferred.size());
+  const uint32_t egrid = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(b->nitems, uint64_t(sms) * 8)));
+  if (int s = b->d_part.ensure(std::max<size_t>(b->nitems, 1) * sizeof(double))) return s;
   // (Re)capture the graph when sizes or the stream changed.
   if (!b->graph || b->graph_plan_bytes != plan_bytes || b->graph_ncirc != nc ||
       b->graph_stream != st || b->graph_grid != grid || b->graph_fn != fn) {
@@ -435,6 +471,18 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
       // External event nodes, so the kernel's device time can be read back.
       cudaEventRecordWithFlags(b->ev0, cs, cudaEventRecordExternal);
       cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, cs);
+      if (ndef) {
+        cudaMemcpyAsync(b->d_def.p, b->h_def.p, b->def_words * sizeof(uint32_t), cudaMemcpyHostToDevice, cs);
+        const uint32_t *defp = static_cast<const uint32_t *>(b->d_def.p);
+        const uint32_t *offp = defp + ndef, *kp = offp + ndef + 1, *jp = kp + b->nitems;
+        double *partp = static_cast<double *>(b->d_part.p);
+        const C2 *cpool = poolp;
+        uint32_t nitems = b->nitems;
+        void *gargs[] = {&cpool, &P, &defp, &kp, &jp, &nitems, &partp};
+        cudaLaunchKernel(reinterpret_cast<const void *>(&sq::batch_energy_grid<Real>), dim3(egrid),
+                         dim3(sq::kReduceThreads), gargs, 0, cs);
+        sq::batch_energy_finalize<<<ndef, sq::kReduceThreads, 0, cs>>>(partp, offp, defp, P.energies);
+      }
       cudaEventRecordWithFlags(b->ev1, cs, cudaEventRecordExternal);
       cudaMemcpyAsync(b->h_energy.p, b->d_energy.p, nc * sizeof(double), cudaMemcpyDeviceToHost, cs);
       SQB_CUDA(cudaStreamEndCapture(cs, &g));
@@ -731,6 +779,9 @@ int sq_batch_destroy(sq_batch *b) {
   b->d_counter.release();
   b->d_occ.release();
   b->h_occ.release();
+  b->d_def.release();
+  b->d_part.release();
+  b->h_def.release();
   b->h_plans.release();
   b->h_table.release();
   b->h_energy.release();

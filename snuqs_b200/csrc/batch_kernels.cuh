@@ -212,16 +212,112 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 1)
       rec += ps.bytes;
     }
     const PauliParams &H = B.hams[C.ham];
-    double e;
-    if (resident)
-      e = batch_energy<Real>(H, n, [&](uint64_t i) { return tile[swz<Real>(uint32_t(i))]; });
-    else
-      e = batch_energy<Real>(H, n, [&](uint64_t i) { return psi[i]; });
-    if (tid == 0) B.energies[c] = e;
+    if (!C.defer) {
+      double e;
+      if (resident)
+        e = batch_energy<Real>(H, n, [&](uint64_t i) { return tile[swz<Real>(uint32_t(i))]; });
+      else
+        e = batch_energy<Real>(H, n, [&](uint64_t i) { return psi[i]; });
+      if (tid == 0) B.energies[c] = e;
+    }
     if (resident && C.keep)
       for (uint32_t j = tid; j < uint32_t(N); j += NT) psi[j] = tile[swz<Real>(j)];
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Energies of the streamed (pool-resident) circuits of a batch, after
+// batch_kernel.  Work item w covers deferred circuit item_k[w] and chunk
+// item_j[w] of its index range (kEnergyChunk pairs of every Pauli group, or
+// 2 kEnergyChunk amplitudes of a diagonal group), so a large state is shared
+// by many blocks at once and stays in L2 across its groups, while a small
+// one is one block's work.  partials[w] receives the block's sum;
+// batch_energy_finalize adds a circuit's items in order.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kEnergyChunkBits = 14;
+
+template <typename Real>
+__global__ void __launch_bounds__(kReduceThreads)
+    batch_energy_grid(const typename Vec2<Real>::T *__restrict__ pool, const __grid_constant__ BatchParams B,
+                      const uint32_t *__restrict__ deferred, const uint32_t *__restrict__ item_k,
+                      const uint32_t *__restrict__ item_j, uint32_t nitems, double *__restrict__ partials) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int U = 4;
+  for (uint32_t w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const BatchCircuit &C = B.circuits[deferred[item_k[w]]];
+    const PauliParams &H = B.hams[C.ham];
+    const C2 *psi = pool + C.state_off;
+    const uint32_t n = C.n;
+    const uint64_t j = item_j[w];
+    double acc = 0.0;
+    for (uint32_t gi = 0; gi < H.ngroups; ++gi) {
+      const PauliGroup &G = H.g[gi];
+      if (G.x == 0) {
+        const uint64_t N = uint64_t(1) << n;
+        const uint64_t lo = j << (kEnergyChunkBits + 1), hi = lo + (uint64_t(2) << kEnergyChunkBits);
+        const uint64_t end = hi < N ? hi : N;
+        for (uint64_t i0 = lo + threadIdx.x; i0 < end; i0 += uint64_t(blockDim.x) * U) {
+          C2 a[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const uint64_t i = i0 + uint64_t(u) * blockDim.x;
+            a[u] = psi[i < end ? i : lo];
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const uint64_t i = i0 + uint64_t(u) * blockDim.x;
+            if (i >= end) continue;
+            const double q = double(a[u].x) * double(a[u].x) + double(a[u].y) * double(a[u].y);
+            double wt = 0.0;
+            for (uint32_t t = G.t0; t < G.t1; ++t) wt += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
+            acc = fma(q, wt, acc);
+          }
+        }
+      } else {
+        const uint32_t hb = 63 - __clzll(G.x);
+        const uint64_t NP = uint64_t(1) << (n - 1);
+        const uint64_t lo = j << kEnergyChunkBits, hi = lo + (uint64_t(1) << kEnergyChunkBits);
+        const uint64_t end = hi < NP ? hi : NP;
+        for (uint64_t h0 = lo + threadIdx.x; h0 < end; h0 += uint64_t(blockDim.x) * U) {
+          C2 a[U], b[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const uint64_t hh = h0 + uint64_t(u) * blockDim.x;
+            const uint64_t i = insert_zero(hh < end ? hh : lo, hb);
+            a[u] = psi[i];
+            b[u] = psi[i ^ G.x];
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const uint64_t hh = h0 + uint64_t(u) * blockDim.x;
+            if (hh >= end) continue;
+            const uint64_t i = insert_zero(hh, hb);
+            const double zr = double(a[u].x) * double(b[u].x) + double(a[u].y) * double(b[u].y);
+            const double zi = double(a[u].x) * double(b[u].y) - double(a[u].y) * double(b[u].x);
+            const double q = 2.0 * (G.odd ? zi : zr);
+            double wt = 0.0;
+            for (uint32_t t = G.t0; t < G.t1; ++t) wt += (__popcll(i & H.zy[t]) & 1) ? -H.f[t] : H.f[t];
+            acc = fma(q, wt, acc);
+          }
+        }
+      }
+    }
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) partials[w] = s;
+  }
+}
+
+// energies[deferred[k]] = sum of partials[item_off[k] .. item_off[k+1]), in
+// order.  One block per deferred circuit.
+static __global__ void __launch_bounds__(kReduceThreads)
+    batch_energy_finalize(const double *__restrict__ partials, const uint32_t *__restrict__ item_off,
+                          const uint32_t *__restrict__ deferred, double *__restrict__ energies) {
+  const uint32_t k = blockIdx.x;
+  double v = 0.0;
+  for (uint32_t i = item_off[k] + threadIdx.x; i < item_off[k + 1]; i += blockDim.x) v += partials[i];
+  v = block_sum(v);
+  if (threadIdx.x == 0) energies[deferred[k]] = v;
 }
 
 // ---------------------------------------------------------------------------

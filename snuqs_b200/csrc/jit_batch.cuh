@@ -25,7 +25,7 @@ struct BatchCircuit {
   // ones in the plan pool; lambda's pool offset (n > tile bits); offset of the
   // circuit's parameter-occurrence inner products in the output array.
   uint32_t nrev;
-  uint32_t pad;
+  uint32_t defer;  // energy runs: 1 = the energy is left to batch_energy_grid (state in the pool)
   uint64_t lam_off;
   uint64_t occ_off;
 };
