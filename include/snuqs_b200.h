@@ -63,7 +63,8 @@ typedef enum {
 
 typedef enum {
   SQ_OPT_FUSION = 0,    /* 1 (default): fused tile sweeps; 0: one unfused kernel per gate */
-  SQ_OPT_TILE_BITS = 1, /* log2 amplitudes per shared-memory tile (4..12; default 12) */
+  SQ_OPT_TILE_BITS = 1, /* log2 amplitudes per shared-memory tile (4..12; default 11 for
+                           complex128, 12 for complex64: 32 KiB either way) */
   SQ_OPT_REORDER = 2,   /* 1 (default): the planner may absorb later gates that commute */
   SQ_OPT_TIMING = 3,    /* 1: record a CUDA event pair around every fused-sweep launch */
   SQ_OPT_JIT = 4,       /* -1 (default): JIT-specialised sweep kernels for states of >= 20
@@ -117,6 +118,7 @@ int sq_gate_matrix_derivative(int gate, const double *angles, uint32_t nangles,
 
 /* ---- state handle -------------------------------------------------------
  * StateVector(DeviceType::CUDA, n): state_vector.cc:21-25 + buffer_cuda.cc:13-17. */
+/* SQ_ERR_OOM when the device cannot hold the state; the library stays usable. */
 int sq_state_create(uint32_t num_qubits, int dtype, sq_state **out);
 /* Wraps caller-owned device memory of 2^n amplitudes (not freed by destroy). */
 int sq_state_wrap(void *device_ptr, uint32_t num_qubits, int dtype,
@@ -178,6 +180,11 @@ int sq_apply_gate_buffer(void *buffer, const void *gate_device,
 int sq_copy_to_host(sq_state *s, void *dst, void *stream);
 int sq_copy_from_host(sq_state *s, const void *src, void *stream);
 int sq_copy_state(sq_state *dst, sq_state *src, void *stream);
+/* Synchronises `stream` and reports a sweep kernel that gave up one of its
+ * bounded waits on this state since the last check (SQ_ERR_TIMEOUT; the
+ * state's contents are then invalid).  No counterpart in the reference,
+ * whose CUDA errors exit the process (utils_cuda.h:8-16). */
+int sq_state_check(sq_state *s, void *stream);
 
 /* ---- results ----------------------------------------------------------- */
 /* |psi_i|^2 into a caller-provided DEVICE array of 2^n doubles
@@ -190,6 +197,41 @@ int sq_expect_pauli(sq_state *s, const char *paulis, const double *weights,
                     uint32_t n_terms, double *out, void *stream);
 /* Squared norm in FP64 (synchronous). */
 int sq_norm2(sq_state *s, double *out, void *stream);
+/* Variance <H^2> - <H>^2 of H = sum_t w_t P_t (paulis as in sq_expect_pauli;
+ * n_terms <= 1024), FP64, synchronous.  H^2 is expanded into Pauli strings on
+ * the host (anticommuting pairs cancel) and both moments run on the device.
+ * Replaces the Variance result type the reference plugin does not register
+ * (src/braket/snuqs/result_types.py:149-151, simulator.py:578-580). */
+int sq_variance_pauli(sq_state *s, const char *paulis, const double *weights,
+                      uint32_t n_terms, double *out, void *stream);
+/* Measurement shots on the device, replacing the host-side
+ * np.random.choice over |psi|^2 after a full state copy
+ * (src/braket/snuqs/simulation.py:208-220).  uniforms_device: `shots`
+ * doubles in [0, 1) (DEVICE memory); out_device: `shots` basis-state indices
+ * (DEVICE memory, uint64; bit n-1-q of an index is qubit q).  Index of shot
+ * s = the inverse CDF of |psi_i|^2 at uniforms[s] * sum|psi|^2, with the
+ * probabilities summed in one fixed binary tree (adjacent pairs first), so
+ * the result is reproducible bit for bit.  Asynchronous on `stream`;
+ * shots <= 2^31 per call; num_qubits <= 34. */
+int sq_sample(sq_state *s, const double *uniforms_device, uint64_t shots,
+              uint64_t *out_device, void *stream);
+/* Amplitudes psi[indices[i]] as complex128 (interleaved doubles) into
+ * out_device; indices_device and out_device are DEVICE arrays of `count`
+ * entries.  Synchronous; SQ_ERR_INVALID if an index is >= 2^n.  The Braket
+ * Amplitude result type (not registered by the reference plugin). */
+int sq_amplitudes(sq_state *s, const uint64_t *indices_device, uint64_t count,
+                  double *out_device, void *stream);
+/* Marginal probabilities of the k target qubits into a DEVICE array of 2^k
+ * doubles; qubits[0] is the most significant bit of the output index (the
+ * Braket Probability result type with targets).  k <= 30. */
+int sq_marginal_probabilities(sq_state *s, const uint32_t *qubits, uint32_t k,
+                              double *out_device, void *stream);
+/* Precision report of one state against another of the same size (either
+ * precision, e.g. a complex64 result against the complex128 one): max_i
+ * |a_i - b_i| and 1 - |<a|b>|^2 / (<a|a><b|b>), accumulated in FP64.
+ * Synchronous.  No counterpart in the reference (complex128 only). */
+int sq_state_distance(sq_state *a, sq_state *b, double *max_abs,
+                      double *one_minus_fidelity, void *stream);
 
 /* ---- adjoint gradient ---------------------------------------------------
  * No counterpart in the reference (its plugin forbids the adjoint-gradient
@@ -246,10 +288,13 @@ int sq_adjoint_gradient(sq_state *psi, sq_state *lam, const sq_circuit_op *ops,
  * 16 KiB device array (2048 doubles) inside the library, which each device
  * holds from the moment the library's device code is loaded on it until the
  * process exits.  The first call on each device looks that array up (make
- * it once, before any stream capture).  Every call on a device shares the
- * array, so calls that overlap on the GPU (different streams, no ordering)
- * race; order them.  Limits: n_terms <= 1024 and at most 256 distinct
- * (X/Y mask, Y parity) groups; larger requests return SQ_ERR_UNSUPPORTED. */
+ * it once, before any stream capture); the look-up is repeated only when the
+ * device's CUDA context has changed (after cudaDeviceReset).  Every call on a
+ * device shares the array, so calls that overlap on the GPU (different
+ * streams, no ordering) race; order them.  Limits: n_terms <= 1024 and at
+ * most 256 distinct (X/Y mask, Y parity) groups; larger requests return
+ * SQ_ERR_UNSUPPORTED.  A call stages the grouped terms on the calling
+ * thread's stack (about 45 KiB). */
 int sq_expect_pauli_noalloc(const void *state, uint32_t num_qubits, int dtype,
                             const char *paulis, const double *weights,
                             uint32_t n_terms, double *out_device, void *stream);
@@ -319,6 +364,11 @@ int sq_jit_batch_adjoint_source(uint32_t num_qubits, int dtype, const sq_circuit
 int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream);
 /* Device time of the last sq_batch_run's kernel (ms) and its CTA count. */
 int sq_batch_last_timing(const sq_batch *b, double *kernel_ms, uint32_t *ctas);
+/* Plan statistics of the last sq_batch_run: circuits streamed through HBM
+ * (more qubits than the tile), their fused sweeps, and their algorithmic HBM
+ * bytes (per streamed circuit (2 x sweeps + 1) x 2^n x amplitude bytes: every
+ * sweep reads and writes the state, the energy pass reads it once). */
+int sq_batch_stats(const sq_batch *b, uint64_t *streamed, uint64_t *sweeps, uint64_t *hbm_bytes);
 
 #ifdef __cplusplus
 }

@@ -58,8 +58,10 @@ def lib() -> ctypes.CDLL:
 
 
 def ref_available() -> bool:
-    return os.path.exists(_REF_SO) or os.path.isdir(
-        "/root/reference/src/braket/snuqs/csrc")
+    """The compiled reference library exists, or its sources do (REF, as in
+    the Makefile) so that build() can make it."""
+    src = os.path.join(os.environ.get("REF", "/root/reference"), "src", "braket", "snuqs", "csrc")
+    return os.path.exists(_REF_SO) or os.path.isdir(src)
 
 
 def ref() -> ctypes.CDLL:
@@ -246,4 +248,96 @@ def expectation(state: np.ndarray, nq: int, terms: Sequence[tuple[float, str]]) 
     total = 0.0
     for w, p in terms:
         total += w * float(np.real(np.vdot(state, apply_pauli_string(state, nq, p))))
+    return total
+
+
+# ---------------------------------------------------------------------------
+# Measurement sampling (restates the device sampler's definition; the
+# reference samples with np.random.choice over |psi|^2, simulation.py:216-220,
+# whose random stream cannot be reproduced on the device).
+# ---------------------------------------------------------------------------
+SAMPLE_LEAF_BITS = 12
+
+
+def probability_tree(state: np.ndarray) -> list:
+    """Levels of the fixed binary tree of FP64 probability sums: level d has
+    2^d nodes, the last level is |psi_i|^2 (padded with zeros to at least
+    2^12 entries); each node is the IEEE sum of its two children."""
+    a = np.asarray(state).astype(np.complex128, copy=False)
+    p = a.real * a.real + a.imag * a.imag  # two products and one sum, no fused multiply-add
+    size = max(p.size, 1 << SAMPLE_LEAF_BITS)
+    if size != p.size:
+        p = np.concatenate([p, np.zeros(size - p.size)])
+    levels = [p]
+    while levels[-1].size > 1:
+        x = levels[-1]
+        levels.append(x[0::2] + x[1::2])
+    levels.reverse()
+    return levels
+
+
+def sample_inverse_cdf(state: np.ndarray, uniforms: np.ndarray) -> np.ndarray:
+    """Shot s: r = u_s * total; walk the tree from the root, going left when
+    r < left sum or the right sum is 0, else r -= left sum and go right."""
+    levels = probability_tree(state)
+    u = np.asarray(uniforms, dtype=np.float64)
+    r = u * levels[0][0]
+    k = np.zeros(u.size, dtype=np.int64)
+    for d in range(1, len(levels)):
+        lv = levels[d]
+        left_sum, right_sum = lv[2 * k], lv[2 * k + 1]
+        left = (r < left_sum) | (right_sum == 0.0)
+        r = np.where(left, r, r - left_sum)
+        k = 2 * k + (~left).astype(np.int64)
+    return k.astype(np.uint64)
+
+
+def marginal_probabilities(state: np.ndarray, nq: int, qubits: Sequence[int]) -> np.ndarray:
+    """Probabilities of the basis states of `qubits` (qubits[0] most
+    significant), the others traced out."""
+    p = (np.abs(np.asarray(state, dtype=np.complex128)) ** 2).reshape([2] * nq)
+    rest = [q for q in range(nq) if q not in qubits]
+    m = p.sum(axis=tuple(rest)) if rest else p
+    # Remaining axes are in ascending qubit order; put them in `qubits` order.
+    order = sorted(qubits)
+    m = np.transpose(m, [order.index(q) for q in qubits]) if len(qubits) > 1 else m
+    return np.asarray(m).reshape(-1)
+
+
+def variance(state: np.ndarray, nq: int, terms: Sequence[tuple[float, str]]) -> float:
+    """<H^2> - <H>^2 with H = sum_t w_t P_t: |H psi|^2 - <psi|H psi>^2."""
+    h = np.zeros_like(np.asarray(state, dtype=np.complex128))
+    for w, pstr in terms:
+        h += w * apply_pauli_string(state, nq, pstr)
+    e1 = float(np.real(np.vdot(state, h)))
+    return float(np.real(np.vdot(h, h))) - e1 * e1
+
+
+def expectation_indexed(state: np.ndarray, nq: int, terms: Sequence[tuple[float, str]]) -> float:
+    """The same sum_t w_t <psi|P_t|psi> as `expectation`, by index arithmetic
+    (P|i> = i^ny (-1)^popc(i & z) |i ^ x> for flip mask x, Z-or-Y mask z and
+    ny Y factors), for larger states."""
+    psi = np.asarray(state, dtype=np.complex128)
+    idx = np.arange(psi.size, dtype=np.uint64)
+    groups: dict = {}
+    for w, p in terms:
+        x = z = 0
+        ny = 0
+        for q, ch in enumerate(p):
+            bit = 1 << (nq - 1 - q)
+            if ch in "XY":
+                x |= bit
+            if ch in "ZY":
+                z |= bit
+            ny += ch == "Y"
+        groups.setdefault(x, []).append((w, z, ny))
+    total = 0.0
+    for x, ts in groups.items():
+        prod = np.conj(psi) * psi[idx ^ np.uint64(x)]  # conj(psi_i) psi_(i^x)
+        for w, z, ny in ts:
+            sign = 1.0 - 2.0 * (np.bitwise_count(idx & np.uint64(z)) & 1)
+            # <psi|P|psi> = sum_i conj(psi_i) (P psi)_i with (P psi)_i = i^ny (-1)^popc((i^x)&z) psi_(i^x)
+            sign_shift = -1.0 if (bin(x & z).count("1") & 1) else 1.0
+            val = (1j ** ny) * sign_shift * np.dot(sign, prod)
+            total += w * float(np.real(val))
     return total

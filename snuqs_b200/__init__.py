@@ -4,8 +4,9 @@
   (``braket.snuqs._C``: operation, operation.gate_operations, functionals,
   result_types, stream, event, core, core.cuda, DeviceType).
 * ``snuqs_b200.capi`` -- ctypes binding of the C ABI (include/snuqs_b200.h).
-* ``snuqs_b200.simulation`` / ``transpile`` / ``gate_operations`` -- the
-  reference's Python driver layer for the no-offload CUDA path.
+* ``snuqs_b200.adjoint`` -- adjoint gradients behind ``torch.autograd``.
+* ``snuqs_b200.circuits`` -- seeded workload generators.
+* ``snuqs_b200.sharding`` -- batches split across ranks (torch.distributed).
 
 The native libraries are built in-tree by ``python -m snuqs_b200.build``.
 Without them every engine entry point raises (``import snuqs_b200._C`` fails,

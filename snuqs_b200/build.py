@@ -24,7 +24,7 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-ENGINE_CU = ["engine.cu", "noalloc.cu", "batch.cu", "jit.cu"]
+ENGINE_CU = ["engine.cu", "noalloc.cu", "batch.cu", "jit.cu", "results.cu"]
 ENGINE_CC = ["gates.cc", "planner.cc", "adjoint_plan.cc"]
 # Fused-sweep kernel instantiations: (precision, tile bits, CTAs per SM).
 # Tile sizes must match kTileBitsC128 / kTileBitsC64 in csrc/sq_plan.h; the

@@ -1,8 +1,7 @@
 """ctypes binding of the C ABI (include/snuqs_b200.h).
 
 This is the binding a maintainer would add on the reference side to call the
-engine without pybind11; the tests use it to drive the
-C ABI directly.  Every call checks its status and raises SqError with the
+engine without pybind11; the tests use it to drive the C ABI directly.  Every call checks its status and raises SqError with the
 library's message.
 """
 from __future__ import annotations
@@ -80,6 +79,12 @@ SIGNATURES = {
     "sq_copy_to_host": (_I, [_P, _P, _P]),
     "sq_copy_from_host": (_I, [_P, _P, _P]),
     "sq_copy_state": (_I, [_P, _P, _P]),
+    "sq_state_check": (_I, [_P, _P]),
+    "sq_variance_pauli": (_I, [_P, ctypes.c_char_p, _PD, _U32, _PD, _P]),
+    "sq_sample": (_I, [_P, _P, _U64, _P, _P]),
+    "sq_amplitudes": (_I, [_P, _P, _U64, _P, _P]),
+    "sq_marginal_probabilities": (_I, [_P, _PU32, _U32, _P, _P]),
+    "sq_state_distance": (_I, [_P, _P, _PD, _PD, _P]),
     "sq_probabilities": (_I, [_P, _P, _P]),
     "sq_expect_pauli": (_I, [_P, ctypes.c_char_p, _PD, _U32, _PD, _P]),
     "sq_norm2": (_I, [_P, _PD, _P]),
@@ -97,6 +102,7 @@ SIGNATURES = {
     "sq_batch_autotune": (_I, [_P, _U32, _P, _P]),
     "sq_batch_state": (_I, [_P, _U32, _P, _P]),
     "sq_batch_last_timing": (_I, [_P, _PD, _PU32]),
+    "sq_batch_stats": (_I, [_P, _PU64, _PU64, _PU64]),
 }
 
 
@@ -315,6 +321,13 @@ class Batch:
         check(lib().sq_batch_state(self.h, circuit, a.ctypes.data_as(_P), None))
         return a
 
+    def stats(self):
+        """(streamed circuits, their sweeps, their algorithmic HBM bytes) of
+        the last run."""
+        a, b, c = _U64(0), _U64(0), _U64(0)
+        check(lib().sq_batch_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
     def last_timing(self):
         ms, ctas = _D(0), _U32(0)
         check(lib().sq_batch_last_timing(self.h, ctypes.byref(ms), ctypes.byref(ctas)))
@@ -452,7 +465,7 @@ class State:
         if out is None:
             out = np.empty(1 << self.n, dtype=self.np_dtype)
         check(lib().sq_copy_to_host(self.h, out.ctypes.data_as(_P), self.stream))
-        check(lib().sq_stream_synchronize(self.stream))
+        check(lib().sq_state_check(self.h, self.stream))
         return out
 
     def from_host(self, a: np.ndarray) -> None:
@@ -468,6 +481,51 @@ class State:
         check(lib().sq_expect_pauli(self.h, flat, _dp(w), len(terms), ctypes.byref(out),
                                     self.stream))
         return out.value
+
+    def variance(self, terms) -> float:
+        """<H^2> - <H>^2 of the Pauli sum `terms` (list of (weight, string))."""
+        flat = "".join(p for _, p in terms).encode()
+        w = np.ascontiguousarray([float(x) for x, _ in terms] or [0.0], dtype=np.float64)
+        out = _D(0)
+        check(lib().sq_variance_pauli(self.h, flat, _dp(w), len(terms), ctypes.byref(out),
+                                      self.stream))
+        return out.value
+
+    def sample(self, uniforms) -> np.ndarray:
+        """Basis-state indices of len(uniforms) shots (device inverse CDF)."""
+        import torch
+
+        u = torch.as_tensor(np.ascontiguousarray(uniforms, dtype=np.float64)).cuda()
+        out = torch.empty(u.numel(), dtype=torch.int64, device="cuda")
+        check(lib().sq_sample(self.h, ctypes.c_void_p(u.data_ptr()), u.numel(),
+                              ctypes.c_void_p(out.data_ptr()), self.stream))
+        check(lib().sq_state_check(self.h, self.stream))
+        return out.cpu().numpy().astype(np.uint64)
+
+    def amplitudes(self, indices) -> np.ndarray:
+        import torch
+
+        idx = torch.as_tensor(np.ascontiguousarray(indices, dtype=np.int64)).cuda()
+        out = torch.empty((idx.numel(), 2), dtype=torch.float64, device="cuda")
+        check(lib().sq_amplitudes(self.h, ctypes.c_void_p(idx.data_ptr()), idx.numel(),
+                                  ctypes.c_void_p(out.data_ptr()), self.stream))
+        o = out.cpu().numpy()
+        return o[:, 0] + 1j * o[:, 1]
+
+    def marginal_probabilities(self, qubits) -> np.ndarray:
+        import torch
+
+        out = torch.empty(1 << len(qubits), dtype=torch.float64, device="cuda")
+        check(lib().sq_marginal_probabilities(self.h, _u32(qubits), len(qubits),
+                                              ctypes.c_void_p(out.data_ptr()), self.stream))
+        check(lib().sq_state_check(self.h, self.stream))
+        return out.cpu().numpy()
+
+    def distance(self, other: "State"):
+        """(max-abs amplitude difference, 1 - fidelity) against `other`."""
+        mx, fl = _D(0), _D(0)
+        check(lib().sq_state_distance(self.h, other.h, ctypes.byref(mx), ctypes.byref(fl), self.stream))
+        return mx.value, fl.value
 
     def norm2(self) -> float:
         out = _D(0)

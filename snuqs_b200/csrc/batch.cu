@@ -121,6 +121,10 @@ struct sq_batch {
   uint64_t version = 0, planned_version = ~uint64_t(0);
   uint32_t planned_m = 0, planned_l = 0, planned_ops = 0;
   size_t planned_bytes = 0;
+  // Plan statistics of the streamed circuits (n > tile bits) of the last
+  // energy plan: count, fused sweeps, and their algorithmic HBM bytes (each
+  // sweep reads and writes the state, the energy pass reads it once).
+  uint64_t stat_streamed = 0, stat_sweeps = 0, stat_bytes = 0;
 };
 
 namespace {
@@ -342,6 +346,13 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   for (auto &th : pool) th.join();
   for (size_t i = 0; i < nc; ++i)
     if (nsweeps[i] < 0) return fail(SQ_ERR_UNSUPPORTED, errs[i]);
+  b->stat_streamed = b->stat_sweeps = b->stat_bytes = 0;
+  for (size_t i = 0; i < nc; ++i)
+    if (b->circs[i].n > M) {
+      b->stat_streamed++;
+      b->stat_sweeps += uint64_t(nsweeps[i]);
+      b->stat_bytes += (2 * uint64_t(nsweeps[i]) + 1) * (uint64_t(1) << b->circs[i].n) * sizeof(C2);
+    }
   // Largest circuits first (dynamic work queue).
   b->order.resize(nc);
   for (size_t i = 0; i < nc; ++i) b->order[i] = uint32_t(i);
@@ -991,6 +1002,14 @@ int sq_batch_state(sq_batch *b, uint32_t circuit, void *host_dst, void *stream) 
   SQB_CUDA(cudaMemcpyAsync(host_dst, static_cast<char *>(b->d_pool.p) + b->state_off[circuit] * amp,
                            n * amp, cudaMemcpyDeviceToHost, st));
   SQB_CUDA(cudaStreamSynchronize(st));
+  return SQ_OK;
+}
+
+int sq_batch_stats(const sq_batch *b, uint64_t *streamed, uint64_t *sweeps, uint64_t *hbm_bytes) {
+  if (!b) return fail(SQ_ERR_INVALID, "null batch");
+  if (streamed) *streamed = b->stat_streamed;
+  if (sweeps) *sweeps = b->stat_sweeps;
+  if (hbm_bytes) *hbm_bytes = b->stat_bytes;
   return SQ_OK;
 }
 

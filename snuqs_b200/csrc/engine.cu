@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
+#include <complex>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -18,6 +19,7 @@
 #include "../../include/snuqs_b200.h"
 #include "adjoint_kernels.cuh"
 #include "adjoint_plan.h"
+#include "engine_internal.h"
 #include "host_ops.h"
 #include "jit.h"
 #include "reduce_kernels.cuh"
@@ -85,6 +87,11 @@ struct sq_state {
   uint32_t low_bits = 0;  // 0: automatic
   int jit = -1;  // -1: automatic (states of >= kJitMinQubits qubits), 0: off, 1: on
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sweep_events;
+  // Device word a sweep kernel sets when one of its bounded waits gives up
+  // (sq::kKernelErrTimeout); read and cleared by sq_state_check.
+  uint32_t *errword = nullptr;
+  void *rscratch = nullptr;  // result kernels' scratch (results.cu)
+  size_t rscratch_bytes = 0;
 };
 
 // JIT-specialised sweeps pay a one-off NVRTC compile per distinct sweep
@@ -288,7 +295,8 @@ static int launch_sweep(sq_state *s, const sq::PlannedSweep &ps, cudaStream_t st
     SQ_CUDA(cudaEventRecord(e0, st));
   }
   C2 *psi = reinterpret_cast<C2 *>(s->data);
-  void *args[] = {&psi, P.get()};
+  uint32_t *errp = s->errword;
+  void *args[] = {&psi, P.get(), &errp};  // the generic kernel takes the first two
   SQ_CUDA(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(threads), args, launch_smem, st));
   SQ_CUDA(cudaGetLastError());
   if (s->timing) {
@@ -475,6 +483,37 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
   return SQ_OK;
 }
 
+static int alloc_errword(sq_state *s) {
+  SQ_CUDA(cudaMalloc(&s->errword, sizeof(uint32_t)));
+  SQ_CUDA(cudaMemset(s->errword, 0, sizeof(uint32_t)));
+  return SQ_OK;
+}
+
+// Reads (and clears) the word a sweep kernel sets when a bounded wait gives
+// up; the caller has synchronised the stream the kernels ran on.
+static int take_kernel_error(sq_state *s) {
+  if (!s->errword) return SQ_OK;
+  uint32_t w = 0;
+  SQ_CUDA(cudaMemcpy(&w, s->errword, sizeof(w), cudaMemcpyDeviceToHost));
+  if (!w) return SQ_OK;
+  SQ_CUDA(cudaMemset(s->errword, 0, sizeof(uint32_t)));
+  return fail(SQ_ERR_TIMEOUT, "a sweep kernel gave up waiting for its tile copies (error word 0x%x); "
+              "the state is invalid", w);
+}
+
+int sq_detail_state_scratch(sq_state *s, size_t bytes, void **out) {
+  if (s->rscratch_bytes < bytes) {
+    SQ_TRY(use_device(s->device));
+    if (s->rscratch) SQ_CUDA(cudaFree(s->rscratch));
+    s->rscratch = nullptr;
+    s->rscratch_bytes = 0;
+    SQ_CUDA(cudaMalloc(&s->rscratch, bytes));
+    s->rscratch_bytes = bytes;
+  }
+  *out = s->rscratch;
+  return SQ_OK;
+}
+
 static int ensure_scratch(sq_state *s, uint32_t len) {
   if (s->scratch_len >= len) return SQ_OK;
   if (s->scratch) SQ_CUDA(cudaFree(s->scratch));
@@ -607,7 +646,19 @@ int sq_state_create(uint32_t num_qubits, int dtype, sq_state **out) {
   s->tile_bits = dtype == SQ_C64 ? sq::kDefaultTileBitsC64 : sq::kDefaultTileBitsC128;
   SQ_CUDA(cudaGetDevice(&s->device));
   const size_t bytes = (size_t(1) << num_qubits) * amp_bytes(dtype);
-  SQ_CUDA(cudaMalloc(&s->data, bytes));
+  const cudaError_t e = cudaMalloc(&s->data, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    s->data = nullptr;
+    return fail(SQ_ERR_OOM, "cannot allocate %zu bytes of device memory for a %u-qubit state", bytes,
+                num_qubits);
+  }
+  SQ_CUDA(e);
+  const int es = alloc_errword(s.get());
+  if (es != SQ_OK) {
+    cudaFree(s->data);
+    return es;
+  }
   *out = s.release();
   return SQ_OK;
 }
@@ -624,6 +675,7 @@ int sq_state_wrap(void *device_ptr, uint32_t num_qubits, int dtype, sq_state **o
   s->owns = false;
   s->tile_bits = dtype == SQ_C64 ? sq::kDefaultTileBitsC64 : sq::kDefaultTileBitsC128;
   SQ_CUDA(cudaGetDevice(&s->device));
+  SQ_TRY(alloc_errword(s.get()));
   *out = s.release();
   return SQ_OK;
 }
@@ -634,6 +686,8 @@ int sq_state_destroy(sq_state *s) {
   SQ_TRY(use_device(s->device));
   if (s->owns && s->data) SQ_CUDA(cudaFree(s->data));
   if (s->scratch) SQ_CUDA(cudaFree(s->scratch));
+  if (s->errword) SQ_CUDA(cudaFree(s->errword));
+  if (s->rscratch) SQ_CUDA(cudaFree(s->rscratch));
   for (auto &ev : s->sweep_events) {
     cudaEventDestroy(ev.first);
     cudaEventDestroy(ev.second);
@@ -810,6 +864,13 @@ int sq_copy_to_host(sq_state *s, void *dst, void *stream) {
   return SQ_OK;
 }
 
+int sq_state_check(sq_state *s, void *stream) {
+  if (!s) return fail(SQ_ERR_INVALID, "null pointer");
+  SQ_TRY(use_device(s->device));
+  SQ_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  return take_kernel_error(s);
+}
+
 int sq_copy_from_host(sq_state *s, const void *src, void *stream) {
   if (!s || !src) return fail(SQ_ERR_INVALID, "null pointer");
   SQ_TRY(use_device(s->device));
@@ -918,7 +979,7 @@ static int expect_impl(sq_state *s, const std::vector<uint64_t> &xm,
   SQ_CUDA(cudaGetLastError());
   SQ_CUDA(cudaMemcpyAsync(out, s->scratch + blocks, sizeof(double), cudaMemcpyDeviceToHost, st));
   SQ_CUDA(cudaStreamSynchronize(st));
-  return SQ_OK;
+  return take_kernel_error(s);
 }
 
 int sq_expect_pauli(sq_state *s, const char *paulis, const double *weights, uint32_t n_terms,
@@ -943,6 +1004,78 @@ int sq_expect_pauli(sq_state *s, const char *paulis, const double *weights, uint
     }
   }
   return expect_impl(s, xm, zym, ny, w, out, static_cast<cudaStream_t>(stream));
+}
+
+// Pauli strings -> (flip mask, Z-or-Y mask, Y count) per term.
+static int parse_paulis(uint32_t n, const char *paulis, uint32_t n_terms, std::vector<uint64_t> &xm,
+                        std::vector<uint64_t> &zym, std::vector<int> &ny) {
+  xm.assign(n_terms, 0);
+  zym.assign(n_terms, 0);
+  ny.assign(n_terms, 0);
+  for (uint32_t t = 0; t < n_terms; ++t) {
+    for (uint32_t q = 0; q < n; ++q) {
+      const uint64_t bit = uint64_t(1) << (n - 1 - q);
+      switch (paulis[size_t(t) * n + q]) {
+        case 'I': case 'i': break;
+        case 'X': case 'x': xm[t] |= bit; break;
+        case 'Y': case 'y': xm[t] |= bit; zym[t] |= bit; ny[t]++; break;
+        case 'Z': case 'z': zym[t] |= bit; break;
+        default:
+          return fail(SQ_ERR_INVALID, "term %u: bad Pauli character at qubit %u", t, q);
+      }
+    }
+  }
+  return SQ_OK;
+}
+
+int sq_variance_pauli(sq_state *s, const char *paulis, const double *weights, uint32_t n_terms,
+                      double *out, void *stream) {
+  if (!s || !out || (n_terms && (!paulis || !weights))) return fail(SQ_ERR_INVALID, "null pointer");
+  if (n_terms > 1024) return fail(SQ_ERR_UNSUPPORTED, "sq_variance_pauli: more than 1024 terms");
+  SQ_TRY(use_device(s->device));
+  const uint32_t n = s->n;
+  auto st = static_cast<cudaStream_t>(stream);
+  std::vector<uint64_t> xm, zym;
+  std::vector<int> ny;
+  SQ_TRY(parse_paulis(n, paulis, n_terms, xm, zym, ny));
+  std::vector<double> w(weights, weights + n_terms);
+  double e1 = 0.0;
+  SQ_TRY(expect_impl(s, xm, zym, ny, w, &e1, st));
+  // H^2 = sum_{s,t} w_s w_t P_s P_t.  With P = i^ny X^x Z^z (x = flip mask,
+  // z = Z-or-Y mask): P_s P_t = i^(ny_s + ny_t) (-1)^popc(z_s & x_t)
+  // X^(x_s ^ x_t) Z^(z_s ^ z_t), which is i^(ny_s + ny_t - ny_u) (-1)^...
+  // times the Pauli string P_u with x_u = x_s ^ x_t, z_u = z_s ^ z_t.
+  std::map<std::pair<uint64_t, uint64_t>, std::complex<double>> acc;
+  for (uint32_t a = 0; a < n_terms; ++a)
+    for (uint32_t b = 0; b < n_terms; ++b) {
+      const uint64_t xu = xm[a] ^ xm[b], zu = zym[a] ^ zym[b];
+      const int nyu = __builtin_popcountll(xu & zu);
+      int ph = (ny[a] + ny[b] - nyu) % 4;
+      if (ph < 0) ph += 4;
+      if (__builtin_popcountll(zym[a] & xm[b]) & 1) ph = (ph + 2) % 4;
+      static const std::complex<double> ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+      acc[{xu, zu}] += ipow[ph] * (w[a] * w[b]);
+    }
+  std::vector<uint64_t> x2, z2;
+  std::vector<int> ny2;
+  std::vector<double> w2;
+  for (const auto &kv : acc) {
+    if (kv.second.real() == 0.0) continue;  // anticommuting pairs cancel
+    x2.push_back(kv.first.first);
+    z2.push_back(kv.first.second);
+    ny2.push_back(__builtin_popcountll(kv.first.first & kv.first.second));
+    w2.push_back(kv.second.real());
+  }
+  if (x2.empty()) {
+    x2.push_back(0);
+    z2.push_back(0);
+    ny2.push_back(0);
+    w2.push_back(0.0);
+  }
+  double e2 = 0.0;
+  SQ_TRY(expect_impl(s, x2, z2, ny2, w2, &e2, st));
+  *out = e2 - e1 * e1;
+  return SQ_OK;
 }
 
 int sq_norm2(sq_state *s, double *out, void *stream) {

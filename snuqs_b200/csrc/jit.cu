@@ -330,7 +330,21 @@ bool lane_indexed(const SweepOp &op) {
 
 struct JitShape {
   bool smem_coef = false, dload = false, dstore = false;
+  int stages = 0;     // > 0: bulk-copy pipeline with this many tiles in flight per CTA
+  bool work = false;  // pipeline: some phase passes the tile through the work buffer
 };
+
+// Tiles in flight per CTA of a pipelined (bulk-copy) sweep; 0 turns the
+// pipeline off.  SQ_JIT_STAGES overrides.
+int jit_stages(bool c64) {
+  static const int env = [] {
+    const char *e = std::getenv("SQ_JIT_STAGES");
+    return e && *e ? std::atoi(e) : -1;
+  }();
+  if (env >= 0 && env <= 4) return env;
+  (void)c64;
+  return 1;
+}
 
 // Direct loads (first phase from HBM, no prefetch into a second tile buffer)
 // measured faster on B200 for complex128 (7.10 vs 7.38 ms per 30-qubit sweep)
@@ -346,6 +360,14 @@ JitShape jit_shape(const PlannedSweep &ps, bool c64) {
   for (const SweepOp &op : ps.op) j.smem_coef |= lane_indexed(op);
   j.dload = dload_on && (ps.h.flags & kDirectLoad);
   j.dstore = (ps.h.flags & kDirectStore) != 0;
+  // The pipeline needs a first phase whose lanes cover the low tile bits (a
+  // direct-load sweep) and runs of at least 16 bytes.
+  const int st = jit_stages(c64);
+  if (st > 0 && (ps.h.flags & kDirectLoad) && ((1u << ps.h.l) * (c64 ? 8u : 16u)) % 16u == 0) {
+    j.stages = st;
+    j.dload = false;
+    j.work = ps.h.nphases > 1 || !j.dstore;
+  }
   return j;
 }
 
@@ -356,24 +378,34 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
   std::ostringstream s;
   s << "extern \"C\" __global__ void __launch_bounds__(" << (1 << (M - kRegBits)) << ", " << minb
     << ")\nsq_jit_sweep(Vec2<" << R << ">::T *__restrict__ psi, const __grid_constant__ SweepParams<"
-    << R << "> P) {\n";
+    << R << "> P, uint32_t *__restrict__ err) {\n";
   s << "  using C2 = Vec2<" << R << ">::T;\n";
   s << "  using Tile = JitTile<" << M << ", " << ps.h.l;
   for (uint32_t i = 0; i < ps.h.m - ps.h.l; ++i) s << ", " << int(ps.h.hi[i]);
   s << ">;\n";
   auto tf = [](bool b) { return b ? "true" : "false"; };
-  s << "  jit_sweep<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dload) << ", "
-    << tf(js.dstore) << ">(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
+  const bool pipe = js.stages > 0;
+  if (pipe)
+    s << "  jit_sweep_pipe<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.work) << ", "
+      << tf(js.dstore) << ", " << js.stages
+      << ">(psi, P, err, [&](const C2 *stage, C2 *tile, const C2 *coef, uint64_t gbase, const PipeCtl<" << R
+      << ", " << M << ", Tile, " << js.stages << "> &ctl) {\n";
+  else
+    s << "  (void)err;\n  jit_sweep<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dload)
+      << ", " << tf(js.dstore) << ">(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
   const uint32_t last = ps.h.nphases - 1;
   for (uint32_t p = 0; p < ps.h.nphases; ++p) {
     const SweepPhase &ph = ps.ph[p];
+    const bool from_stage = p == 0 && pipe;
     const bool from_hbm = p == 0 && js.dload, to_hbm = p == last && js.dstore;
     s << "    {\n      using Ph = JitPhase<" << R << ", " << M << ", Tile, " << int(ph.reg[0]) << ", "
       << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]);
-    for (int t : thread_positions(ph, M, c64, from_hbm || to_hbm)) s << ", " << t;
+    for (int t : thread_positions(ph, M, c64, from_hbm || from_stage || to_hbm)) s << ", " << t;
     s << ">;\n";
     s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << "> A;\n";
-    if (from_hbm)
+    if (from_stage)
+      s << "      Ph::gather_lin(A, stage, jb);\n      ctl.release();\n";
+    else if (from_hbm)
       s << "      Ph::load(A, psi, gbase, jb);\n";
     else
       s << "      Ph::gather(A, tile, jb);\n";
@@ -733,7 +765,9 @@ void jit_prepare_adjoint(const std::vector<const PlannedSweep *> &sweeps, bool c
 
 size_t jit_smem(const PlannedSweep &ps, bool c64) {
   const JitShape js = jit_shape(ps, c64);
-  return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload, js.smem_coef ? (ps.h.ncoef + 1) & ~1u : 0u);
+  const uint32_t nc = js.smem_coef ? (ps.h.ncoef + 1) & ~1u : 0u;
+  if (js.stages > 0) return jit_pipe_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.stages, js.work, nc);
+  return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload, nc);
 }
 
 int jit_minb(bool c64, uint32_t m) {

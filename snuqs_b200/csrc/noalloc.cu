@@ -12,12 +12,18 @@
 // holds until the process exits; nothing is allocated per call.  The caller
 // passes the state and the output location.  The first call on a device
 // looks up the array's device address (make that first call before any
-// stream capture).  All calls on a device share the array, so calls that
-// overlap on the GPU race: order them on one stream or with events.
+// stream capture).  The address is saved per device together with the CUDA
+// context that was current at the look-up; when the context changes (after
+// cudaDeviceReset, or a primary context torn down and rebuilt) the next call
+// looks the address up again instead of using a stale one.  All calls on a
+// device share the array, so calls that overlap on the GPU race: order them
+// on one stream or with events.
 //
 // The array's limits: at most kNoAllocMaxBlocks (2048) reduction blocks
 // (16 KiB of FP64 partials), at most 1024 Pauli terms and 256 distinct
 // (X/Y mask, Y parity) groups per call.  Larger requests are rejected.
+// Each call stages the grouped terms on the calling thread's stack (about
+// 45 KiB: the kernel's parameter block and four term arrays).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,25 +45,38 @@ static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxBlocks];
 
 std::mutex g_mu;
 double *g_partials_ptr[kMaxDevices] = {};
+void *g_partials_ctx[kMaxDevices] = {};
 int g_sms[kMaxDevices] = {};
-
-// Fixed-order sum of the partials into the caller's output (deterministic).
-__global__ void __launch_bounds__(sq::kReduceThreads)
-    noalloc_finalize_kernel(const double *__restrict__ partials, uint32_t n,
-                            double *__restrict__ out) {
-  double v = 0.0;
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
-  const double s = sq::block_sum(v);
-  if (threadIdx.x == 0) out[0] = s;
-}
 
 int fail(int code, const char *msg) { return sq_detail_fail(code, msg); }
 
-// Device set-up, once per device with that device current: the host-side
-// name of a __device__ array is not a device address, so look the address up.
+// The current CUDA context (driver cuCtxGetCurrent, reached through the
+// runtime's entry-point query so that the library needs no libcuda link).
+int current_context(void **ctx) {
+  using GetCurrent = int (*)(void **);
+  static GetCurrent fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCurrent>(f);
+  }();
+  if (!fn) return fail(SQ_ERR_CUDA, "sq_expect_pauli_noalloc: cuCtxGetCurrent unavailable");
+  *ctx = nullptr;
+  if (fn(ctx) != 0 || !*ctx) return fail(SQ_ERR_CUDA, "sq_expect_pauli_noalloc: no current context");
+  return SQ_OK;
+}
+
+// Device set-up, with that device current, once per device and context: the
+// host-side name of a __device__ array is not a device address, so look the
+// address up (and again whenever the device's context has changed).
 int setup_device(int dev, double **partials, int *sms) {
+  void *ctx = nullptr;
+  const int cs = current_context(&ctx);
+  if (cs != SQ_OK) return cs;
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_partials_ptr[dev]) {
+  if (!g_partials_ptr[dev] || g_partials_ctx[dev] != ctx) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess) return fail(SQ_ERR_CUDA, cudaGetErrorString(e));
@@ -65,6 +84,7 @@ int setup_device(int dev, double **partials, int *sms) {
     e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return fail(SQ_ERR_CUDA, cudaGetErrorString(e));
     g_partials_ptr[dev] = static_cast<double *>(p);
+    g_partials_ctx[dev] = ctx;
     g_sms[dev] = n;
   }
   *partials = g_partials_ptr[dev];
@@ -161,7 +181,8 @@ extern "C" int sq_expect_pauli_noalloc(const void *state, uint32_t num_qubits, i
         static_cast<const double2 *>(state), P, partials, 0);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(SQ_ERR_CUDA, cudaGetErrorString(e));
-  noalloc_finalize_kernel<<<1, sq::kReduceThreads, 0, s>>>(partials, blocks, out_device);
+  // Fixed-order sum of the partials into the caller's output (deterministic).
+  sq::finalize_sum_kernel<<<1, sq::kReduceThreads, 0, s>>>(partials, blocks, out_device);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(SQ_ERR_CUDA, cudaGetErrorString(e));
   return SQ_OK;

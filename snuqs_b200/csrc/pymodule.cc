@@ -612,6 +612,15 @@ PYBIND11_MODULE(_C, m) {
                                                   precision == "complex64" ? SQ_C64 : SQ_C128);
            }),
            py::arg("device"), py::arg("num_qubits"), py::arg("precision"))
+      // A host (optionally pinned) state of either precision, e.g. the
+      // destination of a complex64 device state's copy.
+      .def(py::init([](size_t n, bool pinned, const std::string &precision) {
+             if (precision != "complex128" && precision != "complex64")
+               throw py::value_error("precision must be 'complex128' or 'complex64'");
+             return std::make_shared<StateVector>(DeviceType::CPU, n, pinned,
+                                                  precision == "complex64" ? SQ_C64 : SQ_C128);
+           }),
+           py::arg("num_qubits"), py::arg("pinned"), py::arg("precision"))
       .def("cpu", &StateVector::cpu, py::kw_only(), py::arg("stream") = nullptr)
       .def("cuda", &StateVector::cuda, py::kw_only(), py::arg("stream") = nullptr)
       .def("copy", &StateVector::copy, py::arg("other"), py::kw_only(), py::arg("stream") = nullptr)

@@ -589,6 +589,7 @@ struct ParamCoef {
 template <int M, int L, int... HI>
 struct JitTile {
   static_assert(sizeof...(HI) == M - L, "one global bit per high tile position");
+  static constexpr int kLow = L;
   // Global offset of tile-local index j.  Bitwise: off(a | b) = off(a) | off(b)
   // for disjoint a, b.
   __host__ __device__ static constexpr uint64_t off(uint32_t j) {
@@ -649,6 +650,20 @@ struct JitPhase {
       v.x = A.re[ri];
       v.y = A.im[ri];
       tile[slot(sb, ri)] = v;
+    }
+  }
+  // From a row-major (unswizzled) copy of the tile: tile index j at j.
+  __device__ __forceinline__ static constexpr uint32_t loff(int ri) {
+    return ((ri & 1) ? 1u << R0 : 0u) | ((ri & 2) ? 1u << R1 : 0u) | ((ri & 4) ? 1u << R2 : 0u) |
+           ((ri & 8) ? 1u << R3 : 0u);
+  }
+  __device__ __forceinline__ static void gather_lin(Amps<Real> &A, const C2 *stage, uint32_t jbv) {
+    const C2 *p = stage + jbv;
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri) {
+      const C2 v = p[loff(ri)];
+      A.re[ri] = v.x;
+      A.im[ri] = v.y;
     }
   }
   // Straight from HBM into registers (a first phase whose register bits
@@ -753,6 +768,185 @@ __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ p
     }
     cp_async_wait_prev();
     asm volatile("cp.async.wait_all;\n" ::: "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bulk-copy tile pipeline (cp.async.bulk with mbarrier transaction counts).
+//
+// A sweep whose first phase reads its amplitudes with the lanes on the low
+// tile positions (the planner's direct-load sweeps) can take its tile from a
+// plain row-major copy of the tile: the lanes that share a shared-memory
+// wavefront then read consecutive amplitudes, conflict-free without a
+// swizzle.  Such a copy is exactly what the bulk-copy engine produces: one
+// cp.async.bulk per contiguous run of 2^L amplitudes (128 bytes), issued by
+// one warp, completing on the stage's mbarrier.  The copies need no thread
+// registers and no per-thread instructions, so a CTA keeps S tiles in flight
+// while it computes: the loads of tile i + S are issued as soon as every
+// thread has read tile i's stage (right after the first phase's gather), and
+// overlap the remaining phases and stores of tile i.  Later phases pass the
+// tile through a swizzled work buffer as in jit_sweep; the last phase of a
+// direct-store sweep writes to HBM from registers.
+// Every wait is bounded: a stage that has not arrived after kPipeWaitPolls
+// polls sets the sweep's error word (read by the host) and the CTA stops
+// waiting; the remaining tiles are then garbage, which the error reports.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kPipeWaitPolls = 1u << 22;
+constexpr uint32_t kKernelErrTimeout = 1u;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// One arrival that also announces `bytes` of bulk-copy transactions.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for the phase of `bar` with the given parity.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kPipeWaitPolls; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Global -> shared bulk copy completing `bytes` transactions on `bar`
+// (both addresses 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// Orders this thread's earlier generic-proxy shared-memory accesses (made
+// visible to it by a barrier) before its later bulk copies into the same
+// memory.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// Dynamic shared memory of a pipelined JIT sweep: S stages (row-major tiles),
+// the swizzled work buffer when some phase passes the tile through shared
+// memory, the coefficients when a phase reads them there, S mbarriers.
+__host__ __device__ constexpr size_t jit_pipe_smem_bytes(int m, size_t amp_bytes, int stages, bool work,
+                                                         uint32_t smem_coef) {
+  return (size_t(stages) + (work ? 1 : 0)) * (size_t(1) << m) * amp_bytes + size_t(smem_coef) * amp_bytes +
+         size_t(stages) * 8;
+}
+
+// Copy-engine side of the pipeline: warp 0 issues the bulk copies of local
+// tile i (tile blockIdx.x + i * gridDim.x) into stage i % S; release() is
+// called by every thread once it has read the current tile's stage.
+template <typename Real, int M, class Tile, int S>
+struct PipeCtl {
+  using C2 = typename Vec2<Real>::T;
+  static constexpr uint32_t TS = 1u << M;
+  static constexpr int L = Tile::kLow;
+  static constexpr uint32_t RUNS = 1u << (M - L);
+  static constexpr uint32_t RUN_BYTES = (1u << L) * uint32_t(sizeof(C2));
+  static_assert(RUN_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
+  const C2 *psi;
+  C2 *stages;
+  uint64_t *bar;
+  uint64_t ntiles;  // tiles of this CTA
+  uint64_t cur;     // local index of the tile being processed
+  uint32_t lane, warp;
+
+  __device__ __forceinline__ void issue(uint64_t i) const {
+    const int s = int(i % S);
+    if (lane == 0) mbar_arrive_expect_tx(&bar[s], TS * uint32_t(sizeof(C2)));
+    __syncwarp();  // the transaction count is announced before any copy lands
+    const C2 *src = psi + Tile::base(blockIdx.x + i * gridDim.x);
+    C2 *dst = stages + s * TS;
+    for (uint32_t r = lane; r < RUNS; r += 32)
+      bulk_load(dst + (r << L), src + Tile::off(r << L), RUN_BYTES, &bar[s]);
+  }
+  // Every thread has read stage cur % S: hand it to tile cur + S.
+  __device__ __forceinline__ void release() const {
+    __syncthreads();
+    if (warp == 0 && cur + S < ntiles) {
+      fence_proxy_async_smem();
+      issue(cur + S);
+    }
+  }
+};
+
+// The pipelined tile loop.  phases(stage, work, coef, gbase, ctl) runs every
+// phase of one tile; its first phase gathers from `stage` (row-major) and
+// then calls ctl.release(), which hands the stage back to the copy engine.
+//  SMEM_COEF: some phase reads coefficients from shared memory;
+//  WORK:      some phase passes the tile through the work buffer;
+//  DSTORE:    the last phase stores to HBM itself (no copy-out);
+//  S:         stages (tiles in flight per CTA).
+template <typename Real, int M, class Tile, bool SMEM_COEF, bool WORK, bool DSTORE, int S, class Phases>
+__device__ __forceinline__ void jit_sweep_pipe(typename Vec2<Real>::T *__restrict__ psi,
+                                               const SweepParams<Real> &P, uint32_t *__restrict__ err,
+                                               Phases phases) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int NT = 1 << (M - kRegBits);
+  constexpr uint32_t TS = 1u << M;
+  constexpr uint32_t PER = TS / NT;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const SweepHeader &h = P.h;
+  PipeCtl<Real, M, Tile, S> ctl;
+  ctl.psi = psi;
+  ctl.stages = reinterpret_cast<C2 *>(smem_raw);
+  C2 *work = ctl.stages + S * TS;
+  C2 *coef = work + (WORK ? TS : 0);
+  ctl.bar = reinterpret_cast<uint64_t *>(coef + (SMEM_COEF ? ((h.ncoef + 1) & ~1u) : 0u));
+  const uint32_t tid = threadIdx.x;
+  ctl.lane = tid & 31u;
+  ctl.warp = tid >> 5;
+  ctl.ntiles = h.num_tiles > blockIdx.x ? (h.num_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  ctl.cur = 0;
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&ctl.bar[s], 1);
+    fence_mbar_init();
+  }
+  if constexpr (SMEM_COEF) {
+    for (uint32_t i = tid; i < h.ncoef; i += NT) {
+      C2 v;
+      v.x = P.coef[2 * i];
+      v.y = P.coef[2 * i + 1];
+      coef[i] = v;
+    }
+  }
+  __syncthreads();
+  if (ctl.warp == 0)
+    for (uint64_t i = 0; i < uint64_t(S) && i < ctl.ntiles; ++i) ctl.issue(i);
+  const uint32_t s_tid = swz<Real>(tid);
+  const uint64_t toff = Tile::off(tid);
+  bool alive = true;
+  for (uint64_t i = 0; i < ctl.ntiles; ++i) {
+    const int s = int(i % S);
+    if (alive && !mbar_wait_bounded(&ctl.bar[s], uint32_t((i / S) & 1))) {
+      alive = false;
+      atomicOr(err, kKernelErrTimeout);
+    }
+    ctl.cur = i;
+    const uint64_t gbase = Tile::base(blockIdx.x + i * gridDim.x);
+    phases(ctl.stages + s * TS, work, coef, gbase, ctl);
+    if constexpr (!DSTORE) {
+#pragma unroll
+      for (uint32_t it = 0; it < PER; ++it)
+        psi[gbase | toff | Tile::off(it * NT)] = work[s_tid ^ swz<Real>(it * NT)];
+    }
+    __syncthreads();
   }
 }
 

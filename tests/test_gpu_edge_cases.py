@@ -87,13 +87,8 @@ def test_every_qubit_targeted_and_extreme_controls(jit):
     ops += [("CX", (0, n - 1), ()), ("CX", (n - 1, 0), ()), ("CCNot", (0, n - 1, n // 2), ()),
             ("CSwap", (n - 1, 0, 1), ()), ("Swap", (0, n - 1), ()), ("XX", (0, n - 1), (0.4,))]
     a = run(ops, n, jit=jit)
-    b = run(ops, n, jit=0) if jit else None
-    if n <= 16:
-        assert np.abs(a - oracle.run_ops(ops, n)).max() <= TOL
-    else:
-        assert abs(np.vdot(a, a).real - 1.0) <= 1e-12
-        if b is not None:
-            assert np.abs(a - b).max() <= TOL
+    assert np.abs(a - oracle.run_ops(ops, n)).max() <= TOL
+    assert abs(np.vdot(a, a).real - 1.0) <= 1e-12
     # The same pattern at 14 qubits against the oracle.
     m = 14
     small = [op for op in circuits.random_all_gates(m, 0, seed=1)]
