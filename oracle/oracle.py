@@ -341,3 +341,34 @@ def expectation_indexed(state: np.ndarray, nq: int, terms: Sequence[tuple[float,
             val = (1j ** ny) * sign_shift * np.dot(sign, prod)
             total += w * float(np.real(val))
     return total
+
+
+# ---------------------------------------------------------------------------
+# Density matrices (noise channels; the reference defines Kraus channels in
+# noise_operations.py but never simulates them).
+# ---------------------------------------------------------------------------
+def _apply_left(rho: np.ndarray, nq: int, m: np.ndarray, targets: Sequence[int]) -> np.ndarray:
+    """m (on `targets`) times rho: m applied to every column of rho."""
+    out = np.array(rho, dtype=np.complex128, order="F")
+    for j in range(out.shape[1]):
+        col = np.ascontiguousarray(out[:, j])
+        apply_matrix(col, nq, m, targets)
+        out[:, j] = col
+    return out
+
+
+def density_evolve(nq: int, steps) -> np.ndarray:
+    """rho after `steps`, each ("unitary", matrix, targets) or ("kraus",
+    [K_i], targets), from |0...0><0...0|: rho -> U rho U^H and
+    rho -> sum_i K_i rho K_i^H, each product formed column by column."""
+    d = 1 << nq
+    rho = np.zeros((d, d), dtype=np.complex128)
+    rho[0, 0] = 1.0
+    for kind, mats, targets in steps:
+        ks = [mats] if kind == "unitary" else mats
+        new = np.zeros_like(rho)
+        for k in ks:
+            kr = _apply_left(rho, nq, k, targets)                   # K rho
+            new += _apply_left(kr.conj().T, nq, k, targets).conj().T  # (K (K rho)^H)^H
+        rho = new
+    return rho

@@ -76,6 +76,7 @@ def _write_jit_sources() -> None:
     out = os.path.join(BUILD, "jit_sources.inc")
     parts = []
     for var, fname in (("kJitPlanSource", "sq_plan.h"), ("kJitSweepSource", "sweep_kernels.cuh"),
+                       ("kJitKernelsSource", "jit_kernels.cuh"),
                        ("kJitReduceSource", "reduce_kernels.cuh"), ("kJitBatchSource", "jit_batch.cuh")):
         text = open(os.path.join(CSRC, fname)).read()
         assert ")SQJIT\"" not in text

@@ -35,6 +35,7 @@
 #include "host_ops.h"
 #include "jit.h"
 #include "jit_batch.cuh"
+#include "jit_kernels.cuh"
 #include "sweep_kernels.cuh"
 
 int sq_detail_fail(int code, const char *msg);  // engine.cu: sets sq_last_error()
@@ -43,7 +44,7 @@ namespace sq {
 
 namespace {
 
-#include "jit_sources.inc"  // kJit{Plan,Sweep,Reduce,Batch}Source (generated by build.py)
+#include "jit_sources.inc"  // kJit{Plan,Sweep,Kernels,Reduce,Batch}Source (generated by build.py)
 
 // --- NVRTC through dlopen -------------------------------------------------
 typedef int nvrtcResult_t;
@@ -166,7 +167,7 @@ Prelude make_prelude(bool batch) {
   p.text = std::string("typedef unsigned char uint8_t;\ntypedef unsigned short uint16_t;\n"
                        "typedef unsigned int uint32_t;\ntypedef unsigned long long uint64_t;\n"
                        "typedef int int32_t;\ntypedef long long int64_t;\n") +
-           kJitPlanSource + "\n" + kJitSweepSource + "\n";
+           kJitPlanSource + "\n" + kJitSweepSource + "\n" + kJitKernelsSource + "\n";
   if (batch) p.text += std::string(kJitReduceSource) + "\n" + kJitBatchSource + "\n";
   p.text += "using namespace sq;\n";
   p.hash = fnv1a(p.text);
@@ -332,7 +333,18 @@ struct JitShape {
   bool smem_coef = false, dload = false, dstore = false;
   int stages = 0;     // > 0: bulk-copy pipeline with this many tiles in flight per CTA
   bool work = false;  // pipeline: some phase passes the tile through the work buffer
+  bool early = false; // direct load of the next tile's first phase before this tile's phases
 };
+
+// Early first-phase loads (jit_sweep_early) for direct-load sweeps: 1 on,
+// 0 off (default); SQ_JIT_EARLY overrides.
+bool jit_early() {
+  static const int env = [] {
+    const char *e = std::getenv("SQ_JIT_EARLY");
+    return e && *e ? std::atoi(e) : 0;
+  }();
+  return env == 1;
+}
 
 // Tiles in flight per CTA of a pipelined (bulk-copy) sweep; 0 turns the
 // pipeline off.  SQ_JIT_STAGES overrides.
@@ -342,8 +354,12 @@ int jit_stages(bool c64) {
     return e && *e ? std::atoi(e) : -1;
   }();
   if (env >= 0 && env <= 4) return env;
+  // Measured on B200 (30-qubit complex128 mix, 128-byte runs): 11.2 ms per
+  // sweep with one stage and 16.4 ms with two, against 7.2 ms for register
+  // loads: one cp.async.bulk per 128-byte run is bound by the copy engine's
+  // request rate.  Off by default.
   (void)c64;
-  return 1;
+  return 0;
 }
 
 // Direct loads (first phase from HBM, no prefetch into a second tile buffer)
@@ -362,11 +378,15 @@ JitShape jit_shape(const PlannedSweep &ps, bool c64) {
   j.dstore = (ps.h.flags & kDirectStore) != 0;
   // The pipeline needs a first phase whose lanes cover the low tile bits (a
   // direct-load sweep) and runs of at least 16 bytes.
+  // Warp 0 issues the copies: tiles of at least 2^9 amplitudes (32 threads).
   const int st = jit_stages(c64);
-  if (st > 0 && (ps.h.flags & kDirectLoad) && ((1u << ps.h.l) * (c64 ? 8u : 16u)) % 16u == 0) {
+  if (st > 0 && (ps.h.flags & kDirectLoad) && ps.h.m >= 9u &&
+      ((1u << ps.h.l) * (c64 ? 8u : 16u)) % 16u == 0) {
     j.stages = st;
     j.dload = false;
     j.work = ps.h.nphases > 1 || !j.dstore;
+  } else if (j.dload && jit_early()) {
+    j.early = true;
   }
   return j;
 }
@@ -390,7 +410,16 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
       << tf(js.dstore) << ", " << js.stages
       << ">(psi, P, err, [&](const C2 *stage, C2 *tile, const C2 *coef, uint64_t gbase, const PipeCtl<" << R
       << ", " << M << ", Tile, " << js.stages << "> &ctl) {\n";
-  else
+  else if (js.early) {
+    // The first phase's register load, shared by the loop's look-ahead.
+    const SweepPhase &p0 = ps.ph[0];
+    s << "  (void)err;\n  using Ph0 = JitPhase<" << R << ", " << M << ", Tile, " << int(p0.reg[0]) << ", "
+      << int(p0.reg[1]) << ", " << int(p0.reg[2]) << ", " << int(p0.reg[3]);
+    for (int t : thread_positions(p0, M, c64, true)) s << ", " << t;
+    s << ">;\n  jit_sweep_early<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dstore)
+      << ">(psi, P, [&](Amps<" << R << "> &A, uint64_t gb) { Ph0::load(A, psi, gb, Ph0::jb(threadIdx.x)); }, "
+      << "[&](const Amps<" << R << "> &A0, C2 *tile, const C2 *coef, uint64_t gbase) {\n";
+  } else
     s << "  (void)err;\n  jit_sweep<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dload)
       << ", " << tf(js.dstore) << ">(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
   const uint32_t last = ps.h.nphases - 1;
@@ -405,6 +434,8 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
     s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << "> A;\n";
     if (from_stage)
       s << "      Ph::gather_lin(A, stage, jb);\n      ctl.release();\n";
+    else if (p == 0 && js.early)
+      s << "      A = A0;\n";
     else if (from_hbm)
       s << "      Ph::load(A, psi, gbase, jb);\n";
     else
@@ -767,7 +798,7 @@ size_t jit_smem(const PlannedSweep &ps, bool c64) {
   const JitShape js = jit_shape(ps, c64);
   const uint32_t nc = js.smem_coef ? (ps.h.ncoef + 1) & ~1u : 0u;
   if (js.stages > 0) return jit_pipe_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.stages, js.work, nc);
-  return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload, nc);
+  return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload || js.early, nc);
 }
 
 int jit_minb(bool c64, uint32_t m) {
@@ -777,9 +808,11 @@ int jit_minb(bool c64, uint32_t m) {
     return e && *e ? std::atoi(e) : 0;
   }();
   if (env > 0 && env <= 16) return env;
+  // Early loads hold a second register set: one CTA fewer per SM.
+  const int e = jit_early() ? 1 : 0;
   // Register budgets of the precompiled sweep instantiations.
-  if (c64) return m == 10 ? 8 : m == 12 ? 2 : 1;
-  return m == 10 ? 6 : m == 11 ? 3 : 1;
+  if (c64) return m == 10 ? 8 - 2 * e : m == 12 ? 2 : 1;
+  return m == 10 ? 6 - 2 * e : m == 11 ? 3 - e : 1;
 }
 
 const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err) {

@@ -146,3 +146,30 @@ def test_batch_adjoint_source_compiles(dtype, n):
     src = capi.jit_batch_adjoint_source(n, adjoint.bind(ops, [0.3, 0.5, 0.7, 0.9]), dtype)
     assert "sq_jit_batch_adjoint" in src
     capi.jit_compile(src)
+
+
+@pytest.mark.parametrize("env", ["SQ_JIT_EARLY=1", "SQ_JIT_STAGES=1"])
+def test_alternative_tile_loops_compile(env):
+    """The early-load and bulk-copy tile loops (off by default) generate
+    sources that compile, for both precisions (a subprocess: the switches
+    are read once per process)."""
+    import os
+    import subprocess
+    import sys
+
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "from snuqs_b200 import capi, circuits\n"
+        "for n, dt in ((26, capi.SQ_C128), (24, capi.SQ_C64)):\n"
+        "    srcs = capi.jit_sources(n, circuits.random_mix(n, 120, seed=7), dt)\n"
+        "    key = %r\n"
+        "    assert any(key in s for s in srcs), key\n"
+        "    for s in srcs[:3]:\n"
+        "        capi.jit_compile(s)\n"
+    ) % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+         "jit_sweep_early<" if "EARLY" in env else "jit_sweep_pipe<")
+    k, v = env.split("=")
+    # Early loads apply to direct-load sweeps; complex64 turns those on with SQ_JIT_DLOAD.
+    r = subprocess.run([sys.executable, "-c", code], env={**os.environ, k: v, "SQ_JIT_DLOAD": "1"},
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
