@@ -85,6 +85,13 @@ struct PlanOptions {
   // of a sweep into the fewest register phases; 0 = take gates first come
   // first served; -1 = 1 for states of >= kSelectMinQubits qubits.
   int select = -1;
+  // Qubit remapping (needs select): a sweep may store its tile with the low
+  // index bits exchanged for tile bits that the next sweep uses most, so the
+  // low bits every tile must hold carry hot qubits; the plan ends with the
+  // original bit order (a last restoring permutation, merged into the last
+  // sweep when its tile holds every moved bit).  Only the JIT-specialised
+  // sweep kernels implement the permuted store.
+  bool remap = false;
 };
 constexpr uint32_t kSelectMinQubits = 18;
 

@@ -30,6 +30,9 @@ struct SweepBuilder {
   std::vector<uint64_t> phase_regs;  // register bits (global) of each phase
   std::vector<uint32_t> phase_first; // first op index of each phase
   uint32_t ncoef = 0, ninner = 0;
+  // Remap: output global bit of the content of every global bit (size n;
+  // empty = the identity).  Only tile bits move.
+  std::vector<int> outmap;
 
   SweepBuilder(uint32_t n_, uint32_t m_, uint32_t l_) : n(n_), m(m_), l(l_) {
     S = (l >= 64) ? ~uint64_t(0) : ((uint64_t(1) << l) - 1);
@@ -183,13 +186,25 @@ PlannedSweep SweepBuilder::finish() const {
   }
   h.nphases = uint32_t(np);
   const uint32_t lowpos = (1u << std::min<uint32_t>(l, 5)) - 1;
+  // Positions stored to the low global bits (where a direct store needs the
+  // lanes): the low positions themselves, or their images under the remap.
+  uint32_t lowpos_out = lowpos;
+  if (!outmap.empty()) {
+    h.flags |= kRemap;
+    lowpos_out = 0;
+    for (uint32_t p = 0; p < m; ++p) {
+      const int in = p < l ? int(p) : int(h.hi[p - l]);
+      h.out[p] = uint8_t(outmap[size_t(in)]);
+      if (h.out[p] < std::min<uint32_t>(l, 5)) lowpos_out |= 1u << p;
+    }
+  }
   auto regmask = [&](const SweepPhase &ph) {
     uint32_t x = 0;
     for (uint32_t b = 0; b < reg_bits; ++b) x |= 1u << ph.reg[b];
     return x;
   };
   if ((regmask(ps.ph.front()) & lowpos) == 0) h.flags |= kDirectLoad;
-  if ((regmask(ps.ph.back()) & lowpos) == 0) h.flags |= kDirectStore;
+  if ((regmask(ps.ph.back()) & lowpos_out) == 0) h.flags |= kDirectStore;
 
   // Ops.
   for (int p = 0; p < np; ++p) {
@@ -366,8 +381,8 @@ uint32_t absorbed(const std::vector<const HostOp *> &rem, size_t head, uint64_t 
 // the sweep absorbs: grown one bit, or one pair of a two-target gate's
 // bits, at a time by the best gain per added bit.
 uint64_t select_tile(const std::vector<const HostOp *> &rem, size_t head, uint32_t n, uint32_t m,
-                     uint32_t l, const PlanOptions &opt, size_t window) {
-  uint64_t S = (uint64_t(1) << l) - 1;
+                     uint64_t start, const PlanOptions &opt, size_t window) {
+  uint64_t S = start;
   uint32_t cur = absorbed(rem, head, S, n, opt, window);
   while (uint32_t(popc64(S)) < m) {
     // Candidate bits: targets of the next gates outside S.
@@ -408,14 +423,15 @@ uint64_t select_tile(const std::vector<const HostOp *> &rem, size_t head, uint32
 // takes every ready op that fits its register set (diagonal ops fit any
 // phase).  Op j depends on an earlier op i when they do not commute.
 // Returns the new order and the first index of each phase.
-// `low`: the tile's lowest bits.  A first phase whose register set avoids
-// them can load from HBM straight into registers, and a last phase that
-// avoids them can store straight back (the lanes then cover contiguous
-// amplitudes), so the first phase prefers ops off those bits and later
-// phases take the ops on them as early as they can.
+// `low`: the tile's lowest bits; `low_out`: the bits stored to the lowest
+// bits (the same unless the sweep remaps).  A first phase whose register set
+// avoids `low` can load from HBM straight into registers, and a last phase
+// that avoids `low_out` can store straight back (the lanes then cover
+// contiguous amplitudes), so the first phase prefers ops off `low` and
+// later phases take the ops on `low_out` as early as they can.
 void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits, uint64_t low,
-                     std::vector<const HostOp *> &order, std::vector<uint64_t> &phase_regs,
-                     std::vector<uint32_t> &phase_first) {
+                     uint64_t low_out, std::vector<const HostOp *> &order,
+                     std::vector<uint64_t> &phase_regs, std::vector<uint32_t> &phase_first) {
   const size_t N = ops.size();
   std::vector<uint64_t> pred(N, 0);
   for (size_t j = 0; j < N; ++j) {
@@ -454,7 +470,7 @@ void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits, 
         if ((placed & bit) || (pred[x] & ~placed)) continue;
         const uint64_t T = ops[x]->target_mask();
         if (popc64(R | T) > int(reg_bits)) continue;
-        const bool on_low = (T & low) != 0;
+        const bool on_low = (T & (first_phase ? low : low_out)) != 0;
         const int key = (on_low == first_phase ? 16 : 0) + popc64(T & ~R);
         if (key < best_key) best_key = key, best = int(x);
       }
@@ -463,6 +479,85 @@ void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits, 
     }
     phase_regs.push_back(R);
   }
+}
+
+// Moves op `op` through a bit permutation: the content of global bit b is
+// now at bit perm[b].
+void relabel(HostOp &op, const std::vector<int> &perm) {
+  for (int &b : op.tbits) b = perm[size_t(b)];
+  uint64_t cm = 0, cv = 0;
+  for (size_t b = 0; b < perm.size(); ++b) {
+    if ((op.cmask >> b) & 1) cm |= uint64_t(1) << perm[b];
+    if ((op.cval >> b) & 1) cv |= uint64_t(1) << perm[b];
+  }
+  op.cmask = cm;
+  op.cval = cv;
+}
+
+// The remap of one sweep with tile bits S, given the ops that follow it:
+// low bits the next sweep would not choose are exchanged for tile bits it
+// would (earliest used first), as long as the bits moved away from home
+// (virt_at[p] != p) still fit one tile with the low bits, so that one
+// permutation sweep can always restore the order.  With no ops left, the
+// remap restores the order itself when every moved bit is in S.  Returns
+// the output map (empty: store in place) and the bits stored to the low bits.
+std::vector<int> choose_remap(const std::vector<const HostOp *> &after, uint64_t S,
+                              const std::vector<int> &virt_at, uint32_t n, uint32_t m, uint32_t l,
+                              const PlanOptions &opt, size_t window, uint64_t &low_out) {
+  const uint64_t low = (uint64_t(1) << l) - 1;
+  low_out = low;
+  uint64_t moved = 0;
+  for (uint32_t p = 0; p < n; ++p)
+    if (virt_at[p] != int(p)) moved |= uint64_t(1) << p;
+  std::vector<int> out(n);
+  for (uint32_t b = 0; b < n; ++b) out[b] = int(b);
+  if (after.empty()) {
+    if (!moved || (moved & ~S)) return {};
+    low_out = 0;
+    for (uint32_t p = 0; p < n; ++p)
+      if ((moved >> p) & 1) out[p] = virt_at[p];
+    for (uint32_t p = 0; p < n; ++p)
+      if (out[p] < int(l)) low_out |= uint64_t(1) << p;
+    return out;
+  }
+  const uint64_t wish = select_tile(after, 0, n, m, 0, opt, window);
+  uint64_t slots = low & ~wish;
+  std::vector<std::pair<size_t, int>> cands;  // (first use, bit)
+  for (uint32_t b = l; b < n; ++b) {
+    if (!((wish >> b) & 1) || !((S >> b) & 1)) continue;
+    size_t first = after.size();
+    for (size_t i = 0; i < after.size() && i < window; ++i)
+      if ((after[i]->target_mask() >> b) & 1) {
+        first = i;
+        break;
+      }
+    cands.emplace_back(first, int(b));
+  }
+  std::sort(cands.begin(), cands.end());
+  std::vector<int> va(virt_at);
+  bool any = false;
+  for (const auto &cb : cands) {
+    if (!slots) break;
+    const int j = __builtin_ctzll(slots), c = cb.second;
+    std::swap(va[size_t(j)], va[size_t(c)]);
+    uint64_t mv = 0;
+    for (uint32_t p = 0; p < n; ++p)
+      if (va[p] != int(p)) mv |= uint64_t(1) << p;
+    if (uint32_t(popc64(mv | low)) > m) {  // the restoration would not fit one tile
+      std::swap(va[size_t(j)], va[size_t(c)]);
+      continue;
+    }
+    out[size_t(j)] = c;
+    out[size_t(c)] = j;
+    low_out = (low_out & ~(uint64_t(1) << j)) | (uint64_t(1) << c);
+    slots &= slots - 1;
+    any = true;
+  }
+  if (!any) {
+    low_out = low;
+    return {};
+  }
+  return out;
 }
 
 }  // namespace
@@ -482,8 +577,14 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
   const bool select =
       opt.reorder && (opt.select == 1 || (opt.select < 0 && n >= kSelectMinQubits && n > m));
 
+  // The ops in the current bit order (a remapping sweep moves the bits of
+  // every op after it); virt_at[p]: the original bit whose content is at p.
+  std::vector<HostOp> work(ops);
+  std::vector<int> virt_at(n);
+  for (uint32_t b = 0; b < n; ++b) virt_at[b] = int(b);
+  const bool remap = opt.remap && select;
   std::vector<const HostOp *> rem;
-  for (const auto &o : ops) rem.push_back(&o);
+  for (const auto &o : work) rem.push_back(&o);
   size_t head = 0;  // rem[head..] still to place
   while (head < rem.size()) {
     const HostOp &first = *rem[head];
@@ -508,7 +609,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
     if (select) {
       // Tile bits chosen up front; gates that fit them (or grow them while
       // there is room) are collected in circuit order, then scheduled.
-      uint64_t S = select_tile(rem, head, n, m, l, opt, kWindow);
+      uint64_t S = select_tile(rem, head, n, m, (uint64_t(1) << l) - 1, opt, kWindow);
       if (absorbed(rem, head, S, n, opt, kWindow) == 0) S = ((uint64_t(1) << l) - 1) | first.target_mask();
       std::vector<const HostOp *> chosen;
       std::vector<size_t> chosen_idx, skipped_idx;
@@ -546,9 +647,22 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
         }
       }
       if (chosen.empty()) throw std::logic_error("planner: empty sweep");
+      const uint64_t low_in = (uint64_t(1) << std::min<uint32_t>(l, 5)) - 1;
+      uint64_t low_out = low_in;
+      if (remap) {
+        std::vector<const HostOp *> after;
+        for (size_t x : skipped_idx) after.push_back(rem[x]);
+        for (size_t x = i; x < rem.size(); ++x) after.push_back(rem[x]);
+        uint64_t lo = 0;
+        sb.outmap = choose_remap(after, S, virt_at, n, m, l, opt, kWindow, lo);
+        if (!sb.outmap.empty()) {
+          low_out = lo;
+          for (uint32_t b = 0; b < n; ++b)  // every bit the remap moves is a tile bit
+            if (sb.outmap[b] != int(b)) S |= uint64_t(1) << b;
+        }
+      }
       std::vector<const HostOp *> order;
-      schedule_phases(chosen, sb.reg_bits, (uint64_t(1) << std::min<uint32_t>(l, 5)) - 1, order,
-                      sb.phase_regs, sb.phase_first);
+      schedule_phases(chosen, sb.reg_bits, low_in, low_out, order, sb.phase_regs, sb.phase_first);
       // More phases than a sweep holds: the ops of the excess phases go back
       // to the queue (every op they precede is among them).
       std::vector<size_t> back_idx;
@@ -578,6 +692,13 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       std::vector<const HostOp *> next;
       for (size_t x : again) next.push_back(rem[x]);
       next.insert(next.end(), rem.begin() + i, rem.end());
+      if (!sb.outmap.empty()) {
+        // Ops after the sweep see its stored bit order.
+        for (const HostOp *op : next) relabel(const_cast<HostOp &>(*op), sb.outmap);
+        std::vector<int> va(n);
+        for (uint32_t b = 0; b < n; ++b) va[size_t(sb.outmap[b])] = virt_at[b];
+        virt_at.swap(va);
+      }
       rem.swap(next);
       head = 0;
       continue;
@@ -609,6 +730,37 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
     next.insert(next.end(), rem.begin() + i, rem.end());
     rem.swap(next);
     head = 0;
+  }
+  if (remap) {
+    // Bits still away from home: one sweep of no gates whose tile holds them
+    // (and the low bits) stores each at home.
+    uint64_t moved = 0;
+    for (uint32_t p = 0; p < n; ++p)
+      if (virt_at[p] != int(p)) moved |= uint64_t(1) << p;
+    if (moved) {
+      SweepBuilder sb(n, m, l);
+      sb.S |= moved;
+      if (uint32_t(popc64(sb.S)) > m) throw std::logic_error("planner: restoration exceeds a tile");
+      sb.outmap.resize(n);
+      for (uint32_t p = 0; p < n; ++p) sb.outmap[p] = virt_at[p];
+      // One phase without gates: its register bits avoid the bits loaded
+      // from and stored to the low bits where the tile allows.
+      uint64_t tile = sb.S;
+      for (uint32_t b = 0; b < n && uint32_t(popc64(tile)) < m; ++b) tile |= uint64_t(1) << b;
+      uint64_t avoid = (uint64_t(1) << std::min<uint32_t>(l, 5)) - 1;
+      for (uint32_t p = 0; p < n; ++p)
+        if (sb.outmap[p] < int(std::min<uint32_t>(l, 5))) avoid |= uint64_t(1) << p;
+      uint64_t regs = 0;
+      for (int b = int(n) - 1; b >= 0 && popc64(regs) < int(opt.reg_bits); --b)
+        if (((tile >> b) & 1) && !((avoid >> b) & 1)) regs |= uint64_t(1) << b;
+      sb.reg_bits = opt.reg_bits;
+      sb.phase_regs.push_back(regs);
+      sb.phase_first.push_back(0);
+      PlannedLaunch pl;
+      pl.is_sweep = true;
+      pl.sweep = sb.finish();
+      out.push_back(std::move(pl));
+    }
   }
   return out;
 }

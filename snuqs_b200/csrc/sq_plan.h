@@ -94,7 +94,11 @@ SQ_HD constexpr int sq_op_code(int kind, int v, int aux) {
          : kind == kSwInnerDense ? 128 + v
                                  : 96 + v;  // kSwDense
 }
-enum SweepFlags : uint32_t { kDirectLoad = 1u, kDirectStore = 2u };
+// kRemap: the sweep stores tile position p to global bit out[p] instead of
+// the bit it was loaded from (a permutation of the tile's bits), so that the
+// following sweeps find their most used qubits on the low, always-resident
+// index bits.
+enum SweepFlags : uint32_t { kDirectLoad = 1u, kDirectStore = 2u, kRemap = 4u };
 
 struct SweepOp {
   uint8_t kind;    // SweepKind
@@ -131,7 +135,8 @@ struct SweepHeader {
   uint32_t flags;    // SweepFlags
   uint64_t num_tiles;
   uint8_t hi[kMaxTileBits];  // global bit of tile position l+i, ascending
-  uint8_t pad[4];
+  uint8_t out[kMaxTileBits]; // kRemap: global bit tile position p is stored to
+  uint8_t pad[8];
 };
 
 template <typename Real>

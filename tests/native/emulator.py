@@ -45,7 +45,7 @@ def run(state, n, gates, tile_bits=12, reorder=True, low_bits=0):
 
 
 def _reorder_code(reorder):
-    return {"select": 2, "noselect": 3}.get(reorder, int(bool(reorder)))
+    return {"select": 2, "noselect": 3, "remap": 4}.get(reorder, int(bool(reorder)))
 
 
 def plan_stats(n, gates, tile_bits=12, reorder=True, low_bits=0):

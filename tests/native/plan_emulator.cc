@@ -195,9 +195,17 @@ void emulate_sweep_n(cplx *psi, cplx *lam, const PlannedSweep &ps, int reg_bits,
         }
       }
     }
+    // A remapping sweep stores tile position p to global bit out[p].
+    auto addr_out = [&](uint32_t j) {
+      if (!(h.flags & kRemap)) return addr(gbase, j);
+      uint64_t a = gbase;
+      for (uint32_t p = 0; p < m; ++p)
+        if ((j >> p) & 1) a |= uint64_t(1) << h.out[p];
+      return a;
+    };
     for (uint32_t j = 0; j < (1u << m); ++j) {
-      psi[addr(gbase, j)] = tile[j];
-      if (lam) lam[addr(gbase, j)] = ltile[j];
+      psi[addr_out(j)] = tile[j];
+      if (lam) lam[addr_out(j)] = ltile[j];
     }
   }
 }
@@ -268,8 +276,10 @@ int emu_run(double *state, int n, int nops, const int *k, const int *qoff, const
     PlanOptions opt;
     opt.tile_bits = uint32_t(tile_bits);
     opt.reorder = reorder != 0;
-    // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection
-    opt.select = reorder == 2 ? 1 : reorder == 3 ? 0 : -1;
+    // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection,
+    // 4 on + selection + qubit remapping
+    opt.select = (reorder == 2 || reorder == 4) ? 1 : reorder == 3 ? 0 : -1;
+    opt.remap = reorder == 4;
     opt.low_bits = uint32_t(low_bits);
     auto plan = plan_sweeps(ops, uint32_t(n), opt);
     int sweeps = 0, unfused = 0;
@@ -319,8 +329,10 @@ int emu_plan_stats(int n, int nops, const int *k, const int *qoff, const int *qu
     PlanOptions opt;
     opt.tile_bits = uint32_t(tile_bits);
     opt.reorder = reorder != 0;
-    // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection
-    opt.select = reorder == 2 ? 1 : reorder == 3 ? 0 : -1;
+    // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection,
+    // 4 on + selection + qubit remapping
+    opt.select = (reorder == 2 || reorder == 4) ? 1 : reorder == 3 ? 0 : -1;
+    opt.remap = reorder == 4;
     opt.low_bits = uint32_t(low_bits);
     auto plan = plan_sweeps(ops, uint32_t(n), opt);
     for (int i = 0; i < 12; ++i) out[i] = 0;
