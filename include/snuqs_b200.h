@@ -69,10 +69,14 @@ typedef enum {
   SQ_OPT_TIMING = 3,    /* 1: record a CUDA event pair around every fused-sweep launch */
   SQ_OPT_JIT = 4,       /* -1 (default): JIT-specialised sweep kernels for states of >= 20
                            qubits when NVRTC is present; 1: always; 0: never */
-  SQ_OPT_LOW_BITS = 5   /* contiguous low index bits in every tile (each global access
+  SQ_OPT_LOW_BITS = 5,  /* contiguous low index bits in every tile (each global access
                            covers runs of 2^value amplitudes); 0 (default): 3 for
                            complex128, 4 for complex64 (128-byte runs) when the state
                            spans several tiles; ignored unless value + 4 <= tile bits */
+  SQ_OPT_REMAP = 6      /* 1 (default): JIT-specialised sweeps may store their tiles with
+                           index bits permuted so that the next sweeps find their most
+                           used qubits on the low bits every tile holds; every flush ends
+                           in the original order.  0: never */
 } sq_option;
 
 /* ---- library / device ------------------------------------------------ */

@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(_HERE, "libsnuqs_b200.so")
 
 SQ_OK, SQ_ERR_INVALID, SQ_ERR_CUDA, SQ_ERR_OOM, SQ_ERR_UNSUPPORTED, SQ_ERR_TIMEOUT = range(6)
 SQ_C128, SQ_C64 = 0, 1
-SQ_OPT_FUSION, SQ_OPT_TILE_BITS, SQ_OPT_REORDER, SQ_OPT_TIMING, SQ_OPT_JIT, SQ_OPT_LOW_BITS = range(6)
+(SQ_OPT_FUSION, SQ_OPT_TILE_BITS, SQ_OPT_REORDER, SQ_OPT_TIMING, SQ_OPT_JIT, SQ_OPT_LOW_BITS,
+ SQ_OPT_REMAP) = range(7)
 
 GATE_NAMES = [
     "Identity", "Hadamard", "PauliX", "PauliY", "PauliZ", "CX", "CY", "CZ", "S", "Si", "T",

@@ -70,6 +70,16 @@ struct PendingOp {
   std::vector<uint8_t> cvals;
 };
 
+// Qubit remapping in fused sweeps (SQ_OPT_REMAP), on by default; SQ_REMAP=0
+// turns the default off.
+static int default_remap() {
+  static const int v = [] {
+    const char *e = std::getenv("SQ_REMAP");
+    return e && *e ? (e[0] == '0' ? 0 : 1) : 1;
+  }();
+  return v;
+}
+
 struct sq_state {
   uint32_t n = 0;
   int dtype = SQ_C128;
@@ -86,6 +96,7 @@ struct sq_state {
   int timing = 0;
   uint32_t low_bits = 0;  // 0: automatic
   int jit = -1;  // -1: automatic (states of >= kJitMinQubits qubits), 0: off, 1: on
+  int remap = default_remap();  // SQ_OPT_REMAP
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sweep_events;
   // Device word a sweep kernel sets when one of its bounded waits gives up
   // (sq::kKernelErrTimeout); read and cleared by sq_state_check.
@@ -282,6 +293,7 @@ static int launch_sweep(sq_state *s, const sq::PlannedSweep &ps, cudaStream_t st
     sq::jit_note_launch(fn != nullptr);
   }
   if (!fn) {
+    if (ps.h.flags & sq::kRemap) return fail(SQ_ERR_INVALID, "internal: remapping sweep without its JIT kernel");
     fn = sweep_fn<Real>(m);
     if (!fn) return fail(SQ_ERR_INVALID, "internal: no sweep kernel for %u tile bits", m);
     SQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
@@ -447,8 +459,8 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
     return SQ_OK;
   }
   std::vector<sq::PlannedLaunch> plan;
+  sq::PlanOptions opt;
   try {
-    sq::PlanOptions opt;
     opt.tile_bits = pick_tile_bits(s->dtype, n, s->tile_bits);
     if (opt.tile_bits < uint32_t(sq::kRegBits)) return fail(SQ_ERR_INVALID, "internal: no tile size");
     opt.reorder = s->reorder != 0;
@@ -460,6 +472,8 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
       opt.low_bits = s->low_bits;
     else
       opt.low_bits = sq::auto_low_bits(c64, n, opt.tile_bits);
+    // Remapping sweeps exist only as JIT-specialised kernels.
+    opt.remap = s->remap && use_jit(s);
     plan = sq::plan_sweeps(ops, n, opt);
   } catch (const std::exception &e) {
     return fail(SQ_ERR_INVALID, "planner: %s", e.what());
@@ -469,6 +483,25 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
     for (const auto &pl : plan)
       if (pl.is_sweep) sweeps.push_back(&pl.sweep);
     sq::jit_prepare(sweeps, c64);
+    // A remapping sweep whose kernel did not compile cannot fall back to the
+    // generic kernel: plan again without remapping.
+    bool ready = true;
+    for (const auto *ps : sweeps) {
+      std::string err;
+      if ((ps->h.flags & sq::kRemap) && !sq::jit_sweep_kernel(*ps, c64, err)) ready = false;
+    }
+    if (!ready) {
+      try {
+        opt.remap = false;
+        plan = sq::plan_sweeps(ops, n, opt);
+      } catch (const std::exception &e) {
+        return fail(SQ_ERR_INVALID, "planner: %s", e.what());
+      }
+      sweeps.clear();
+      for (const auto &pl : plan)
+        if (pl.is_sweep) sweeps.push_back(&pl.sweep);
+      sq::jit_prepare(sweeps, c64);
+    }
   }
   for (const auto &pl : plan) {
     if (pl.is_sweep) {
@@ -710,6 +743,7 @@ int sq_set_option(sq_state *s, int option, int64_t value) {
       return SQ_OK;
     case SQ_OPT_REORDER: s->reorder = value != 0; return SQ_OK;
     case SQ_OPT_TIMING: s->timing = value != 0; return SQ_OK;
+    case SQ_OPT_REMAP: s->remap = value != 0; return SQ_OK;
     case SQ_OPT_LOW_BITS:
       if (value < 0 || value > 8) return fail(SQ_ERR_INVALID, "SQ_OPT_LOW_BITS takes 0..8");
       s->low_bits = uint32_t(value);

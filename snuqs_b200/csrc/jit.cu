@@ -283,7 +283,7 @@ void jit_note_launch(bool jit) { (jit ? g_launches : g_fallbacks)++; }
 // stores straight to HBM keeps all thread bits ascending (the lanes then
 // cover contiguous amplitudes).
 std::vector<int> thread_positions(const SweepPhase &ph, int m, bool c64, bool direct_store,
-                                  int nreg = kRegBits) {
+                                  int nreg = kRegBits, const uint8_t *outbits = nullptr) {
   const int W = c64 ? Swz<float>::W : Swz<double>::W;
   const uint8_t *img = c64 ? Swz<float>::kImage : Swz<double>::kImage;
   uint32_t regs = 0;
@@ -291,7 +291,12 @@ std::vector<int> thread_positions(const SweepPhase &ph, int m, bool c64, bool di
   std::vector<int> nonreg;
   for (int p = 0; p < m; ++p)
     if (!((regs >> p) & 1)) nonreg.push_back(p);
-  if (direct_store) return nonreg;
+  if (direct_store) {
+    // Lanes on the positions stored to the lowest global bits first.
+    if (outbits)
+      std::stable_sort(nonreg.begin(), nonreg.end(), [&](int a, int b) { return outbits[a] < outbits[b]; });
+    return nonreg;
+  }
   std::vector<int> lanes;
   int basis[8] = {0};
   for (int p : nonreg) {
@@ -336,12 +341,14 @@ struct JitShape {
   bool early = false; // direct load of the next tile's first phase before this tile's phases
 };
 
-// Early first-phase loads (jit_sweep_early) for direct-load sweeps: 1 on,
-// 0 off (default); SQ_JIT_EARLY overrides.
+// Early first-phase loads (jit_sweep_early) for direct-load sweeps, on by
+// default: measured on B200 at 30 qubits, 6.84 vs 7.11 ms per complex128
+// sweep and 3.59 vs 3.81 ms per complex64 sweep (with direct loads, which
+// alone measured slower for complex64).  SQ_JIT_EARLY=0 turns them off.
 bool jit_early() {
   static const int env = [] {
     const char *e = std::getenv("SQ_JIT_EARLY");
-    return e && *e ? std::atoi(e) : 0;
+    return e && *e ? std::atoi(e) : 1;
   }();
   return env == 1;
 }
@@ -364,18 +371,21 @@ int jit_stages(bool c64) {
 
 // Direct loads (first phase from HBM, no prefetch into a second tile buffer)
 // measured faster on B200 for complex128 (7.10 vs 7.38 ms per 30-qubit sweep)
-// and slightly slower for complex64 (3.86 vs 3.76 ms); SQ_JIT_DLOAD=0/1
-// overrides the choice for both precisions.
+// and, without early loads, slightly slower for complex64 (3.86 vs 3.76 ms);
+// SQ_JIT_DLOAD=0/1 overrides the choice for both precisions.
 JitShape jit_shape(const PlannedSweep &ps, bool c64) {
   static const int dload_env = [] {
     const char *e = std::getenv("SQ_JIT_DLOAD");
     return e && *e ? (e[0] == '0' ? 0 : 1) : -1;
   }();
-  const bool dload_on = dload_env < 0 ? !c64 : dload_env == 1;
+  const bool dload_on = dload_env < 0 ? (!c64 || jit_early()) : dload_env == 1;
   JitShape j;
   for (const SweepOp &op : ps.op) j.smem_coef |= lane_indexed(op);
   j.dload = dload_on && (ps.h.flags & kDirectLoad);
   j.dstore = (ps.h.flags & kDirectStore) != 0;
+  // A one-phase remapping sweep cannot place its lanes for both a coalesced
+  // load and a coalesced permuted store: it stores through shared memory.
+  if ((ps.h.flags & kRemap) && ps.h.nphases == 1 && (ps.h.flags & kDirectLoad)) j.dstore = false;
   // The pipeline needs a first phase whose lanes cover the low tile bits (a
   // direct-load sweep) and runs of at least 16 bytes.
   // Warp 0 issues the copies: tiles of at least 2^9 amplitudes (32 threads).
@@ -403,12 +413,20 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
   s << "  using Tile = JitTile<" << M << ", " << ps.h.l;
   for (uint32_t i = 0; i < ps.h.m - ps.h.l; ++i) s << ", " << int(ps.h.hi[i]);
   s << ">;\n";
+  const bool remap = (ps.h.flags & kRemap) != 0;
+  if (remap) {
+    s << "  using TileOut = JitTileMap<" << M;
+    for (int p = 0; p < M; ++p) s << ", " << int(ps.h.out[p]);
+    s << ">;\n";
+  } else {
+    s << "  using TileOut = Tile;\n";
+  }
   auto tf = [](bool b) { return b ? "true" : "false"; };
   const bool pipe = js.stages > 0;
   if (pipe)
     s << "  jit_sweep_pipe<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.work) << ", "
       << tf(js.dstore) << ", " << js.stages
-      << ">(psi, P, err, [&](const C2 *stage, C2 *tile, const C2 *coef, uint64_t gbase, const PipeCtl<" << R
+      << ", TileOut>(psi, P, err, [&](const C2 *stage, C2 *tile, const C2 *coef, uint64_t gbase, const PipeCtl<" << R
       << ", " << M << ", Tile, " << js.stages << "> &ctl) {\n";
   else if (js.early) {
     // The first phase's register load, shared by the loop's look-ahead.
@@ -417,11 +435,11 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
       << int(p0.reg[1]) << ", " << int(p0.reg[2]) << ", " << int(p0.reg[3]);
     for (int t : thread_positions(p0, M, c64, true)) s << ", " << t;
     s << ">;\n  jit_sweep_early<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dstore)
-      << ">(psi, P, [&](Amps<" << R << "> &A, uint64_t gb) { Ph0::load(A, psi, gb, Ph0::jb(threadIdx.x)); }, "
+      << ", TileOut>(psi, P, [&](Amps<" << R << "> &A, uint64_t gb) { Ph0::load(A, psi, gb, Ph0::jb(threadIdx.x)); }, "
       << "[&](const Amps<" << R << "> &A0, C2 *tile, const C2 *coef, uint64_t gbase) {\n";
   } else
     s << "  (void)err;\n  jit_sweep<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dload)
-      << ", " << tf(js.dstore) << ">(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
+      << ", " << tf(js.dstore) << ", TileOut>(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
   const uint32_t last = ps.h.nphases - 1;
   for (uint32_t p = 0; p < ps.h.nphases; ++p) {
     const SweepPhase &ph = ps.ph[p];
@@ -429,7 +447,9 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
     const bool from_hbm = p == 0 && js.dload, to_hbm = p == last && js.dstore;
     s << "    {\n      using Ph = JitPhase<" << R << ", " << M << ", Tile, " << int(ph.reg[0]) << ", "
       << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]);
-    for (int t : thread_positions(ph, M, c64, from_hbm || from_stage || to_hbm)) s << ", " << t;
+    const auto tpos = thread_positions(ph, M, c64, from_hbm || from_stage || to_hbm, kRegBits,
+                                       to_hbm && remap && !from_hbm && !from_stage ? ps.h.out : nullptr);
+    for (int t : tpos) s << ", " << t;
     s << ">;\n";
     s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << "> A;\n";
     if (from_stage)
@@ -473,7 +493,12 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
           << ");\n";
       }
     }
-    if (p == last && js.dstore) {
+    if (p == last && js.dstore && remap) {
+      s << "      using PhO = JitPhase<" << R << ", " << M << ", TileOut, " << int(ph.reg[0]) << ", "
+        << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]);
+      for (int t : tpos) s << ", " << t;
+      s << ">;\n      PhO::store(A, psi, gbase, jb);\n    }\n";
+    } else if (p == last && js.dstore) {
       s << "      Ph::store(A, psi, gbase, jb);\n    }\n";
     } else {
       s << "      Ph::scatter(A, tile, jb);\n      __syncthreads();\n    }\n";
@@ -873,6 +898,9 @@ extern "C" int sq_jit_source(uint32_t num_qubits, int dtype, const sq_circuit_op
     }
     opt.max_dense_k = c64 ? 4 : 3;
     opt.low_bits = sq::auto_low_bits(c64, num_qubits, opt.tile_bits);
+    // As a state of the engine plans with its default options (remapping on).
+    const char *re = std::getenv("SQ_REMAP");
+    opt.remap = !(re && re[0] == '0');
     plan = sq::plan_sweeps(ap.forward, num_qubits, opt);
   } catch (const std::exception &e) {
     return sq_detail_fail(SQ_ERR_INVALID, e.what());

@@ -51,6 +51,44 @@ struct JitTile {
     ((x = ((x >> HI) << (HI + 1)) | (x & ((uint64_t(1) << HI) - 1))), ...);
     return x;
   }
+  // Output order of the copy-out: tile positions are already ascending by
+  // global bit, so output index o is tile element o.
+  __host__ __device__ static constexpr uint32_t src(uint32_t o) { return o; }
+  __host__ __device__ static constexpr uint64_t soff(uint32_t o) { return off(o); }
+};
+
+// Output geometry of a remapping sweep: tile position p is stored to global
+// bit OUT[p] (a permutation of the tile's bits; the tile base is unchanged).
+// off(j): global offset of tile element j on the way out.  For the copy-out,
+// output index o numbers the outputs in ascending global-bit order (bit i of
+// o <-> the i-th lowest output bit): src(o) is the tile element stored there
+// and soff(o) its offset.  All three are linear over disjoint bits.
+template <int M, int... OUT>
+struct JitTileMap {
+  static_assert(sizeof...(OUT) == M, "one output bit per tile position");
+  __host__ __device__ static constexpr uint64_t off(uint32_t j) {
+    uint64_t x = 0;
+    int p = 0;
+    ((x |= uint64_t((j >> p++) & 1u) << OUT), ...);
+    return x;
+  }
+  // Tile position holding the i-th lowest output bit.
+  __host__ __device__ static constexpr int sorted_pos(int i) {
+    const int out[M] = {OUT...};
+    for (int p = 0; p < M; ++p) {
+      int below = 0;
+      for (int q = 0; q < M; ++q) below += out[q] < out[p] ? 1 : 0;
+      if (below == i) return p;
+    }
+    return 0;
+  }
+  __host__ __device__ static constexpr uint32_t src(uint32_t o) {
+    uint32_t x = 0;
+    for (int i = 0; i < M; ++i)
+      if ((o >> i) & 1u) x |= 1u << sorted_pos(i);
+    return x;
+  }
+  __host__ __device__ static constexpr uint64_t soff(uint32_t o) { return off(src(o)); }
 };
 
 // One phase: register bits R0..R3 (tile positions, ascending), thread bit i
@@ -155,7 +193,7 @@ __host__ __device__ constexpr size_t jit_smem_bytes(int m, size_t amp_bytes, boo
 // phases run, so every CTA keeps one tile's loads in flight while it computes
 // (at the price of a second register set).  phases(A0, tile, coef, gbase)
 // runs every phase of one tile starting from the first phase's registers A0.
-template <typename Real, int M, class Tile, bool SMEM_COEF, bool DSTORE, class Load0, class Phases>
+template <typename Real, int M, class Tile, bool SMEM_COEF, bool DSTORE, class Out, class Load0, class Phases>
 __device__ __forceinline__ void jit_sweep_early(typename Vec2<Real>::T *__restrict__ psi,
                                                 const SweepParams<Real> &P, Load0 load0, Phases phases) {
   using C2 = typename Vec2<Real>::T;
@@ -177,6 +215,8 @@ __device__ __forceinline__ void jit_sweep_early(typename Vec2<Real>::T *__restri
     __syncthreads();
   }
   const uint32_t s_tid = swz<Real>(tid);
+  const uint32_t o_tid = swz<Real>(Out::src(tid));  // copy-out: output index tid
+  const uint64_t ooff = Out::soff(tid);
   const uint64_t toff = Tile::off(tid);
   Amps<Real> next;
   if (blockIdx.x < h.num_tiles) load0(next, Tile::base(blockIdx.x));
@@ -189,13 +229,13 @@ __device__ __forceinline__ void jit_sweep_early(typename Vec2<Real>::T *__restri
     if constexpr (!DSTORE) {
 #pragma unroll
       for (uint32_t it = 0; it < PER; ++it)
-        psi[gbase | toff | Tile::off(it * NT)] = tile[s_tid ^ swz<Real>(it * NT)];
+        psi[gbase | ooff | Out::soff(it * NT)] = tile[o_tid ^ swz<Real>(Out::src(it * NT))];
     }
     __syncthreads();
   }
 }
 
-template <typename Real, int M, class Tile, bool SMEM_COEF, bool DLOAD, bool DSTORE, class Phases>
+template <typename Real, int M, class Tile, bool SMEM_COEF, bool DLOAD, bool DSTORE, class Out, class Phases>
 __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ psi,
                                           const SweepParams<Real> &P, Phases phases) {
   using C2 = typename Vec2<Real>::T;
@@ -218,6 +258,8 @@ __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ p
   }
   // Element j = it * NT + tid of a tile: global offset off(it * NT) | off(tid).
   const uint32_t s_tid = swz<Real>(tid);
+  const uint32_t o_tid = swz<Real>(Out::src(tid));  // copy-out: output index tid
+  const uint64_t ooff = Out::soff(tid);
   const uint64_t toff = Tile::off(tid);
   if constexpr (DLOAD) {
     for (uint64_t t = blockIdx.x; t < h.num_tiles; t += gridDim.x) {
@@ -226,7 +268,7 @@ __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ p
       if constexpr (!DSTORE) {
 #pragma unroll
         for (uint32_t it = 0; it < PER; ++it)
-          psi[gbase | toff | Tile::off(it * NT)] = bufs[s_tid ^ swz<Real>(it * NT)];
+          psi[gbase | ooff | Out::soff(it * NT)] = bufs[o_tid ^ swz<Real>(Out::src(it * NT))];
       }
       __syncthreads();
     }
@@ -252,7 +294,7 @@ __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ p
       if constexpr (!DSTORE) {
 #pragma unroll
         for (uint32_t it = 0; it < PER; ++it)
-          psi[gbase | toff | Tile::off(it * NT)] = tile[s_tid ^ swz<Real>(it * NT)];
+          psi[gbase | ooff | Out::soff(it * NT)] = tile[o_tid ^ swz<Real>(Out::src(it * NT))];
       }
       __syncthreads();
       cur ^= 1;
@@ -384,7 +426,8 @@ struct PipeCtl {
 //  WORK:      some phase passes the tile through the work buffer;
 //  DSTORE:    the last phase stores to HBM itself (no copy-out);
 //  S:         stages (tiles in flight per CTA).
-template <typename Real, int M, class Tile, bool SMEM_COEF, bool WORK, bool DSTORE, int S, class Phases>
+template <typename Real, int M, class Tile, bool SMEM_COEF, bool WORK, bool DSTORE, int S, class Out,
+          class Phases>
 __device__ __forceinline__ void jit_sweep_pipe(typename Vec2<Real>::T *__restrict__ psi,
                                                const SweepParams<Real> &P, uint32_t *__restrict__ err,
                                                Phases phases) {
@@ -392,7 +435,7 @@ __device__ __forceinline__ void jit_sweep_pipe(typename Vec2<Real>::T *__restric
   constexpr int NT = 1 << (M - kRegBits);
   constexpr uint32_t TS = 1u << M;
   constexpr uint32_t PER = TS / NT;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const SweepHeader &h = P.h;
   PipeCtl<Real, M, Tile, S> ctl;
   ctl.psi = psi;
@@ -421,6 +464,8 @@ __device__ __forceinline__ void jit_sweep_pipe(typename Vec2<Real>::T *__restric
   if (ctl.warp == 0)
     for (uint64_t i = 0; i < uint64_t(S) && i < ctl.ntiles; ++i) ctl.issue(i);
   const uint32_t s_tid = swz<Real>(tid);
+  const uint32_t o_tid = swz<Real>(Out::src(tid));  // copy-out: output index tid
+  const uint64_t ooff = Out::soff(tid);
   const uint64_t toff = Tile::off(tid);
   bool alive = true;
   for (uint64_t i = 0; i < ctl.ntiles; ++i) {

@@ -494,66 +494,93 @@ void relabel(HostOp &op, const std::vector<int> &perm) {
   op.cval = cv;
 }
 
-// The remap of one sweep with tile bits S, given the ops that follow it:
-// low bits the next sweep would not choose are exchanged for tile bits it
-// would (earliest used first), as long as the bits moved away from home
-// (virt_at[p] != p) still fit one tile with the low bits, so that one
-// permutation sweep can always restore the order.  With no ops left, the
-// remap restores the order itself when every moved bit is in S.  Returns
-// the output map (empty: store in place) and the bits stored to the low bits.
+// The remap of one sweep with tile bits S, given the ops that follow it: a
+// permutation of the tile's bits applied on the way out.  Low bits the next
+// sweep would not choose get tile bits it would (earliest used first); every
+// other bit away from home (virt_at[p] != p) goes home when its home is in
+// the tile and free; the rest stay or fill the remaining places.  The bits
+// away from home must still fit one tile with the low bits, so that one
+// permutation sweep can always restore the order.  With no ops left, only
+// homing happens.  Returns the output map (content of bit b goes to bit
+// out[b]; empty: store in place) and the bits stored to the low bits.
 std::vector<int> choose_remap(const std::vector<const HostOp *> &after, uint64_t S,
                               const std::vector<int> &virt_at, uint32_t n, uint32_t m, uint32_t l,
                               const PlanOptions &opt, size_t window, uint64_t &low_out) {
   const uint64_t low = (uint64_t(1) << l) - 1;
-  low_out = low;
-  uint64_t moved = 0;
-  for (uint32_t p = 0; p < n; ++p)
-    if (virt_at[p] != int(p)) moved |= uint64_t(1) << p;
-  std::vector<int> out(n);
-  for (uint32_t b = 0; b < n; ++b) out[b] = int(b);
-  if (after.empty()) {
-    if (!moved || (moved & ~S)) return {};
-    low_out = 0;
-    for (uint32_t p = 0; p < n; ++p)
-      if ((moved >> p) & 1) out[p] = virt_at[p];
-    for (uint32_t p = 0; p < n; ++p)
-      if (out[p] < int(l)) low_out |= uint64_t(1) << p;
-    return out;
-  }
-  const uint64_t wish = select_tile(after, 0, n, m, 0, opt, window);
-  uint64_t slots = low & ~wish;
-  std::vector<std::pair<size_t, int>> cands;  // (first use, bit)
-  for (uint32_t b = l; b < n; ++b) {
-    if (!((wish >> b) & 1) || !((S >> b) & 1)) continue;
-    size_t first = after.size();
-    for (size_t i = 0; i < after.size() && i < window; ++i)
-      if ((after[i]->target_mask() >> b) & 1) {
-        first = i;
-        break;
-      }
-    cands.emplace_back(first, int(b));
-  }
-  std::sort(cands.begin(), cands.end());
-  std::vector<int> va(virt_at);
-  bool any = false;
-  for (const auto &cb : cands) {
-    if (!slots) break;
-    const int j = __builtin_ctzll(slots), c = cb.second;
-    std::swap(va[size_t(j)], va[size_t(c)]);
-    uint64_t mv = 0;
-    for (uint32_t p = 0; p < n; ++p)
-      if (va[p] != int(p)) mv |= uint64_t(1) << p;
-    if (uint32_t(popc64(mv | low)) > m) {  // the restoration would not fit one tile
-      std::swap(va[size_t(j)], va[size_t(c)]);
-      continue;
+  S |= low;
+  std::vector<std::pair<int, int>> swaps;  // (low slot, tile bit moved there)
+  if (!after.empty()) {
+    const uint64_t wish = select_tile(after, 0, n, m, 0, opt, window);
+    uint64_t slots = low & ~wish;
+    std::vector<std::pair<size_t, int>> cands;  // (first use, bit)
+    for (uint32_t b = l; b < n; ++b) {
+      if (!((wish >> b) & 1) || !((S >> b) & 1)) continue;
+      size_t first = after.size();
+      for (size_t i = 0; i < after.size() && i < window; ++i)
+        if ((after[i]->target_mask() >> b) & 1) {
+          first = i;
+          break;
+        }
+      cands.emplace_back(first, int(b));
     }
-    out[size_t(j)] = c;
-    out[size_t(c)] = j;
-    low_out = (low_out & ~(uint64_t(1) << j)) | (uint64_t(1) << c);
-    slots &= slots - 1;
-    any = true;
+    std::sort(cands.begin(), cands.end());
+    for (const auto &cb : cands) {
+      if (!slots) break;
+      swaps.emplace_back(__builtin_ctzll(slots), cb.second);
+      slots &= slots - 1;
+    }
   }
-  if (!any) {
+  // Builds the permutation for the first `k` swaps; returns the bits away
+  // from home afterwards.
+  std::vector<int> out;
+  auto build = [&](size_t k) {
+    out.assign(n, -1);
+    uint64_t taken = 0;
+    for (size_t i = 0; i < k; ++i) {
+      out[size_t(swaps[i].second)] = swaps[i].first;
+      taken |= uint64_t(1) << swaps[i].first;
+    }
+    // Homing.
+    for (uint32_t p = 0; p < n; ++p) {
+      if (!((S >> p) & 1) || out[p] >= 0) continue;
+      const int v = virt_at[p];
+      if (v != int(p) && ((S >> v) & 1) && !((taken >> v) & 1)) {
+        out[p] = v;
+        taken |= uint64_t(1) << v;
+      }
+    }
+    // The rest: in place when free, else any free place in the tile.
+    std::vector<int> free_pos;
+    for (uint32_t p = 0; p < n; ++p) {
+      if (!((S >> p) & 1) || out[p] >= 0) continue;
+      if (!((taken >> p) & 1)) {
+        out[p] = int(p);
+        taken |= uint64_t(1) << p;
+      }
+    }
+    for (uint32_t p = 0; p < n; ++p)
+      if (((S >> p) & 1) && !((taken >> p) & 1)) free_pos.push_back(int(p));
+    size_t f = 0;
+    for (uint32_t p = 0; p < n; ++p) {
+      if (!((S >> p) & 1)) out[p] = int(p);
+      else if (out[p] < 0) out[p] = free_pos[f++];
+    }
+    uint64_t moved = 0;
+    for (uint32_t p = 0; p < n; ++p) {
+      // After the store, bit out[p] holds virtual bit virt_at[p].
+      if (virt_at[p] != out[p]) moved |= uint64_t(1) << out[p];
+    }
+    return moved;
+  };
+  size_t k = swaps.size();
+  uint64_t moved = build(k);
+  while (k > 0 && uint32_t(popc64(moved | low)) > m) moved = build(--k);
+  bool identity = true;
+  for (uint32_t p = 0; p < n; ++p) identity = identity && out[p] == int(p);
+  low_out = 0;
+  for (uint32_t p = 0; p < n; ++p)
+    if (out[p] < int(l)) low_out |= uint64_t(1) << p;
+  if (identity) {
     low_out = low;
     return {};
   }

@@ -187,3 +187,27 @@ def test_round_trip_33_qubits_complex64_400_gates():
     if not device_ram_ok(33, 8, 1.05):
         pytest.skip("needs 68 GiB free device memory")
     _round_trip(33, capi.SQ_C64, 400, 1e-4, 1e-3)
+
+
+@pytest.mark.parametrize("low_bits", [0, 4, 5])
+def test_remapping_sweeps_against_reference(low_bits):
+    """Qubit remapping on and off (SQ_OPT_REMAP), with the default and with
+    longer contiguous runs: the same state as the reference CPU path, and
+    the remapping plan uses fewer sweeps or as many."""
+    n = 24
+    for ops in (circuits.random_mix(n, 400, seed=24), circuits.quantum_volume(n, 12, seed=24)):
+        ref = reference(ops, n)
+        launches = {}
+        for remap in (1, 0):
+            st = capi.State(n)
+            st.set_option(capi.SQ_OPT_REMAP, remap)
+            if low_bits:
+                st.set_option(capi.SQ_OPT_LOW_BITS, low_bits)
+            st.init_basis(0)
+            st.apply_ops(ops)
+            st.flush()
+            launches[remap] = st.launches()
+            psi = st.to_host()
+            st.close()
+            assert max_abs_diff(psi, ref) <= TOL128, (low_bits, remap)
+        assert launches[1] <= launches[0] + 1

@@ -44,14 +44,16 @@ def test_sources_cover_every_op_kind():
                 seen.add("tile_control")
             if "Ph::store(" in body:
                 seen.add("direct_store")
-            if "Ph::load(" in body:
+            if "Ph::load(" in body or "Ph0::load(" in body:
                 seen.add("direct_load")
+            if "JitTileMap<" in body:
+                seen.add("remapping_store")
             if "Ph::gather_lin(" in body and "jit_sweep_pipe<" in body:
                 seen.add("bulk_copy_pipeline")
     # Direct-load sweeps take their tiles through the bulk-copy pipeline by
     # default (SQ_JIT_STAGES=0 brings back the register loads).
     first = "bulk_copy_pipeline" if "bulk_copy_pipeline" in seen else "direct_load"
-    assert seen >= set(OP_ROUTINES) | {"global_control", "direct_store", first}, seen
+    assert seen >= set(OP_ROUTINES) | {"global_control", "direct_store", first, "remapping_store"}, seen
 
 
 def test_sources_depend_on_structure_not_angles():
@@ -96,15 +98,21 @@ def test_lane_placement_is_a_permutation_and_conflict_free(dtype):
     phases = conflict_free = 0
     for src in capi.jit_sources(n, circuits.random_mix(n, 200, seed=13), dtype):
         body = src[src.rindex("sq_jit_sweep"):]
+        # Direct-store phases of remapping sweeps place their lanes for a
+        # coalesced permuted store (output order), not for the gather.
+        permuted = set(re.findall(r"JitPhase<\w+, \d+, TileOut, ([\d, ]+)>", body))
         for mm, args in re.findall(r"JitPhase<\w+, (\d+), Tile, ([\d, ]+)>", body):
             vals = [int(x) for x in args.split(",")]
             m, regs, threads = int(mm), vals[:4], vals[4:]
             assert sorted(regs + threads) == list(range(m))
+            if args in permuted:
+                continue
             phases += 1
             conflict_free += _rank([img[p] for p in threads[:W]]) == W
     assert phases > 0
-    # Every phase except the direct-store ones (ascending lanes from tile
-    # position 0, also conflict-free) gets independent lane images.
+    # Every other phase gets independent lane images (direct-load and
+    # direct-store phases have ascending lanes from tile position 0, also
+    # conflict-free).
     assert conflict_free == phases
 
 

@@ -108,3 +108,24 @@ def test_diagonal_and_identity_gates_fold():
     psi, sweeps, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops))
     assert np.abs(psi - ref).max() <= 1e-12
     assert sweeps == 1
+
+
+@pytest.mark.parametrize("n,tb,lb", [(14, 9, 3), (18, 11, 3), (20, 11, 5), (21, 10, 4), (22, 11, 3)])
+def test_remapping_plans_match_oracle_and_save_sweeps(n, tb, lb):
+    """Qubit remapping: sweeps store their tiles with low bits exchanged for
+    the next sweep's hot bits; the plan still ends in the original order
+    (the emulator stores through each sweep's output map)."""
+    for ops in (circuits.random_mix(n, 300, seed=n), circuits.random_all_gates(n, 200, seed=n + 1),
+                circuits.quantum_volume(n, 8, seed=n + 2)):
+        ref = oracle.run_ops(ops, n)
+        psi, sweeps, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops), tb, "remap", lb)
+        assert np.abs(psi - ref).max() <= 1e-12, n
+        _, plain, _ = emulator.run(oracle.basis_state(n), n, gates_of(ops), tb, "select", lb)
+        assert sweeps <= plain + 1
+
+
+def test_remapping_saves_sweeps_on_the_benchmark_mix():
+    g = gates_of(circuits.random_mix(30, 400, seed=1234))
+    plain = emulator.plan_stats(30, g, tile_bits=11, reorder="select", low_bits=3)["sweeps"]
+    remap = emulator.plan_stats(30, g, tile_bits=11, reorder="remap", low_bits=3)["sweeps"]
+    assert remap < plain
