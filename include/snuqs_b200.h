@@ -73,10 +73,10 @@ typedef enum {
                            covers runs of 2^value amplitudes); 0 (default): 3 for
                            complex128, 4 for complex64 (128-byte runs) when the state
                            spans several tiles; ignored unless value + 4 <= tile bits */
-  SQ_OPT_REMAP = 6      /* 1 (default): JIT-specialised sweeps may store their tiles with
-                           index bits permuted so that the next sweeps find their most
-                           used qubits on the low bits every tile holds; every flush ends
-                           in the original order.  0: never */
+  SQ_OPT_REMAP = 6      /* 1: JIT-specialised sweeps may store their tiles with index bits
+                           permuted so that the next sweeps find their most used qubits
+                           on the low bits every tile holds; every flush ends in the
+                           original order.  0 (default; SQ_REMAP=1 changes it): never */
 } sq_option;
 
 /* ---- library / device ------------------------------------------------ */

@@ -898,9 +898,10 @@ extern "C" int sq_jit_source(uint32_t num_qubits, int dtype, const sq_circuit_op
     }
     opt.max_dense_k = c64 ? 4 : 3;
     opt.low_bits = sq::auto_low_bits(c64, num_qubits, opt.tile_bits);
-    // As a state of the engine plans with its default options (remapping on).
+    // As a state of the engine plans with its default options (remapping off
+    // unless SQ_REMAP=1).
     const char *re = std::getenv("SQ_REMAP");
-    opt.remap = !(re && re[0] == '0');
+    opt.remap = re && re[0] == '1';
     plan = sq::plan_sweeps(ap.forward, num_qubits, opt);
   } catch (const std::exception &e) {
     return sq_detail_fail(SQ_ERR_INVALID, e.what());

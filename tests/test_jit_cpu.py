@@ -53,7 +53,7 @@ def test_sources_cover_every_op_kind():
     # Direct-load sweeps take their tiles through the bulk-copy pipeline by
     # default (SQ_JIT_STAGES=0 brings back the register loads).
     first = "bulk_copy_pipeline" if "bulk_copy_pipeline" in seen else "direct_load"
-    assert seen >= set(OP_ROUTINES) | {"global_control", "direct_store", first, "remapping_store"}, seen
+    assert seen >= set(OP_ROUTINES) | {"global_control", "direct_store", first}, seen
 
 
 def test_sources_depend_on_structure_not_angles():
@@ -156,7 +156,7 @@ def test_batch_adjoint_source_compiles(dtype, n):
     capi.jit_compile(src)
 
 
-@pytest.mark.parametrize("env", ["SQ_JIT_EARLY=1", "SQ_JIT_STAGES=1"])
+@pytest.mark.parametrize("env", ["SQ_JIT_EARLY=1", "SQ_JIT_STAGES=1", "SQ_REMAP=1"])
 def test_alternative_tile_loops_compile(env):
     """The early-load and bulk-copy tile loops (off by default) generate
     sources that compile, for both precisions (a subprocess: the switches
@@ -175,7 +175,8 @@ def test_alternative_tile_loops_compile(env):
         "    for s in srcs[:3]:\n"
         "        capi.jit_compile(s)\n"
     ) % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
-         "jit_sweep_early<" if "EARLY" in env else "jit_sweep_pipe<")
+         {"SQ_JIT_EARLY": "jit_sweep_early<", "SQ_JIT_STAGES": "jit_sweep_pipe<",
+          "SQ_REMAP": "JitTileMap<"}[env.split("=")[0]])
     k, v = env.split("=")
     # Early loads apply to direct-load sweeps; complex64 turns those on with SQ_JIT_DLOAD.
     r = subprocess.run([sys.executable, "-c", code], env={**os.environ, k: v, "SQ_JIT_DLOAD": "1"},
