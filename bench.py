@@ -888,11 +888,15 @@ def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED):
                       "around the batch's kernels (median of 3)"}
 
 
-def e2e(n, ops, args, amp):
-    """Same metric through the reference-facing `_C` drop-in, as
-    simulation.py drives it: initialize_basis_z, one functionals.apply per
-    gate, then the state copied to a pinned host StateVector (the result).
-    Every step is timed, K steps as the device-timed line."""
+def e2e(n, ops, args, amp, shots: int = 1_000_000):
+    """Same metric through the reference-facing `_C` drop-in, as a shot-based
+    Braket task drives it (simulation.py: initialize_basis_z, one
+    functionals.apply per gate, then retrieve_samples): each step applies the
+    circuit and returns `shots` measurement samples -- the step's uniforms go
+    to the device, only the shot indices come back (functionals.sample).
+    Every step is timed, K steps as the device-timed line.  The same with the
+    StateVector result (the whole state copied to a pinned host buffer) is
+    reported beside it."""
     import torch
 
     from snuqs_b200 import _C
@@ -901,33 +905,60 @@ def e2e(n, ops, args, amp):
     prec = args.precision
     try:
         sv = _C.result_types.StateVector(_C.DeviceType.CUDA, n, prec)
-        host = _C.result_types.StateVector(n, True, prec)
-    except Exception as e:  # pinned allocation can fail on small hosts
+    except Exception as e:
         return {"value": None, "unit": "GB/s", "note": f"e2e skipped: {e}"}
     gops = [G.Unitary(list(op[1]), op[3]) if op[0] == "Unitary" else
             getattr(G, op[0])(list(op[1]), *op[2]) for op in ops]
     h2d = sum(16 * (1 << (2 * len(g.targets))) for g in gops)
     steps = args.steps
+    rng = np.random.default_rng(SEED + 7)
+    uniforms = [rng.random(shots) for _ in range(steps + 1)]
 
-    def one():
+    def one(u):
         _C.functionals.initialize_basis_z(sv)
         for g in gops:
             _C.functionals.apply(sv, g, n, g.targets)
-        host.copy(sv)
-        return np.array(host, copy=False)[0]
+        return _C.functionals.sample(sv, u)
 
-    one()
+    one(uniforms[-1])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(steps):
-        one()
+    for s in range(steps):
+        samples = one(uniforms[s])
     t = (time.perf_counter() - t0) / steps
-    del sv, host
-    return {"value": round(args.gates * 2 * amp * (1 << n) / t / 1e9, 2), "unit": "GB/s",
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": (1 << n) * amp,
-            "ms_per_step": round(t * 1e3, 2), "steps": steps, "precision": prec,
-            "path": "_C.functionals.apply per gate + StateVector.copy to pinned host",
-            "timing": "host wall clock around synchronous steps"}
+    out = {"value": round(args.gates * 2 * amp * (1 << n) / t / 1e9, 2), "unit": "GB/s",
+           "h2d_bytes_per_step": h2d + shots * 8, "d2h_bytes_per_step": shots * 8,
+           "ms_per_step": round(t * 1e3, 2), "steps": steps, "precision": prec, "shots": shots,
+           "samples_checksum": int(np.sum(samples.astype(np.uint64) % np.uint64(1 << 20))),
+           "path": "_C.functionals.apply per gate + functionals.sample (shot indices to the host)",
+           "timing": "host wall clock around synchronous steps"}
+    # The StateVector result: the whole state to pinned host memory per step.
+    try:
+        host = _C.result_types.StateVector(n, True, prec)
+        sv_steps = max(1, min(steps, 3))
+
+        def one_sv():
+            _C.functionals.initialize_basis_z(sv)
+            for g in gops:
+                _C.functionals.apply(sv, g, n, g.targets)
+            host.copy(sv)
+            return np.array(host, copy=False)[0]
+
+        one_sv()
+        t0 = time.perf_counter()
+        for _ in range(sv_steps):
+            one_sv()
+        tsv = (time.perf_counter() - t0) / sv_steps
+        out["state_vector_result"] = {
+            "value": round(args.gates * 2 * amp * (1 << n) / tsv / 1e9, 2), "unit": "GB/s",
+            "ms_per_step": round(tsv * 1e3, 2), "steps": sv_steps, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": (1 << n) * amp,
+            "path": "_C.functionals.apply per gate + StateVector.copy to pinned host"}
+        del host
+    except Exception as e:  # pinned allocation can fail on small hosts
+        out["state_vector_result"] = {"note": f"skipped: {e}"}
+    del sv
+    return out
 
 
 def cpu_baseline(n, ops):

@@ -83,6 +83,7 @@ SIGNATURES = {
     "sq_state_check": (_I, [_P, _P]),
     "sq_variance_pauli": (_I, [_P, ctypes.c_char_p, _PD, _U32, _PD, _P]),
     "sq_sample": (_I, [_P, _P, _U64, _P, _P]),
+    "sq_sample_host": (_I, [_P, _PD, _U64, _PU64, _P]),
     "sq_amplitudes": (_I, [_P, _P, _U64, _P, _P]),
     "sq_marginal_probabilities": (_I, [_P, _PU32, _U32, _P, _P]),
     "sq_state_distance": (_I, [_P, _P, _PD, _PD, _P]),

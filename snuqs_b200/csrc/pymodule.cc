@@ -588,6 +588,23 @@ PYBIND11_MODULE(_C, m) {
       py::arg("state_vector"), py::arg("paulis"), py::arg("weights"), py::kw_only(),
       py::arg("stream") = nullptr);
   m_functionals.def(
+      "sample",
+      [](StateVector &sv, py::array_t<double, py::array::c_style | py::array::forcecast> uniforms,
+         std::shared_ptr<Stream> stream) {
+        auto u = uniforms.unchecked<1>();
+        py::array_t<uint64_t> out(u.shape(0));
+        const double *up = uniforms.data();
+        uint64_t *op = out.mutable_data();
+        const uint64_t shots = uint64_t(u.shape(0));
+        {
+          py::gil_scoped_release nogil;
+          check(sq_sample_host(sv.dev(), up, shots, op, stream_ptr(stream)));
+        }
+        return out;
+      },
+      py::arg("state_vector"), py::arg("uniforms"), py::kw_only(), py::arg("stream") = nullptr,
+      "Measurement shots on the device: basis-state indices at the given uniforms in [0, 1).");
+  m_functionals.def(
       "set_option",
       [](StateVector &sv, int option, int64_t value) { check(sq_set_option(sv.dev(), option, value)); },
       py::arg("state_vector"), py::arg("option"), py::arg("value"));

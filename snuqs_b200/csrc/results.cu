@@ -320,21 +320,24 @@ int fail(int code, const std::string &msg) { return sq_detail_fail(code, msg.c_s
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Scratch bytes of sample_impl: the upper tree, per-leaf counts / offsets /
+// cursors, per-shot leaf, residual and bucket order.
+size_t sample_scratch_bytes(uint32_t n, uint64_t shots) {
+  const uint32_t depth = n > uint32_t(kLeafBits) ? n - kLeafBits : 0;
+  const uint64_t nleaves = uint64_t(1) << depth;
+  return align256((2 * nleaves - 1) * sizeof(double)) + 3 * align256(nleaves * sizeof(uint32_t)) +
+         2 * align256(shots * sizeof(uint32_t)) + align256(shots * sizeof(double));
+}
+
 template <typename C2>
-int sample_impl(sq_state *s, const C2 *psi, uint32_t n, const double *u, uint64_t shots, uint64_t *out,
+int sample_impl(const C2 *psi, uint32_t n, const double *u, uint64_t shots, uint64_t *out, void *scr,
                 cudaStream_t st) {
   const uint64_t N = uint64_t(1) << n;
   const uint32_t depth = n > uint32_t(kLeafBits) ? n - kLeafBits : 0;
   const uint64_t nleaves = uint64_t(1) << depth;
-  // Scratch: the upper tree, per-leaf counts / offsets / cursors, per-shot
-  // leaf, residual and bucket order.
   const size_t b_tree = align256((2 * nleaves - 1) * sizeof(double));
   const size_t b_leafu = align256(nleaves * sizeof(uint32_t));
   const size_t b_shot32 = align256(shots * sizeof(uint32_t));
-  const size_t b_shot64 = align256(shots * sizeof(double));
-  void *scr = nullptr;
-  const int rc = sq_detail_state_scratch(s, b_tree + 3 * b_leafu + 2 * b_shot32 + b_shot64, &scr);
-  if (rc != SQ_OK) return rc;
   char *p = static_cast<char *>(scr);
   double *tree = reinterpret_cast<double *>(p);
   p += b_tree;
@@ -386,9 +389,39 @@ int sq_sample(sq_state *s, const double *uniforms_device, uint64_t shots, uint64
   if (rc != SQ_OK || shots == 0) return rc;
   const uint32_t n = sq_state_num_qubits(s);
   if (n > uint32_t(kLeafBits) + 22) return fail(SQ_ERR_UNSUPPORTED, "sq_sample: more than 34 qubits");
+  void *scr = nullptr;
+  const int sc = sq_detail_state_scratch(s, sample_scratch_bytes(n, shots), &scr);
+  if (sc != SQ_OK) return sc;
   if (sq_state_dtype(s) == SQ_C64)
-    return sample_impl(s, static_cast<const float2 *>(sq_state_data(s)), n, uniforms_device, shots, out_device, st);
-  return sample_impl(s, static_cast<const double2 *>(sq_state_data(s)), n, uniforms_device, shots, out_device, st);
+    return sample_impl(static_cast<const float2 *>(sq_state_data(s)), n, uniforms_device, shots, out_device, scr, st);
+  return sample_impl(static_cast<const double2 *>(sq_state_data(s)), n, uniforms_device, shots, out_device, scr,
+                     st);
+}
+
+int sq_sample_host(sq_state *s, const double *uniforms, uint64_t shots, uint64_t *out, void *stream) {
+  if (!s || (shots && (!uniforms || !out))) return fail(SQ_ERR_INVALID, "sq_sample_host: null pointer");
+  if (shots > (uint64_t(1) << 31)) return fail(SQ_ERR_UNSUPPORTED, "sq_sample_host: more than 2^31 shots per call");
+  auto st = static_cast<cudaStream_t>(stream);
+  int rc = sq_flush(s, stream);
+  if (rc != SQ_OK || shots == 0) return rc;
+  const uint32_t n = sq_state_num_qubits(s);
+  if (n > uint32_t(kLeafBits) + 22) return fail(SQ_ERR_UNSUPPORTED, "sq_sample_host: more than 34 qubits");
+  // The state's scratch holds the uniforms and the indices, then the sampler's own scratch.
+  const size_t b_u = align256(shots * sizeof(double)), b_o = align256(shots * sizeof(uint64_t));
+  void *scr = nullptr;
+  rc = sq_detail_state_scratch(s, b_u + b_o + sample_scratch_bytes(n, shots), &scr);
+  if (rc != SQ_OK) return rc;
+  char *p = static_cast<char *>(scr);
+  double *du = reinterpret_cast<double *>(p);
+  uint64_t *dout = reinterpret_cast<uint64_t *>(p + b_u);
+  RQ_CUDA(cudaMemcpyAsync(du, uniforms, shots * sizeof(double), cudaMemcpyHostToDevice, st));
+  rc = sq_state_dtype(s) == SQ_C64
+           ? sample_impl(static_cast<const float2 *>(sq_state_data(s)), n, du, shots, dout, p + b_u + b_o, st)
+           : sample_impl(static_cast<const double2 *>(sq_state_data(s)), n, du, shots, dout, p + b_u + b_o, st);
+  if (rc != SQ_OK) return rc;
+  RQ_CUDA(cudaMemcpyAsync(out, dout, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  RQ_CUDA(cudaStreamSynchronize(st));
+  return SQ_OK;
 }
 
 int sq_amplitudes(sq_state *s, const uint64_t *indices_device, uint64_t count, double *out_device, void *stream) {

@@ -133,3 +133,22 @@ def test_state_distance_reports_complex64_error():
     assert a.distance(a) == (0.0, pytest.approx(0.0, abs=1e-15))
     a.close()
     b.close()
+
+
+def test_host_sampling_through_the_pybind_layer():
+    """_C.functionals.sample (sq_sample_host): host uniforms in, shot indices
+    out, the same indices as the oracle's walk."""
+    from snuqs_b200 import _C
+
+    n = 15
+    ops = circuits.random_all_gates(n, 120, seed=15)
+    G = _C.operation.gate_operations
+    sv = _C.result_types.StateVector(_C.DeviceType.CUDA, n)
+    _C.functionals.initialize_basis_z(sv)
+    for op in ops:
+        g = getattr(G, op[0])(list(op[1]), *op[2])
+        _C.functionals.apply(sv, g, n, list(op[1]))
+    u = np.random.default_rng(3).random(30000)
+    got = _C.functionals.sample(sv, u)
+    want = oracle.sample_inverse_cdf(oracle.run_ops(ops, n), u)
+    assert got.dtype == np.uint64 and np.array_equal(got, want)
