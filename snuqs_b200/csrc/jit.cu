@@ -788,35 +788,108 @@ size_t jit_adjoint_smem(const PlannedSweep &ps, bool c64) {
   return jit_adjoint_smem_bytes(int(ps.h.m), c64 ? 8 : 16, ps.h.ncoef);
 }
 
-const void *jit_adjoint_kernel(const PlannedSweep &ps, bool c64, std::string &err) {
+// Kernel lookup by plan structure.  A generated kernel depends only on the
+// sweep's header, phases and ops (and the process-wide tile-loop switches),
+// not on its coefficient values, so a structure seen before skips source
+// generation and hashing (the host cost of every flush and gradient of a
+// repeated circuit).  Two independent 64-bit FNV-1a hashes of the raw bytes
+// (the planner zero-fills every padding byte) form the key.
+struct PlanKey {
+  uint64_t a, b;
+  bool operator<(const PlanKey &o) const { return a != o.a ? a < o.a : b < o.b; }
+};
+
+PlanKey plan_key(const PlannedSweep &ps, bool c64, int kind) {
+  uint64_t a = 1469598103934665603ull, b = 0x9ae16a3b2f90404full;
+  auto mix = [&](const void *p, size_t n) {
+    const unsigned char *q = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < n; ++i) {
+      a = (a ^ q[i]) * 1099511628211ull;
+      b = (b ^ q[i]) * 0x100000001b3ull + 0x9e3779b97f4a7c15ull;
+    }
+  };
+  mix(&ps.h, sizeof(ps.h));
+  mix(ps.ph.data(), ps.ph.size() * sizeof(SweepPhase));
+  mix(ps.op.data(), ps.op.size() * sizeof(SweepOp));
+  const uint8_t extra[2] = {uint8_t(c64), uint8_t(kind)};
+  mix(extra, sizeof(extra));
+  return {a, b};
+}
+
+std::mutex g_plan_mu;
+std::map<PlanKey, Entry *> g_plan_entries;  // nullptr: not covered by the generated form
+
+// The cached entry for this structure (*found = false when it must be made).
+Entry *plan_lookup(const PlanKey &k, bool *found) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = g_plan_entries.find(k);
+  *found = it != g_plan_entries.end();
+  return *found ? it->second : nullptr;
+}
+
+void plan_store(const PlanKey &k, Entry *e) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  g_plan_entries[k] = e;
+}
+
+Entry *adjoint_entry(const PlannedSweep &ps, bool c64) {
+  const PlanKey k = plan_key(ps, c64, 1);
+  bool found = false;
+  Entry *e = plan_lookup(k, &found);
+  if (found) return e;
   const std::string body = jit_adjoint_body(ps, c64, 2);
-  if (body.empty()) {
+  e = body.empty() ? nullptr : &get_entry(body, "sq_jit_adjoint");
+  plan_store(k, e);
+  return e;
+}
+
+Entry &sweep_entry(const PlannedSweep &ps, bool c64) {
+  const PlanKey k = plan_key(ps, c64, 0);
+  bool found = false;
+  Entry *e = plan_lookup(k, &found);
+  if (found) return *e;
+  e = &get_entry(jit_body(ps, c64, jit_minb(c64, ps.h.m)));
+  plan_store(k, e);
+  return *e;
+}
+
+const void *jit_adjoint_kernel(const PlannedSweep &ps, bool c64, std::string &err) {
+  Entry *e = adjoint_entry(ps, c64);
+  if (!e) {
     err = "sweep not covered by the JIT adjoint form";
     return nullptr;
   }
-  Entry &e = get_entry(body, "sq_jit_adjoint");
-  if (e.failed) {
-    err = e.err;
+  if (e->failed) {
+    err = e->err;
     return nullptr;
   }
-  return reinterpret_cast<const void *>(e.kernel);
+  return reinterpret_cast<const void *>(e->kernel);
+}
+
+// Compiles (in parallel) the kernels of structures not seen before.
+template <class F>
+void prepare_parallel(const std::vector<const PlannedSweep *> &sweeps, F make) {
+  std::vector<const PlannedSweep *> todo;
+  for (const auto *ps : sweeps) todo.push_back(ps);
+  std::atomic<size_t> next{0};
+  const unsigned nth = std::max(1u, std::min<unsigned>(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < std::min<size_t>(nth, todo.size()); ++t)
+    pool.emplace_back([&] {
+      for (size_t i = next++; i < todo.size(); i = next++) make(*todo[i]);
+    });
+  for (auto &th : pool) th.join();
 }
 
 void jit_prepare_adjoint(const std::vector<const PlannedSweep *> &sweeps, bool c64) {
   if (!jit_available() || sweeps.empty()) return;
-  std::vector<std::string> bodies;
+  std::vector<const PlannedSweep *> todo;
   for (const auto *ps : sweeps) {
-    std::string b = jit_adjoint_body(*ps, c64, 2);
-    if (!b.empty()) bodies.push_back(std::move(b));
+    bool found = false;
+    plan_lookup(plan_key(*ps, c64, 1), &found);
+    if (!found) todo.push_back(ps);
   }
-  std::atomic<size_t> next{0};
-  const unsigned nth = std::max(1u, std::min<unsigned>(16u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> pool;
-  for (unsigned t = 0; t < std::min<size_t>(nth, bodies.size()); ++t)
-    pool.emplace_back([&] {
-      for (size_t i = next++; i < bodies.size(); i = next++) get_entry(bodies[i], "sq_jit_adjoint");
-    });
-  for (auto &th : pool) th.join();
+  prepare_parallel(todo, [&](const PlannedSweep &ps) { adjoint_entry(ps, c64); });
 }
 
 size_t jit_smem(const PlannedSweep &ps, bool c64) {
@@ -841,7 +914,7 @@ int jit_minb(bool c64, uint32_t m) {
 }
 
 const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err) {
-  Entry &e = get_entry(jit_body(ps, c64, jit_minb(c64, ps.h.m)));
+  Entry &e = sweep_entry(ps, c64);
   if (e.failed) {
     err = e.err;
     return nullptr;
@@ -851,17 +924,13 @@ const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err)
 
 void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64) {
   if (!jit_available() || sweeps.empty()) return;
-  std::vector<std::string> srcs;
-  srcs.reserve(sweeps.size());
-  for (const auto *ps : sweeps) srcs.push_back(jit_body(*ps, c64, jit_minb(c64, ps->h.m)));
-  std::atomic<size_t> next{0};
-  const unsigned nth = std::max(1u, std::min<unsigned>(16u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> pool;
-  for (unsigned t = 0; t < std::min<size_t>(nth, srcs.size()); ++t)
-    pool.emplace_back([&] {
-      for (size_t i = next++; i < srcs.size(); i = next++) get_entry(srcs[i]);
-    });
-  for (auto &th : pool) th.join();
+  std::vector<const PlannedSweep *> todo;
+  for (const auto *ps : sweeps) {
+    bool found = false;
+    plan_lookup(plan_key(*ps, c64, 0), &found);
+    if (!found) todo.push_back(ps);
+  }
+  prepare_parallel(todo, [&](const PlannedSweep &ps) { sweep_entry(ps, c64); });
 }
 
 }  // namespace sq
