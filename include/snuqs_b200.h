@@ -378,6 +378,19 @@ int sq_batch_last_timing(const sq_batch *b, double *kernel_ms, uint32_t *ctas);
  * bytes (per streamed circuit (2 x sweeps + 1) x 2^n x amplitude bytes: every
  * sweep reads and writes the state, the energy pass reads it once). */
 int sq_batch_stats(const sq_batch *b, uint64_t *streamed, uint64_t *sweeps, uint64_t *hbm_bytes);
+/* Structure groups of the last sq_batch_run: streamed circuits whose plans
+ * differ only in their angles (the same circuit with other parameters) run
+ * as one multi-state JIT launch per sweep over all of their states instead of
+ * one CTA per circuit (needs NVRTC; SQ_BATCH_MULTI=0 turns it off).  Writes
+ * the number of groups and of the circuits they hold. */
+int sq_batch_groups(const sq_batch *b, uint32_t *groups, uint32_t *circuits);
+/* Test hook: CUDA source of the multi-state JIT kernel (sq_jit_msweep) of
+ * sweep `sweep_index` of a circuit as a batch energy run plans it with the
+ * default tile size (num_qubits above it).  Writes at most cap bytes
+ * (NUL-terminated), the full length to *len and the number of sweeps to
+ * *nsweeps.  Needs no GPU. */
+int sq_jit_multi_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
+                        uint32_t sweep_index, char *buf, uint64_t cap, uint64_t *len, uint32_t *nsweeps);
 
 #ifdef __cplusplus
 }

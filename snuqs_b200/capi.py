@@ -105,6 +105,8 @@ SIGNATURES = {
     "sq_batch_state": (_I, [_P, _U32, _P, _P]),
     "sq_batch_last_timing": (_I, [_P, _PD, _PU32]),
     "sq_batch_stats": (_I, [_P, _PU64, _PU64, _PU64]),
+    "sq_batch_groups": (_I, [_P, _PU32, _PU32]),
+    "sq_jit_multi_source": (_I, [_U32, _I, _P, _U32, _U32, ctypes.c_char_p, _U64, _PU64, _PU32]),
 }
 
 
@@ -133,11 +135,14 @@ def jit_info():
     return bool(av.value), a.value, b.value
 
 
-def jit_sources(n: int, ops, dtype: int = SQ_C128, limit: int | None = None, adjoint: bool = False):
+def jit_sources(n: int, ops, dtype: int = SQ_C128, limit: int | None = None, adjoint: bool = False,
+                multi: bool = False):
     """CUDA sources of the JIT kernels of the fused sweeps of a circuit (with
-    adjoint=True: of the reverse sweeps of its adjoint-gradient plan; "" for
-    a sweep the generic kernel runs)."""
-    fn = lib().sq_jit_adjoint_source if adjoint else lib().sq_jit_source
+    adjoint=True: of the reverse sweeps of its adjoint-gradient plan; with
+    multi=True: the multi-state kernels of its batch energy plan; "" for a
+    sweep the generic kernel runs)."""
+    fn = (lib().sq_jit_adjoint_source if adjoint else
+          lib().sq_jit_multi_source if multi else lib().sq_jit_source)
     arr, keep = circuit_ops(ops)
     ln, ns = _U64(0), _U32(0)
     check(fn(n, dtype, ctypes.cast(arr, _P), len(ops), 0, None, 0, ctypes.byref(ln), ctypes.byref(ns)))
@@ -329,6 +334,13 @@ class Batch:
         a, b, c = _U64(0), _U64(0), _U64(0)
         check(lib().sq_batch_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
+
+    def groups(self):
+        """(structure groups, circuits in them) of the last run: circuits run
+        by multi-state JIT sweeps."""
+        g, c = _U32(0), _U32(0)
+        check(lib().sq_batch_groups(self.h, ctypes.byref(g), ctypes.byref(c)))
+        return g.value, c.value
 
     def last_timing(self):
         ms, ctas = _D(0), _U32(0)

@@ -12,6 +12,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <thread>
@@ -22,6 +23,7 @@
 #include "batch_kernels.cuh"
 #include "host_ops.h"
 #include "jit.h"
+#include "jit_kernels.cuh"
 #include "sweep_registry.h"
 
 int sq_detail_fail(int code, const char *msg);
@@ -87,6 +89,27 @@ struct HostBuf {
 
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// One sweep of a structure group: its multi-state JIT kernel, dynamic shared
+// memory, resident CTAs per SM, coefficient count, and the byte offset of its
+// coefficients within a circuit's packed plan.
+struct MultiSweep {
+  const void *fn = nullptr;
+  size_t smem = 0;
+  int per_sm = 1;
+  uint32_t ncoef = 0;
+  uint64_t coef_at = 0;
+};
+
+// Streamed circuits whose plans differ only in coefficient values: their
+// states lie back to back in the pool and their packed plans back to back in
+// the plan buffer (table positions first .. first + count - 1), and each
+// sweep runs as one multi-state launch over all of them.
+struct MultiGroup {
+  uint32_t n = 0, count = 0, first = 0;
+  uint64_t pool_off = 0, plan_off = 0, rec_bytes = 0;
+  std::vector<MultiSweep> sweeps;
+};
+
 }  // namespace
 
 struct sq_batch {
@@ -125,6 +148,10 @@ struct sq_batch {
   // energy plan: count, fused sweeps, and their algorithmic HBM bytes (each
   // sweep reads and writes the state, the energy pass reads it once).
   uint64_t stat_streamed = 0, stat_sweeps = 0, stat_bytes = 0;
+  // Structure groups of the last energy plan (run by multi-state JIT sweeps)
+  // and the table positions [0, n_interp) that batch_kernel runs.
+  std::vector<MultiGroup> groups;
+  uint32_t n_interp = 0;
 };
 
 namespace {
@@ -252,6 +279,81 @@ int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
   }
 }
 
+// Byte ranges of the coefficient values in a packed plan.
+template <typename Real>
+std::vector<std::pair<size_t, size_t>> coef_ranges(const std::vector<unsigned char> &p) {
+  using C2 = typename sq::Vec2<Real>::T;
+  std::vector<std::pair<size_t, size_t>> holes;
+  for (size_t off = 0; off < p.size();) {
+    const auto &ps = *reinterpret_cast<const sq::PackedSweep *>(p.data() + off);
+    holes.emplace_back(off + ps.coef_off, off + ps.coef_off + size_t(ps.h.ncoef) * sizeof(C2));
+    off += ps.bytes;
+  }
+  return holes;
+}
+
+// Packed plans a and b are equal except for coefficient values (`holes`:
+// a's coefficient ranges).
+bool same_structure(const std::vector<unsigned char> &a, const std::vector<unsigned char> &b,
+                    const std::vector<std::pair<size_t, size_t>> &holes) {
+  if (a.size() != b.size()) return false;
+  size_t pos = 0;
+  for (const auto &h : holes) {
+    if (std::memcmp(a.data() + pos, b.data() + pos, h.first - pos) != 0) return false;
+    pos = h.second;
+  }
+  return std::memcmp(a.data() + pos, b.data() + pos, a.size() - pos) == 0;
+}
+
+// Hash of a packed plan's bytes outside its coefficient ranges, and of n.
+std::pair<uint64_t, uint64_t> structure_key(const std::vector<unsigned char> &p,
+                                            const std::vector<std::pair<size_t, size_t>> &holes, uint32_t n) {
+  uint64_t a = 1469598103934665603ull ^ n, b = 0x9ae16a3b2f90404full + n;
+  auto mix = [&](size_t from, size_t to) {
+    for (size_t i = from; i < to; ++i) {
+      a = (a ^ p[i]) * 1099511628211ull;
+      b = (b ^ p[i]) * 0x100000001b3ull + 0x9e3779b97f4a7c15ull;
+    }
+  };
+  size_t pos = 0;
+  for (const auto &h : holes) {
+    mix(pos, h.first);
+    pos = h.second;
+  }
+  mix(pos, p.size());
+  return {a, b ^ p.size()};
+}
+
+// The sweeps of a packed plan (structure only: coefficients are left zero)
+// and the byte offset of each sweep's coefficients.
+std::vector<sq::PlannedSweep> unpack_sweeps(const std::vector<unsigned char> &p, std::vector<uint64_t> &coef_at) {
+  std::vector<sq::PlannedSweep> out;
+  coef_at.clear();
+  for (size_t off = 0; off < p.size();) {
+    const auto &rec = *reinterpret_cast<const sq::PackedSweep *>(p.data() + off);
+    sq::PlannedSweep ps;
+    ps.h = rec.h;
+    const auto *ph = reinterpret_cast<const sq::SweepPhase *>(p.data() + off + rec.phase_off);
+    const auto *op = reinterpret_cast<const sq::SweepOp *>(p.data() + off + rec.op_off);
+    ps.ph.assign(ph, ph + rec.h.nphases);
+    ps.op.assign(op, op + rec.nops);
+    ps.coef.assign(rec.h.ncoef, cplx(0.0, 0.0));
+    out.push_back(std::move(ps));
+    coef_at.push_back(off + rec.coef_off);
+    off += rec.bytes;
+  }
+  return out;
+}
+
+// Multi-state JIT sweeps for the energy runs: on unless SQ_JIT=0 or
+// SQ_BATCH_MULTI=0, and only with NVRTC present.
+bool multi_enabled() {
+  const char *j = std::getenv("SQ_JIT");
+  const char *m = std::getenv("SQ_BATCH_MULTI");
+  if ((j && j[0] == '0') || (m && m[0] == '0')) return false;
+  return sq::jit_available();
+}
+
 // Energy kernel of (precision, tile bits); nullptr when not compiled.
 template <typename Real>
 const void *batch_fn(uint32_t m) {
@@ -331,42 +433,140 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   size_t plan_bytes = b->planned_bytes;
   if (replan) {
   b->deferred.clear();
+  int sms = 0;
+  SQB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  // Candidates for multi-state JIT sweeps: streamed circuits, planned with
+  // the default tile, low-bit and fusion settings (so the autotuner's trials
+  // reuse the same compiled kernels); the rest with the batch's settings.
+  const uint32_t MJ = batch_default_bits<Real>();
+  const bool multi = multi_enabled();
+  std::vector<char> cand(nc, 0);
+  for (size_t i = 0; i < nc; ++i) cand[i] = multi && b->circs[i].n > std::max(M, MJ);
   // Plan all circuits in parallel.
   std::vector<std::vector<unsigned char>> packed(nc);
   std::vector<int> nsweeps(nc, 0);
   std::vector<std::string> errs(nc);
   std::atomic<size_t> next{0};
   const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> pool;
-  for (unsigned t = 0; t < nth; ++t)
-    pool.emplace_back([&]() {
-      for (size_t i = next++; i < nc; i = next++)
-        nsweeps[i] = plan_circuit<Real>(b->circs[i], M, b->low_bits, b->max_ops, packed[i], errs[i]);
-    });
-  for (auto &th : pool) th.join();
+  auto plan_all = [&](const std::vector<uint32_t> &ids) {
+    next = 0;
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < std::min<size_t>(nth, ids.size()); ++t)
+      pool.emplace_back([&]() {
+        for (size_t k = next++; k < ids.size(); k = next++) {
+          const uint32_t i = ids[k];
+          packed[i].clear();
+          nsweeps[i] = cand[i] ? plan_circuit<Real>(b->circs[i], MJ, 0, 0, packed[i], errs[i])
+                               : plan_circuit<Real>(b->circs[i], M, b->low_bits, b->max_ops, packed[i], errs[i]);
+        }
+      });
+    for (auto &th : pool) th.join();
+  };
+  {
+    std::vector<uint32_t> all(nc);
+    for (size_t i = 0; i < nc; ++i) all[i] = uint32_t(i);
+    plan_all(all);
+  }
   for (size_t i = 0; i < nc; ++i)
     if (nsweeps[i] < 0) return fail(SQ_ERR_UNSUPPORTED, errs[i]);
+  // Structure groups among the candidates.  A group needs at least two
+  // tiles per SM in total and a compiled kernel for every sweep; candidates
+  // left out are planned again with the batch's settings.
+  b->groups.clear();
+  std::vector<int> group_of(nc, -1);
+  {
+    std::map<std::pair<uint64_t, uint64_t>, std::vector<uint32_t>> by_key;
+    for (size_t i = 0; i < nc; ++i)
+      if (cand[i] && nsweeps[i] > 0)
+        by_key[structure_key(packed[i], coef_ranges<Real>(packed[i]), b->circs[i].n)].push_back(uint32_t(i));
+    std::vector<std::vector<uint32_t>> members;
+    std::vector<std::vector<sq::PlannedSweep>> gsweeps;
+    std::vector<std::vector<uint64_t>> gcoef;
+    for (auto &kv : by_key) {
+      const auto &ids = kv.second;
+      const auto holes = coef_ranges<Real>(packed[ids[0]]);
+      std::vector<uint32_t> same;
+      for (uint32_t i : ids)
+        if (b->circs[i].n == b->circs[ids[0]].n && same_structure(packed[ids[0]], packed[i], holes))
+          same.push_back(i);
+      const uint32_t n = b->circs[ids[0]].n;
+      if ((uint64_t(same.size()) << (n - MJ)) < 2 * uint64_t(sms)) continue;
+      members.push_back(same);
+      gcoef.emplace_back();
+      gsweeps.push_back(unpack_sweeps(packed[ids[0]], gcoef.back()));
+    }
+    std::vector<const sq::PlannedSweep *> todo;
+    for (const auto &g : gsweeps)
+      for (const auto &ps : g) todo.push_back(&ps);
+    sq::jit_prepare_multi(todo, sizeof(Real) == 4);
+    for (size_t g = 0; g < members.size(); ++g) {
+      MultiGroup G;
+      G.n = b->circs[members[g][0]].n;
+      G.count = uint32_t(members[g].size());
+      G.rec_bytes = packed[members[g][0]].size();
+      bool ok = true;
+      for (size_t k = 0; k < gsweeps[g].size() && ok; ++k) {
+        const sq::PlannedSweep &ps = gsweeps[g][k];
+        MultiSweep w;
+        std::string err;
+        w.fn = sq::jit_msweep_kernel(ps, sizeof(Real) == 4, err);
+        w.smem = sq::jit_msweep_smem(ps, sizeof(Real) == 4);
+        w.ncoef = ps.h.ncoef;
+        w.coef_at = gcoef[g][k];
+        ok = w.fn != nullptr &&
+             cudaFuncSetAttribute(w.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(w.smem)) == cudaSuccess &&
+             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&w.per_sm, w.fn, 1 << (MJ - sq::kRegBits), w.smem) ==
+                 cudaSuccess;
+        if (!ok) cudaGetLastError();
+        w.per_sm = std::max(w.per_sm, 1);
+        G.sweeps.push_back(w);
+      }
+      if (!ok) continue;
+      for (uint32_t i : members[g]) group_of[i] = int(b->groups.size());
+      b->groups.push_back(std::move(G));
+    }
+    std::vector<uint32_t> again;
+    for (size_t i = 0; i < nc; ++i)
+      if (cand[i] && group_of[i] < 0) {
+        cand[i] = 0;
+        again.push_back(uint32_t(i));
+      }
+    if (!again.empty()) {
+      plan_all(again);
+      for (uint32_t i : again)
+        if (nsweeps[i] < 0) return fail(SQ_ERR_UNSUPPORTED, errs[i]);
+    }
+  }
   b->stat_streamed = b->stat_sweeps = b->stat_bytes = 0;
   for (size_t i = 0; i < nc; ++i)
-    if (b->circs[i].n > M) {
+    if (b->circs[i].n > M || group_of[i] >= 0) {
       b->stat_streamed++;
       b->stat_sweeps += uint64_t(nsweeps[i]);
       b->stat_bytes += (2 * uint64_t(nsweeps[i]) + 1) * (uint64_t(1) << b->circs[i].n) * sizeof(C2);
     }
-  // Largest circuits first (dynamic work queue).
-  b->order.resize(nc);
-  for (size_t i = 0; i < nc; ++i) b->order[i] = uint32_t(i);
+  // Table order: the circuits batch_kernel runs, largest first (its dynamic
+  // work queue), then each structure group's circuits together.
+  b->order.clear();
+  for (size_t i = 0; i < nc; ++i)
+    if (group_of[i] < 0) b->order.push_back(uint32_t(i));
   std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) {
     const uint64_t cx = (uint64_t(1) << b->circs[x].n) * (uint64_t(nsweeps[x]) + 1);
     const uint64_t cy = (uint64_t(1) << b->circs[y].n) * (uint64_t(nsweeps[y]) + 1);
     return cx > cy;
   });
-  // State pool: circuits that do not fit one tile, or whose state is kept.
+  b->n_interp = uint32_t(b->order.size());
+  for (size_t g = 0; g < b->groups.size(); ++g) {
+    b->groups[g].first = uint32_t(b->order.size());
+    for (size_t i = 0; i < nc; ++i)
+      if (group_of[i] == int(g)) b->order.push_back(uint32_t(i));
+  }
+  // State pool: circuits that do not fit one tile, or whose state is kept
+  // (in table order, so a group's states lie back to back).
   b->state_off.assign(nc, ~uint64_t(0));
   uint64_t pool_amps = 0;
   for (uint32_t id : b->order) {
     const Circ &c = b->circs[id];
-    if (c.n > M || b->keep) {
+    if (c.n > M || b->keep || group_of[id] >= 0) {
       b->state_off[id] = pool_amps;
       pool_amps += uint64_t(1) << c.n;
     }
@@ -406,9 +606,13 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     t.nrev = 0;
     t.lam_off = t.occ_off = 0;
     // A streamed state (n > M) leaves its energy to the grid-wide pass.
-    t.defer = c.n > M ? 1u : 0u;
+    t.defer = c.n > M || group_of[id] >= 0 ? 1u : 0u;
     if (t.defer) b->deferred.push_back(uint32_t(pos));
     off += packed[id].size();
+  }
+  for (auto &G : b->groups) {
+    G.pool_off = tab[G.first].state_off;
+    G.plan_off = tab[G.first].plan_off;
   }
   // Work items of the energy pass: chunks of 2^kEnergyChunkBits pairs.
   // Staged as [deferred | item_off (ndef+1) | item_k | item_j].
@@ -446,7 +650,8 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   int sms = 0;
   SQB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
   const int cps = b->ctas_per_sm ? std::min<int>(per_sm, int(b->ctas_per_sm)) : per_sm;
-  const uint32_t grid = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(nc, uint64_t(cps) * uint64_t(sms))));
+  const uint32_t grid =
+      uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(b->n_interp, uint64_t(cps) * uint64_t(sms))));
   if (!b->ev0) {
     SQB_CUDA(cudaEventCreate(&b->ev0));
     SQB_CUDA(cudaEventCreate(&b->ev1));
@@ -467,7 +672,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     P.circuits = static_cast<const sq::BatchCircuit *>(b->d_table.p);
     P.plans = static_cast<const unsigned char *>(b->d_plans.p);
     P.hams = static_cast<const sq::PauliParams *>(b->d_hams.p);
-    P.ncircuits = uint32_t(nc);
+    P.ncircuits = b->n_interp;
     P.counter = static_cast<unsigned *>(b->d_counter.p);
     P.energies = static_cast<double *>(b->d_energy.p);
     C2 *poolp = static_cast<C2 *>(b->d_pool.p);
@@ -481,7 +686,26 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
       cudaMemsetAsync(b->d_counter.p, 0, sizeof(unsigned), cs);
       // External event nodes, so the kernel's device time can be read back.
       cudaEventRecordWithFlags(b->ev0, cs, cudaEventRecordExternal);
-      cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, cs);
+      if (b->n_interp) cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, cs);
+      // Structure groups: |0...0> in every state, then one launch per sweep.
+      const uint32_t MJ = batch_default_bits<Real>();
+      for (const MultiGroup &G : b->groups) {
+        C2 *gpsi = poolp + G.pool_off;
+        const uint64_t total = uint64_t(G.count) << G.n;
+        const uint32_t ig = uint32_t(std::min<uint64_t>((total + 255) / 256, uint64_t(sms) * 8));
+        sq::batch_group_init<Real><<<ig, 256, 0, cs>>>(gpsi, total, G.n);
+        for (const MultiSweep &w : G.sweeps) {
+          sq::MultiParams Q;
+          Q.coefs = static_cast<const unsigned char *>(b->d_plans.p) + G.plan_off + w.coef_at;
+          Q.stride = G.rec_bytes;
+          Q.tile_shift = G.n - MJ;
+          Q.tiles = uint64_t(G.count) << Q.tile_shift;
+          Q.ncoef = w.ncoef;
+          const uint64_t mg = std::min<uint64_t>(Q.tiles, uint64_t(w.per_sm) * uint64_t(sms));
+          void *margs[] = {&gpsi, &Q};
+          cudaLaunchKernel(w.fn, dim3(unsigned(mg)), dim3(1u << (MJ - sq::kRegBits)), margs, w.smem, cs);
+        }
+      }
       if (ndef) {
         cudaMemcpyAsync(b->d_def.p, b->h_def.p, b->def_words * sizeof(uint32_t), cudaMemcpyHostToDevice, cs);
         const uint32_t *defp = static_cast<const uint32_t *>(b->d_def.p);
@@ -571,31 +795,17 @@ template <typename Real>
 bool uniform_plans(const sq_batch *b, const std::vector<std::vector<unsigned char>> &packed,
                    const std::vector<uint32_t> &nfwd, const std::vector<uint32_t> &nrev,
                    const std::vector<std::vector<std::pair<int32_t, double>>> &occs, uint32_t M) {
-  using C2 = typename sq::Vec2<Real>::T;
   const char *env = std::getenv("SQ_JIT");
   if ((env && env[0] == '0') || !sq::jit_available() || b->circs.empty()) return false;
   const size_t nc = b->circs.size();
   const uint32_t n = b->circs[0].n;
   if (n <= M) return false;
   const std::vector<unsigned char> &p0 = packed[0];
-  // Coefficient byte ranges of circuit 0's records.
-  std::vector<std::pair<size_t, size_t>> holes;
-  for (size_t off = 0; off < p0.size();) {
-    const auto &ps = *reinterpret_cast<const sq::PackedSweep *>(p0.data() + off);
-    holes.emplace_back(off + ps.coef_off, off + ps.coef_off + size_t(ps.h.ncoef) * sizeof(C2));
-    off += ps.bytes;
-  }
-  for (size_t i = 1; i < nc; ++i) {
-    if (b->circs[i].n != n || nfwd[i] != nfwd[0] || nrev[i] != nrev[0] || packed[i].size() != p0.size() ||
-        occs[i] != occs[0])
+  const auto holes = coef_ranges<Real>(p0);
+  for (size_t i = 1; i < nc; ++i)
+    if (b->circs[i].n != n || nfwd[i] != nfwd[0] || nrev[i] != nrev[0] || occs[i] != occs[0] ||
+        !same_structure(p0, packed[i], holes))
       return false;
-    size_t pos = 0;
-    for (const auto &h : holes) {
-      if (std::memcmp(packed[i].data() + pos, p0.data() + pos, h.first - pos) != 0) return false;
-      pos = h.second;
-    }
-    if (std::memcmp(packed[i].data() + pos, p0.data() + pos, p0.size() - pos) != 0) return false;
-  }
   return true;
 }
 
@@ -989,6 +1199,45 @@ int sq_jit_batch_adjoint_source(uint32_t num_qubits, int dtype, const sq_circuit
     std::memcpy(buf, src.data(), n);
     buf[n] = '\0';
   }
+  return SQ_OK;
+}
+
+int sq_jit_multi_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
+                        uint32_t sweep_index, char *buf, uint64_t cap, uint64_t *len, uint32_t *nsweeps) {
+  if ((nops && !ops) || !len) return fail(SQ_ERR_INVALID, "null pointer");
+  if (dtype != SQ_C128 && dtype != SQ_C64) return fail(SQ_ERR_INVALID, "bad dtype");
+  const bool c64 = dtype == SQ_C64;
+  const uint32_t M = c64 ? sq::kBatchTileBitsC64 : sq::kBatchTileBitsC128;
+  if (num_qubits <= M || num_qubits > 30) return fail(SQ_ERR_INVALID, "num_qubits must exceed the tile bits");
+  Circ c;
+  c.n = num_qubits;
+  c.ops.assign(ops, ops + nops);
+  std::vector<unsigned char> packed;
+  std::string err;
+  const int ns = c64 ? plan_circuit<float>(c, M, 0, 0, packed, err) : plan_circuit<double>(c, M, 0, 0, packed, err);
+  if (ns < 0) return fail(SQ_ERR_UNSUPPORTED, err);
+  if (nsweeps) *nsweeps = uint32_t(ns);
+  if (sweep_index >= uint32_t(ns)) return fail(SQ_ERR_INVALID, "no such sweep");
+  std::vector<uint64_t> coef_at;
+  const auto sweeps = unpack_sweeps(packed, coef_at);
+  const sq::PlannedSweep &ps = sweeps[sweep_index];
+  const std::string body = sq::jit_body(ps, c64, sq::jit_minb(c64, ps.h.m), true);
+  const std::string src = body.empty() ? std::string() : sq::jit_source(ps, c64, sq::jit_minb(c64, ps.h.m), true);
+  *len = src.size();
+  if (buf && cap) {
+    const size_t n = std::min<size_t>(cap - 1, src.size());
+    std::memcpy(buf, src.data(), n);
+    buf[n] = '\0';
+  }
+  return SQ_OK;
+}
+
+int sq_batch_groups(const sq_batch *b, uint32_t *groups, uint32_t *circuits) {
+  if (!b) return fail(SQ_ERR_INVALID, "null batch");
+  uint32_t c = 0;
+  for (const auto &g : b->groups) c += g.count;
+  if (groups) *groups = uint32_t(b->groups.size());
+  if (circuits) *circuits = c;
   return SQ_OK;
 }
 

@@ -320,6 +320,21 @@ static __global__ void __launch_bounds__(kReduceThreads)
   if (threadIdx.x == 0) energies[deferred[k]] = v;
 }
 
+// |0...0> in each of the K states of 2^n amplitudes that lie back to back
+// from psi (a structure group of a batch, before its multi-state sweeps);
+// total = K 2^n.
+template <typename Real>
+__global__ void batch_group_init(typename Vec2<Real>::T *__restrict__ psi, uint64_t total, uint32_t n) {
+  const uint64_t mask = (uint64_t(1) << n) - 1;
+  for (uint64_t j = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; j < total;
+       j += uint64_t(gridDim.x) * blockDim.x) {
+    typename Vec2<Real>::T v;
+    v.x = Real((j & mask) == 0 ? 1 : 0);
+    v.y = Real(0);
+    psi[j] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Batched adjoint gradients: one circuit per CTA (work queue as above).  For
 // each circuit: forward sweeps on psi, lambda = H psi with E = Re <psi|lambda>,

@@ -373,7 +373,7 @@ int jit_stages(bool c64) {
 // measured faster on B200 for complex128 (7.10 vs 7.38 ms per 30-qubit sweep)
 // and, without early loads, slightly slower for complex64 (3.86 vs 3.76 ms);
 // SQ_JIT_DLOAD=0/1 overrides the choice for both precisions.
-JitShape jit_shape(const PlannedSweep &ps, bool c64) {
+JitShape jit_shape(const PlannedSweep &ps, bool c64, bool multi = false) {
   static const int dload_env = [] {
     const char *e = std::getenv("SQ_JIT_DLOAD");
     return e && *e ? (e[0] == '0' ? 0 : 1) : -1;
@@ -389,7 +389,10 @@ JitShape jit_shape(const PlannedSweep &ps, bool c64) {
   // The pipeline needs a first phase whose lanes cover the low tile bits (a
   // direct-load sweep) and runs of at least 16 bytes.
   // Warp 0 issues the copies: tiles of at least 2^9 amplitudes (32 threads).
-  const int st = jit_stages(c64);
+  // Multi-state sweeps reload the coefficients per state: always from
+  // shared memory, and no bulk-copy pipeline.
+  if (multi) j.smem_coef = true;
+  const int st = multi ? 0 : jit_stages(c64);
   if (st > 0 && (ps.h.flags & kDirectLoad) && ps.h.m >= 9u &&
       ((1u << ps.h.l) * (c64 ? 8u : 16u)) % 16u == 0) {
     j.stages = st;
@@ -401,14 +404,23 @@ JitShape jit_shape(const PlannedSweep &ps, bool c64) {
   return j;
 }
 
-std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
+// Source of the JIT kernel of one planned sweep.  multi: the multi-state
+// form sq_jit_msweep (one launch over K states sharing the sweep's
+// structure, coefficients per state); empty when the sweep remaps qubits
+// (not covered by that form).
+std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi) {
   const char *R = c64 ? "float" : "double";
   const int M = int(ps.h.m);
-  const JitShape js = jit_shape(ps, c64);
+  const JitShape js = jit_shape(ps, c64, multi);
+  if (multi && (ps.h.flags & kRemap)) return std::string();
   std::ostringstream s;
-  s << "extern \"C\" __global__ void __launch_bounds__(" << (1 << (M - kRegBits)) << ", " << minb
-    << ")\nsq_jit_sweep(Vec2<" << R << ">::T *__restrict__ psi, const __grid_constant__ SweepParams<"
-    << R << "> P, uint32_t *__restrict__ err) {\n";
+  if (multi)
+    s << "extern \"C\" __global__ void __launch_bounds__(" << (1 << (M - kRegBits)) << ", " << minb
+      << ")\nsq_jit_msweep(Vec2<" << R << ">::T *__restrict__ psi, const __grid_constant__ MultiParams Q) {\n";
+  else
+    s << "extern \"C\" __global__ void __launch_bounds__(" << (1 << (M - kRegBits)) << ", " << minb
+      << ")\nsq_jit_sweep(Vec2<" << R << ">::T *__restrict__ psi, const __grid_constant__ SweepParams<"
+      << R << "> P, uint32_t *__restrict__ err) {\n";
   s << "  using C2 = Vec2<" << R << ">::T;\n";
   s << "  using Tile = JitTile<" << M << ", " << ps.h.l;
   for (uint32_t i = 0; i < ps.h.m - ps.h.l; ++i) s << ", " << int(ps.h.hi[i]);
@@ -431,13 +443,21 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
   else if (js.early) {
     // The first phase's register load, shared by the loop's look-ahead.
     const SweepPhase &p0 = ps.ph[0];
-    s << "  (void)err;\n  using Ph0 = JitPhase<" << R << ", " << M << ", Tile, " << int(p0.reg[0]) << ", "
-      << int(p0.reg[1]) << ", " << int(p0.reg[2]) << ", " << int(p0.reg[3]);
+    s << (multi ? "" : "  (void)err;\n") << "  using Ph0 = JitPhase<" << R << ", " << M << ", Tile, "
+      << int(p0.reg[0]) << ", " << int(p0.reg[1]) << ", " << int(p0.reg[2]) << ", " << int(p0.reg[3]);
     for (int t : thread_positions(p0, M, c64, true)) s << ", " << t;
-    s << ">;\n  jit_sweep_early<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dstore)
-      << ", TileOut>(psi, P, [&](Amps<" << R << "> &A, uint64_t gb) { Ph0::load(A, psi, gb, Ph0::jb(threadIdx.x)); }, "
+    s << ">;\n";
+    if (multi)
+      s << "  jit_msweep_early<" << R << ", " << M << ", Tile, " << tf(js.dstore) << ">(psi, Q, ";
+    else
+      s << "  jit_sweep_early<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dstore)
+        << ", TileOut>(psi, P, ";
+    s << "[&](Amps<" << R << "> &A, uint64_t gb) { Ph0::load(A, psi, gb, Ph0::jb(threadIdx.x)); }, "
       << "[&](const Amps<" << R << "> &A0, C2 *tile, const C2 *coef, uint64_t gbase) {\n";
-  } else
+  } else if (multi)
+    s << "  jit_msweep<" << R << ", " << M << ", Tile, " << tf(js.dload) << ", " << tf(js.dstore)
+      << ">(psi, Q, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
+  else
     s << "  (void)err;\n  jit_sweep<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dload)
       << ", " << tf(js.dstore) << ", TileOut>(psi, P, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
   const uint32_t last = ps.h.nphases - 1;
@@ -475,7 +495,7 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
       std::string tmpl;
       op_routine(op, c64, tmpl);
       std::ostringstream cexpr;
-      if (lane_indexed(op))
+      if (multi || lane_indexed(op))
         cexpr << "coef + " << op.coef;
       else
         cexpr << "ParamCoef<" << R << ", " << op.coef << ">{P.coef}";
@@ -508,8 +528,8 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb) {
   return s.str();
 }
 
-std::string jit_source(const PlannedSweep &ps, bool c64, int minb) {
-  return prelude() + jit_body(ps, c64, minb);
+std::string jit_source(const PlannedSweep &ps, bool c64, int minb, bool multi) {
+  return prelude() + jit_body(ps, c64, minb, multi);
 }
 
 // Source of the JIT kernel of one reverse (two-state) adjoint sweep; empty
@@ -853,6 +873,17 @@ Entry &sweep_entry(const PlannedSweep &ps, bool c64) {
   return *e;
 }
 
+Entry *msweep_entry(const PlannedSweep &ps, bool c64) {
+  const PlanKey k = plan_key(ps, c64, 2);
+  bool found = false;
+  Entry *e = plan_lookup(k, &found);
+  if (found) return e;
+  const std::string body = jit_body(ps, c64, jit_minb(c64, ps.h.m), true);
+  e = body.empty() ? nullptr : &get_entry(body, "sq_jit_msweep");
+  plan_store(k, e);
+  return e;
+}
+
 const void *jit_adjoint_kernel(const PlannedSweep &ps, bool c64, std::string &err) {
   Entry *e = adjoint_entry(ps, c64);
   if (!e) {
@@ -920,6 +951,35 @@ const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err)
     return nullptr;
   }
   return reinterpret_cast<const void *>(e.kernel);
+}
+
+const void *jit_msweep_kernel(const PlannedSweep &ps, bool c64, std::string &err) {
+  Entry *e = msweep_entry(ps, c64);
+  if (!e) {
+    err = "sweep not covered by the multi-state JIT form";
+    return nullptr;
+  }
+  if (e->failed) {
+    err = e->err;
+    return nullptr;
+  }
+  return reinterpret_cast<const void *>(e->kernel);
+}
+
+size_t jit_msweep_smem(const PlannedSweep &ps, bool c64) {
+  const JitShape js = jit_shape(ps, c64, true);
+  return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload || js.early, (ps.h.ncoef + 1) & ~1u);
+}
+
+void jit_prepare_multi(const std::vector<const PlannedSweep *> &sweeps, bool c64) {
+  if (!jit_available() || sweeps.empty()) return;
+  std::vector<const PlannedSweep *> todo;
+  for (const auto *ps : sweeps) {
+    bool found = false;
+    plan_lookup(plan_key(*ps, c64, 2), &found);
+    if (!found) todo.push_back(ps);
+  }
+  prepare_parallel(todo, [&](const PlannedSweep &ps) { msweep_entry(ps, c64); });
 }
 
 void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64) {

@@ -10,10 +10,11 @@ namespace sq {
 bool jit_available();
 // Counts a sweep launch that ran a JIT kernel (true) or fell back (false).
 void jit_note_launch(bool jit);
-// CUDA source of the kernel specialised for `ps` (`minb` CTAs per SM).
-std::string jit_source(const PlannedSweep &ps, bool c64, int minb);
+// CUDA source of the kernel specialised for `ps` (`minb` CTAs per SM);
+// multi: its multi-state form (jit_msweep_kernel).
+std::string jit_source(const PlannedSweep &ps, bool c64, int minb, bool multi = false);
 // The part of that source that depends on `ps` (the cache key).
-std::string jit_body(const PlannedSweep &ps, bool c64, int minb);
+std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi = false);
 // Dynamic shared memory the JIT kernel of `ps` needs.
 size_t jit_smem(const PlannedSweep &ps, bool c64);
 // CTAs per SM the kernels of (precision, tile bits) are built for.
@@ -37,6 +38,12 @@ const void *jit_batch_adjoint_kernel(const unsigned char *plan, uint32_t nfwd, u
 std::string jit_batch_adjoint_body(const unsigned char *plan, uint32_t nfwd, uint32_t nrev, uint32_t n,
                                    uint32_t M, bool c64);
 std::string jit_batch_source(const std::string &body);
+// Multi-state sweeps (sq_jit_msweep: one launch applies the sweep to K states
+// that share its structure, sq::MultiParams): the kernel (or nullptr with
+// `err`), its dynamic shared memory, and a parallel pre-compile.
+const void *jit_msweep_kernel(const PlannedSweep &ps, bool c64, std::string &err);
+size_t jit_msweep_smem(const PlannedSweep &ps, bool c64);
+void jit_prepare_multi(const std::vector<const PlannedSweep *> &sweeps, bool c64);
 // Compiles the kernels of several sweeps in parallel (fills the cache).
 void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64);
 

@@ -305,6 +305,135 @@ __device__ __forceinline__ void jit_sweep(typename Vec2<Real>::T *__restrict__ p
 }
 
 // ---------------------------------------------------------------------------
+// Multi-state sweeps: one launch applies one sweep to K states of 2^n
+// amplitudes that share the sweep's structure (the circuits of a batch with
+// one plan structure and different angles).  The states lie back to back
+// (state c at psi + c 2^n), so together they form one index space whose bits
+// above n number the state: tile t of the launch is Tile::base(t), with
+// t >> tile_shift the state (tile_shift = n - M), and the ops' conditions on
+// global bits (all below n) hold per state.  State c's coefficients are the
+// ncoef complex values at coefs + c stride (bytes), i.e. the coefficient
+// block of this sweep's packed record in circuit c's plan.  Each CTA takes a
+// contiguous range of tiles, so it reloads the shared-memory copy of the
+// coefficients only when its range crosses into the next state.
+struct MultiParams {
+  const unsigned char *coefs;  // state 0's coefficients of this sweep
+  uint64_t stride;             // bytes between consecutive states' coefficients
+  uint64_t tiles;              // K << tile_shift
+  uint32_t tile_shift;         // log2 tiles per state
+  uint32_t ncoef;
+};
+
+template <typename Real>
+__device__ __forceinline__ void jit_multi_coef(typename Vec2<Real>::T *coef, const MultiParams &Q, uint64_t c) {
+  const auto *g = reinterpret_cast<const typename Vec2<Real>::T *>(Q.coefs + c * Q.stride);
+  for (uint32_t i = threadIdx.x; i < Q.ncoef; i += blockDim.x) coef[i] = g[i];
+}
+
+// This CTA's tiles [t0, t1): an equal share of the launch's tiles.
+__device__ __forceinline__ void jit_multi_range(const MultiParams &Q, uint64_t &t0, uint64_t &t1) {
+  const uint64_t per = (Q.tiles + gridDim.x - 1) / gridDim.x;
+  t0 = uint64_t(blockIdx.x) * per;
+  t1 = t0 + per < Q.tiles ? t0 + per : Q.tiles;
+}
+
+// jit_sweep_early over the tiles of K states (coefficients always in shared
+// memory).
+template <typename Real, int M, class Tile, bool DSTORE, class Load0, class Phases>
+__device__ __forceinline__ void jit_msweep_early(typename Vec2<Real>::T *__restrict__ psi, const MultiParams &Q,
+                                                 Load0 load0, Phases phases) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int NT = 1 << (M - kRegBits);
+  constexpr uint32_t TS = 1u << M;
+  constexpr uint32_t PER = TS / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *tile = reinterpret_cast<C2 *>(smem_raw);
+  C2 *coef = tile + TS;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t s_tid = swz<Real>(tid);
+  const uint64_t toff = Tile::off(tid);
+  uint64_t t0, t1;
+  jit_multi_range(Q, t0, t1);
+  uint64_t cur_c = ~uint64_t(0);
+  Amps<Real> next;
+  if (t0 < t1) load0(next, Tile::base(t0));
+  for (uint64_t t = t0; t < t1; ++t) {
+    const Amps<Real> cur = next;
+    if (t + 1 < t1) load0(next, Tile::base(t + 1));
+    const uint64_t c = t >> Q.tile_shift;
+    if (c != cur_c) {  // uniform: the previous tile ended with a barrier
+      jit_multi_coef<Real>(coef, Q, c);
+      cur_c = c;
+      __syncthreads();
+    }
+    const uint64_t gbase = Tile::base(t);
+    phases(cur, tile, coef, gbase);
+    if constexpr (!DSTORE) {
+#pragma unroll
+      for (uint32_t it = 0; it < PER; ++it)
+        psi[gbase | toff | Tile::off(it * NT)] = tile[s_tid ^ swz<Real>(it * NT)];
+    }
+    __syncthreads();
+  }
+}
+
+// jit_sweep over the tiles of K states (coefficients always in shared
+// memory; the first phase loads from HBM itself when DLOAD, else the next
+// tile streams into a second buffer by cp.async).
+template <typename Real, int M, class Tile, bool DLOAD, bool DSTORE, class Phases>
+__device__ __forceinline__ void jit_msweep(typename Vec2<Real>::T *__restrict__ psi, const MultiParams &Q,
+                                           Phases phases) {
+  using C2 = typename Vec2<Real>::T;
+  constexpr int NT = 1 << (M - kRegBits);
+  constexpr uint32_t TS = 1u << M;
+  constexpr uint32_t PER = TS / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *bufs = reinterpret_cast<C2 *>(smem_raw);
+  C2 *coef = bufs + (DLOAD ? 1 : 2) * TS;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t s_tid = swz<Real>(tid);
+  const uint64_t toff = Tile::off(tid);
+  uint64_t t0, t1;
+  jit_multi_range(Q, t0, t1);
+  uint64_t cur_c = ~uint64_t(0);
+  auto prefetch = [&](uint64_t t, C2 *dst) {
+    const C2 *src = psi + (Tile::base(t) | toff);
+#pragma unroll
+    for (uint32_t it = 0; it < PER; ++it)
+      cp_async<sizeof(C2)>(dst + (s_tid ^ swz<Real>(it * NT)), src + Tile::off(it * NT));
+  };
+  uint32_t cur = 0;
+  if constexpr (!DLOAD) {
+    if (t0 < t1) prefetch(t0, bufs);
+    cp_async_commit();
+  }
+  for (uint64_t t = t0; t < t1; ++t) {
+    C2 *tile = bufs + (DLOAD ? 0 : cur * TS);
+    if constexpr (!DLOAD) {
+      if (t + 1 < t1) prefetch(t + 1, bufs + (cur ^ 1) * TS);
+      cp_async_commit();
+    }
+    const uint64_t c = t >> Q.tile_shift;
+    if (c != cur_c) {
+      jit_multi_coef<Real>(coef, Q, c);
+      cur_c = c;
+    }
+    if constexpr (!DLOAD) cp_async_wait_prev();
+    __syncthreads();
+    const uint64_t gbase = Tile::base(t);
+    phases(tile, coef, gbase);
+    if constexpr (!DSTORE) {
+#pragma unroll
+      for (uint32_t it = 0; it < PER; ++it)
+        psi[gbase | toff | Tile::off(it * NT)] = tile[s_tid ^ swz<Real>(it * NT)];
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  if constexpr (!DLOAD) asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
 // Bulk-copy tile pipeline (cp.async.bulk with mbarrier transaction counts).
 //
 // A sweep whose first phase reads its amplitudes with the lanes on the low

@@ -182,3 +182,16 @@ def test_alternative_tile_loops_compile(env):
     r = subprocess.run([sys.executable, "-c", code], env={**os.environ, k: v, "SQ_JIT_DLOAD": "1"},
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("dtype,n", [(capi.SQ_C128, 16), (capi.SQ_C64, 14)])
+def test_multi_state_sources_compile(dtype, n):
+    """The multi-state kernels of a batch energy plan (one launch per sweep
+    over every state of a structure group) compile; coefficients come from
+    the shared-memory copy of each state's block."""
+    ops = circuits.vqe_ansatz(n, np.random.default_rng(n).uniform(0, 2 * np.pi, 12 * n))
+    srcs = capi.jit_sources(n, ops, dtype, multi=True)
+    assert srcs and all("sq_jit_msweep" in s and "MultiParams Q" in s for s in srcs)
+    assert not any("ParamCoef<" in s.split("sq_jit_msweep")[1] for s in srcs)
+    for s in srcs[:2]:
+        capi.jit_compile(s)
