@@ -649,11 +649,20 @@ def adjoint_metric(precision: str):
         e, g = adjoint.adjoint_gradient(ws, ops, theta, terms, 2 * p)
     t_adj = (time.perf_counter() - t0) / reps
     sweeps = (ws.psi.launches() - l0) / reps
-    # Forward sweeps alone (the rest of the launches are reverse sweeps).
+    # Device time of the sweeps of one gradient (CUDA events around every
+    # forward and reverse sweep launch), then of the forward sweeps alone.
+    torch.cuda.synchronize()
+    ws.psi.sweep_timing()
+    ws.psi.set_option(capi.SQ_OPT_TIMING, 1)
+    adjoint.adjoint_gradient(ws, ops, theta, terms, 2 * p)
+    grad_sweep_ms, _ = ws.psi.sweep_timing()
     l0 = ws.psi.launches()
     adjoint.energy(ws.psi, ops, theta, terms)
     fwd = ws.psi.launches() - l0
+    fwd_ms, _ = ws.psi.sweep_timing()
+    ws.psi.set_option(capi.SQ_OPT_TIMING, 0)
     rev = sweeps - fwd
+    rev_ms = grad_sweep_ms - fwd_ms
     # Algorithmic HBM bytes: forward sweeps read+write psi; lambda = H psi
     # reads psi and writes lambda (one Pauli flip group for MaxCut); every
     # reverse sweep reads and writes both states.
@@ -671,6 +680,11 @@ def adjoint_metric(precision: str):
             "gate_occurrences": evals // 2, "energy": e,
             "adjoint_ms": round(t_adj * 1e3, 3), "adjoint_grads_per_s": round(1.0 / t_adj, 3),
             "forward_sweeps": fwd, "reverse_sweeps": rev,
+            "forward_sweeps_ms": round(fwd_ms, 3), "reverse_sweeps_ms": round(rev_ms, 3),
+            "reverse_sweep_frac": round(4 * amp * (1 << n) * rev / (rev_ms * 1e-3) / 1e9 / peak, 4)
+            if rev_ms > 0 else None,
+            "forward_sweep_frac": round(2 * amp * (1 << n) * fwd / (fwd_ms * 1e-3) / 1e9 / peak, 4)
+            if fwd_ms > 0 else None,
             "roofline": {"bound": "hbm", "achieved": round(alg / t_adj / 1e9, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(alg / t_adj / 1e9 / peak, 4),
                          "algorithmic_bytes": alg, "peak_source": peak_kind,

@@ -162,7 +162,8 @@ int sq_pending(const sq_state *s, uint32_t *count);
 int sq_launch_count(const sq_state *s, uint64_t *count);
 /* With SQ_OPT_TIMING on: total device time (ms) and number of the fused-sweep
  * launches recorded since the last call (synchronises on the recorded
- * events, then clears them). */
+ * events, then clears them).  The reverse two-state sweeps of
+ * sq_adjoint_gradient are recorded on its psi state. */
 int sq_sweep_timing(sq_state *s, double *total_ms, uint64_t *launches);
 /* JIT-specialised sweeps, process-wide: whether NVRTC could be loaded, and
  * how many sweeps ran a JIT kernel / fell back to the generic kernel. */

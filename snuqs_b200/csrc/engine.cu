@@ -1228,7 +1228,17 @@ int adjoint_sweep(sq_state *psi, sq_state *lam, const sq::PlannedSweep &ps, doub
   C2 *a = static_cast<C2 *>(psi->data);
   C2 *b = static_cast<C2 *>(lam->data);
   void *args[] = {&a, &b, P.get(), &partials};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (psi->timing) {
+    SQ_CUDA(cudaEventCreate(&e0));
+    SQ_CUDA(cudaEventCreate(&e1));
+    SQ_CUDA(cudaEventRecord(e0, st));
+  }
   SQ_CUDA(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(threads), args, smem, st));
+  if (psi->timing) {
+    SQ_CUDA(cudaEventRecord(e1, st));
+    psi->sweep_events.emplace_back(e0, e1);
+  }
   psi->launches++;
   if (!ps.inner_global.empty()) {
     sq::InnerSlots S;
