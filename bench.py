@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--tile-bits", type=int, default=0, help="override the engine's tile size")
     p.add_argument("--low-bits", type=int, default=0,
                    help="override the contiguous low bits of every tile")
+    p.add_argument("--adjoint-only", action="store_true",
+                   help="only the QAOA-26 adjoint gradient, without the parameter-shift comparison "
+                        "(a short command for profiling the adjoint kernels)")
     p.add_argument("--kernel-tour", action="store_true",
                    help="run each kernel family once on a small case (for ncu captures) "
                         "instead of the benchmark line")
@@ -347,6 +350,9 @@ def main():
     if args.kernel_tour:
         kernel_tour()
         return
+    if args.adjoint_only:
+        print(json.dumps(adjoint_metric(args.precision, shift=False)))
+        return
     if args.op_cost:
         op_cost(args)
         return
@@ -626,10 +632,11 @@ def qaoa_workload(n=26, p=8, seed=SEED):
     return ops, circuits.maxcut_hamiltonian(n, edges), theta
 
 
-def adjoint_metric(precision: str):
+def adjoint_metric(precision: str, shift: bool = True):
     """Adjoint gradient (one forward + one fused reverse pass) against the
     parameter-shift rule on the same engine, QAOA MaxCut 26 qubits p = 8:
-    the full 1040-evaluation shift gradient is computed and compared."""
+    the full 1040-evaluation shift gradient is computed and compared
+    (shift=False: the adjoint gradient alone)."""
     import torch
 
     from snuqs_b200 import adjoint, capi
@@ -655,31 +662,31 @@ def adjoint_metric(precision: str):
     ws.psi.sweep_timing()
     ws.psi.set_option(capi.SQ_OPT_TIMING, 1)
     adjoint.adjoint_gradient(ws, ops, theta, terms, 2 * p)
-    grad_sweep_ms, _ = ws.psi.sweep_timing()
-    l0 = ws.psi.launches()
+    grad_sweep_ms, grad_sweeps = ws.psi.sweep_timing()
     adjoint.energy(ws.psi, ops, theta, terms)
-    fwd = ws.psi.launches() - l0
-    fwd_ms, _ = ws.psi.sweep_timing()
+    fwd_ms, fwd = ws.psi.sweep_timing()
     ws.psi.set_option(capi.SQ_OPT_TIMING, 0)
-    rev = sweeps - fwd
+    rev = grad_sweeps - fwd
     rev_ms = grad_sweep_ms - fwd_ms
     # Algorithmic HBM bytes: forward sweeps read+write psi; lambda = H psi
     # reads psi and writes lambda (one Pauli flip group for MaxCut); every
-    # reverse sweep reads and writes both states.
+    # reverse sweep reads and writes both states.  (launches per gradient also
+    # count lambda = H psi and the energy reduction.)
     alg = (2 * fwd + 2 + 4 * rev) * amp * (1 << n)
     peak, peak_kind = measured_peak()
     # The full parameter-shift gradient (2 evaluations per gate occurrence).
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    g_shift = adjoint.parameter_shift_gradient(ws.psi, ops, theta, terms, 2 * p)
-    t_shift = time.perf_counter() - t0
     evals = done = adjoint.count_shift_evaluations(ops)
+    if shift:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g_shift = adjoint.parameter_shift_gradient(ws.psi, ops, theta, terms, 2 * p)
+        t_shift = time.perf_counter() - t0
+        diff = float(np.abs(np.asarray(g) - np.asarray(g_shift)).max())
     ws.close()
-    diff = float(np.abs(np.asarray(g) - np.asarray(g_shift)).max())
-    return {"workload": f"qaoa_maxcut_{n}q_p{p}_{precision}", "params": 2 * p,
+    out = {"workload": f"qaoa_maxcut_{n}q_p{p}_{precision}", "params": 2 * p,
             "gate_occurrences": evals // 2, "energy": e,
             "adjoint_ms": round(t_adj * 1e3, 3), "adjoint_grads_per_s": round(1.0 / t_adj, 3),
-            "forward_sweeps": fwd, "reverse_sweeps": rev,
+            "launches_per_gradient": sweeps, "forward_sweeps": fwd, "reverse_sweeps": rev,
             "forward_sweeps_ms": round(fwd_ms, 3), "reverse_sweeps_ms": round(rev_ms, 3),
             "reverse_sweep_frac": round(4 * amp * (1 << n) * rev / (rev_ms * 1e-3) / 1e9 / peak, 4)
             if rev_ms > 0 else None,
@@ -689,14 +696,19 @@ def adjoint_metric(precision: str):
                          "unit": "GB/s", "frac": round(alg / t_adj / 1e9 / peak, 4),
                          "algorithmic_bytes": alg, "peak_source": peak_kind,
                          "note": "whole gradient (host wall clock) over its algorithmic bytes"},
-            "param_shift_evals_per_grad": evals, "param_shift_evals_done": done,
-            "param_shift_ms": round(t_shift * 1e3, 1),
-            "param_shift_grads_per_s": round(1.0 / t_shift, 4),
-            "speedup_vs_param_shift": round(t_shift / t_adj, 1),
-            "max_abs_adjoint_minus_shift": diff,
-            "tolerance": 1e-10 if dtype == capi.SQ_C128 else 1e-4,
-            "timing": "host wall clock around synchronous calls; the parameter-shift gradient is "
-                      "computed in full (every shifted evaluation) and compared with the adjoint one"}
+           "timing": "host wall clock around synchronous calls; sweep times are CUDA events around "
+                     "each sweep launch"}
+    if shift:
+        out.update({"param_shift_evals_per_grad": evals, "param_shift_evals_done": done,
+                    "param_shift_ms": round(t_shift * 1e3, 1),
+                    "param_shift_grads_per_s": round(1.0 / t_shift, 4),
+                    "speedup_vs_param_shift": round(t_shift / t_adj, 1),
+                    "max_abs_adjoint_minus_shift": diff,
+                    "tolerance": 1e-10 if dtype == capi.SQ_C128 else 1e-4,
+                    "timing": "host wall clock around synchronous calls; the parameter-shift gradient "
+                              "is computed in full (every shifted evaluation) and compared with the "
+                              "adjoint one; sweep times are CUDA events around each sweep launch"})
+    return out
 
 
 def vqe_batch_circuits(ncirc: int = 4096, seed: int = SEED):

@@ -334,6 +334,31 @@ bool lane_indexed(const SweepOp &op) {
   return false;
 }
 
+// Call of the inner-product routine of a kSwInnerDiag / kSwInnerDense op
+// (`bits`: the statement that sets b, the op's non-register target bits),
+// accumulating into doubles sr, si.  Pauli-form ops (kAuxPauli) take the
+// four-FMA-per-amplitude routines.
+std::string inner_call(const SweepOp &op, const char *R, const std::string &bits) {
+  std::ostringstream s;
+  const bool pauli = op.aux & kAuxPauli;
+  if (op.kind == kSwInnerDiag) {
+    s << bits << " ";
+    if (pauli)
+      s << "inner_diag_pauli<" << R << ", " << int(op.vmask) << ", " << int(op.aux & 7) << ">";
+    else
+      s << "inner_diag<" << R << ", " << int(op.vmask) << ">";
+    s << "(F, G, coef + " << op.coef << ", b, sr, si); ";
+  } else {
+    if (pauli)
+      s << "inner_dense_pauli<" << R << ", " << int(op.vmask) << ", " << int(op.aux & 7) << ", "
+        << int((op.aux >> 3) & 7) << ">";
+    else
+      s << "inner_dense<" << R << ", " << int(op.vmask) << ">";
+    s << "(F, G, coef + " << op.coef << ", sr, si); ";
+  }
+  return s.str();
+}
+
 struct JitShape {
   bool smem_coef = false, dload = false, dstore = false;
   int stages = 0;     // > 0: bulk-copy pipeline with this many tiles in flight per CTA
@@ -574,13 +599,8 @@ std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb) {
       if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
         // Inner products carry no conditions (as in the generic kernel).
         if (op.gmask || op.lmask || op.rmask || op.slot >= uint32_t(kMaxInner)) return std::string();
-        s << "      { double sr = 0.0, si = 0.0; ";
-        if (op.kind == kSwInnerDiag)
-          s << diag_bits(op) << " inner_diag<" << R << ", " << int(op.vmask) << ">(F, G, coef + " << op.coef
-            << ", b, sr, si); ";
-        else
-          s << "inner_dense<" << R << ", " << int(op.vmask) << ">(F, G, coef + " << op.coef << ", sr, si); ";
-        s << "jit_inner_acc<" << NT << ", " << op.slot << ">(acc, sr, si); }\n";
+        s << "      { double sr = 0.0, si = 0.0; " << inner_call(op, R, diag_bits(op)) << "jit_inner_acc<" << NT
+          << ", " << op.slot << ">(acc, sr, si); }\n";
         continue;
       }
       s << "      ";
@@ -594,11 +614,12 @@ std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb) {
       }
       std::string tmpl;
       op_routine(op, c64, tmpl, kAdjAmps);
+      // Coefficients from the shared-memory copy: read from the parameter
+      // block, the compiler keeps every coefficient of the sweep in registers
+      // across the tile loop (255 registers and spills for a QAOA sweep,
+      // 160-165 without spills from shared memory at 3 CTAs per SM).
       std::ostringstream cexpr;
-      if (lane_indexed(op))
-        cexpr << "coef + " << op.coef;
-      else
-        cexpr << "ParamCoef<" << R << ", " << op.coef << ">{P.coef}";
+      cexpr << "coef + " << op.coef;
       if (op.kind == kSwDiag) {
         s << "{ " << diag_bits(op) << " " << tmpl << "(F, " << cexpr.str() << ", b); " << tmpl << "(G, "
           << cexpr.str() << ", b); }\n";
@@ -721,13 +742,8 @@ std::string jit_batch_adjoint_body(const unsigned char *plan, uint32_t nfwd, uin
           const SweepOp &op = ops[oi];
           if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
             if (op.gmask || op.lmask || op.rmask || op.slot >= uint32_t(kMaxInner)) return std::string();
-            fns << "      { double sr = 0.0, si = 0.0; ";
-            if (op.kind == kSwInnerDiag)
-              fns << diag_bits_src(op) << " inner_diag<" << R << ", " << int(op.vmask) << ">(F, G, coef + "
-                  << op.coef << ", b, sr, si); ";
-            else
-              fns << "inner_dense<" << R << ", " << int(op.vmask) << ">(F, G, coef + " << op.coef << ", sr, si); ";
-            fns << "jit_inner_acc<" << NT << ", " << op.slot << ">(acc, sr, si); }\n";
+            fns << "      { double sr = 0.0, si = 0.0; " << inner_call(op, R, diag_bits_src(op)) << "jit_inner_acc<"
+                << NT << ", " << op.slot << ">(acc, sr, si); }\n";
             continue;
           }
           std::string tmpl;
@@ -852,12 +868,17 @@ void plan_store(const PlanKey &k, Entry *e) {
   g_plan_entries[k] = e;
 }
 
+// CTAs per SM of the two-state (reverse) JIT sweeps: complex128 fits 3
+// (160-165 registers, 68 KB of shared memory per CTA for 2^10-amplitude
+// tiles); complex64 (2^11 tiles, 256 threads) 2.
+int jit_adjoint_minb(bool c64) { return c64 ? 2 : 3; }
+
 Entry *adjoint_entry(const PlannedSweep &ps, bool c64) {
   const PlanKey k = plan_key(ps, c64, 1);
   bool found = false;
   Entry *e = plan_lookup(k, &found);
   if (found) return e;
-  const std::string body = jit_adjoint_body(ps, c64, 2);
+  const std::string body = jit_adjoint_body(ps, c64, jit_adjoint_minb(c64));
   e = body.empty() ? nullptr : &get_entry(body, "sq_jit_adjoint");
   plan_store(k, e);
   return e;
@@ -1079,7 +1100,7 @@ extern "C" int sq_jit_adjoint_source(uint32_t num_qubits, int dtype, const sq_ci
     if (pl.is_sweep) sweeps.push_back(&pl.sweep);
   if (nsweeps) *nsweeps = uint32_t(sweeps.size());
   if (sweep_index >= sweeps.size()) return sq_detail_fail(SQ_ERR_INVALID, "no such sweep");
-  const std::string body = sq::jit_adjoint_body(*sweeps[sweep_index], c64, 2);
+  const std::string body = sq::jit_adjoint_body(*sweeps[sweep_index], c64, sq::jit_adjoint_minb(c64));
   const std::string src = body.empty() ? std::string() : sq::prelude() + body;
   *len = src.size();
   if (buf && cap) {

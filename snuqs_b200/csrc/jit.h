@@ -28,6 +28,7 @@ const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err)
 const void *jit_adjoint_kernel(const PlannedSweep &ps, bool c64, std::string &err);
 size_t jit_adjoint_smem(const PlannedSweep &ps, bool c64);
 std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb);
+int jit_adjoint_minb(bool c64);
 void jit_prepare_adjoint(const std::vector<const PlannedSweep *> &sweeps, bool c64);
 // Batched gradients of circuits that share one packed plan structure
 // (`plan`: one circuit's packed records, nfwd forward then nrev reverse

@@ -88,6 +88,31 @@ int rank_in(uint64_t mask, int b) { return popc64(mask & ((uint64_t(1) << b) - 1
 
 // Picks the cheapest sweep-op kind for a dense k-qubit matrix in canonical
 // order and appends its coefficients.
+// Pauli form of an inner-product op's K (canonical local order): K = alpha P
+// with P_(r, r^x) = (-1)^popc(r & z) times K's row-0 entry in column x and
+// every other entry zero, each to within 1e-14 |alpha| (rotation generators
+// computed as dU/da U^dagger carry rounding of that size).  d: dimension;
+// diag: K holds only the d diagonal entries.
+bool pauli_form(const cplx *K, int d, bool diag, uint32_t &x, uint32_t &z) {
+  x = 0;
+  if (!diag)
+    for (int c = 1; c < d; ++c)
+      if (std::abs(K[c]) > std::abs(K[x])) x = uint32_t(c);
+  const cplx a = diag ? K[0] : K[x];
+  const double tol = 1e-14 * std::abs(a);
+  if (std::abs(a) == 0.0) return false;
+  auto at = [&](int r, int c) { return diag ? (r == c ? K[r] : cplx(0, 0)) : K[size_t(r) * d + c]; };
+  z = 0;
+  for (int j = 0; (1 << j) < d; ++j)
+    if (std::abs(at(1 << j, (1 << j) ^ int(x)) + a) <= tol) z |= 1u << j;
+  for (int r = 0; r < d; ++r)
+    for (int c = 0; c < d; ++c) {
+      const cplx want = c == (r ^ int(x)) ? ((__builtin_popcount(uint32_t(r) & z) & 1) ? -a : a) : cplx(0, 0);
+      if (std::abs(at(r, c) - want) > tol) return false;
+    }
+  return true;
+}
+
 void encode_dense(SweepOp &so, const std::vector<cplx> &cm, int k, std::vector<cplx> &coef) {
   const int d = 1 << k;
   auto M = [&](int r, int c) { return cm[size_t(r) * d + c]; };
@@ -287,6 +312,9 @@ PlannedSweep SweepBuilder::finish() const {
               if ((x >> (k - 1 - t)) & 1) y |= size_t(1) << newbit[t];
             cd[y] = op.m[x];
           }
+          uint32_t px = 0, pz = 0;
+          if (op.kind == kOpInner && k <= 3 && pauli_form(cd.data(), int(cd.size()), true, px, pz))
+            so.aux = uint8_t(kAuxPauli | pz);
           ps.coef.insert(ps.coef.end(), cd.begin(), cd.end());
         }
       } else {
@@ -318,6 +346,8 @@ PlannedSweep SweepBuilder::finish() const {
           so.kind = kSwInnerDense;
           so.slot = uint32_t(ps.inner_global.size());
           ps.inner_global.push_back(op.slot);
+          uint32_t px = 0, pz = 0;
+          if (k <= 3 && pauli_form(cm.data(), d, false, px, pz)) so.aux = uint8_t(kAuxPauli | px | (pz << 3));
           ps.coef.insert(ps.coef.end(), cm.begin(), cm.end());
         } else {
           encode_dense(so, cm, k, ps.coef);

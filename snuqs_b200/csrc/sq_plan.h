@@ -50,6 +50,12 @@ enum SweepAux : uint8_t {
   kAuxXMask = 3,  // XRot: partner XOR mask over the op's canonical local bits
   kAuxImag = 4,   // XRot: f = i
   kAuxPure = 8,   // Anti1/Swap2: unit phases (pure permutation); Phase: p = -1
+  // kSwInnerDiag / kSwInnerDense: K = alpha P for one Pauli string P = X^x Z^z
+  // over the op's canonical local bits (up to a phase folded into alpha):
+  // bits 0-2 x, bits 3-5 z (diagonal: bits 0-2 z).  The full K coefficients
+  // stay in place (the generic kernels use them); alpha is K's row-0 entry in
+  // column x.
+  kAuxPauli = 128,
 };
 enum DiagSrc : uint8_t { kSrcGlobal = 0, kSrcLocal = 1, kSrcReg = 2 };
 

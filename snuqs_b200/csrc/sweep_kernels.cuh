@@ -562,6 +562,70 @@ __device__ __forceinline__ void inner_dense(const Amps<Real, kAdjAmps> &F, const
   }
 }
 
+// Inner products of ops flagged kAuxPauli, K = alpha P with P a Pauli string
+// over the op's canonical local bits (the generator of a rotation gate):
+// (K phi)_r = alpha (-1)^popc(r & Z) phi_(r ^ X), alpha = c[X] (row 0).  Four
+// FMAs per amplitude instead of a dense K phi.
+//
+// Diagonal form (X = 0): canonical index (b << popc(V)) | ext_V(ri) as for
+// inner_diag; Z over those bits.
+template <typename Real, int V, int Z>
+__device__ __forceinline__ void inner_diag_pauli(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                                 const typename Vec2<Real>::T *__restrict__ c, uint32_t b,
+                                                 double &sr, double &si) {
+  double pr = 0.0, pi = 0.0, mr = 0.0, mi = 0.0;
+#pragma unroll
+  for (int ri = 0; ri < kAdjAmps; ++ri) {
+    const double gr = double(G.re[ri]), gi = double(G.im[ri]);
+    const double fr = double(F.re[ri]), fi = double(F.im[ri]);
+    if (__popc(uint32_t(ct_ext<V>(ri) & Z)) & 1) {
+      mr = fma(gr, fr, fma(gi, fi, mr));
+      mi = fma(gr, fi, fma(-gi, fr, mi));
+    } else {
+      pr = fma(gr, fr, fma(gi, fi, pr));
+      pi = fma(gr, fi, fma(-gi, fr, pi));
+    }
+  }
+  double qr = pr - mr, qi = pi - mi;
+  if (__popc(b & uint32_t(Z >> ct_popc<V>())) & 1) {
+    qr = -qr;
+    qi = -qi;
+  }
+  const auto a = c[0];
+  sr += double(a.x) * qr - double(a.y) * qi;
+  si += double(a.x) * qi + double(a.y) * qr;
+}
+
+// Dense form: register targets V, canonical local index r, partner r ^ X.
+template <typename Real, int V, int X, int Z>
+__device__ __forceinline__ void inner_dense_pauli(const Amps<Real, kAdjAmps> &F, const Amps<Real, kAdjAmps> &G,
+                                                  const typename Vec2<Real>::T *__restrict__ c, double &sr,
+                                                  double &si) {
+  constexpr int D = 1 << ct_popc<V>();
+  double pr = 0.0, pi = 0.0, mr = 0.0, mi = 0.0;
+#pragma unroll
+  for (int g = 0; g < kAdjAmps; ++g) {
+    if (g & V) continue;
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+      const int ir = g | ct_dep<V>(r), ix = g | ct_dep<V>(r ^ X);
+      const double gr = double(G.re[ir]), gi = double(G.im[ir]);
+      const double fr = double(F.re[ix]), fi = double(F.im[ix]);
+      if (__popc(uint32_t(r & Z)) & 1) {
+        mr = fma(gr, fr, fma(gi, fi, mr));
+        mi = fma(gr, fi, fma(-gi, fr, mi));
+      } else {
+        pr = fma(gr, fr, fma(gi, fi, pr));
+        pi = fma(gr, fi, fma(-gi, fr, pi));
+      }
+    }
+  }
+  const double qr = pr - mr, qi = pi - mi;
+  const auto a = c[X];
+  sr += double(a.x) * qr - double(a.y) * qi;
+  si += double(a.x) * qi + double(a.y) * qr;
+}
+
 // ---------------------------------------------------------------------------
 // Unfused gate: one thread per group of 2^k amplitudes (k <= 4), 64-bit
 // grid-stride loop.  Only groups whose target bits are zero are enumerated,

@@ -142,6 +142,25 @@ def test_adjoint_sources_compile(dtype):
     assert compiled > 0
 
 
+def test_adjoint_inner_products_take_the_pauli_form():
+    """Rotation generators (RotX: X, ZZ: Z x Z, RotY: Y) are single Pauli
+    strings: their inner products use the four-FMA routines; PhaseShift's
+    generator (I - Z)/2 is not and keeps the general routine.  Coefficients of
+    the reverse sweeps come from shared memory (no parameter-block reads)."""
+    srcs = capi.jit_sources(20, _qaoa(20, 1, seed=2), capi.SQ_C128, adjoint=True)
+    body = "".join(s.split("sq_jit_adjoint(")[1] for s in srcs if s)
+    assert "inner_dense_pauli<" in body and "inner_diag_pauli<" in body
+    assert "inner_dense<" not in body and "inner_diag<" not in body
+    assert "ParamCoef<" not in body
+    ops = [("Hadamard", (q,), ()) for q in range(20)]
+    ops += [("PhaseShift", (q,), (0.2,), (0,)) for q in range(20)]
+    ops += [("RotY", (q,), (0.4,), (1,)) for q in range(20)]
+    srcs = capi.jit_sources(20, ops, capi.SQ_C128, adjoint=True)
+    body = "".join(s.split("sq_jit_adjoint(")[1] for s in srcs if s)
+    assert "inner_diag<" in body and "inner_dense_pauli<" in body
+    capi.jit_compile(next(s for s in srcs if s))
+
+
 @pytest.mark.parametrize("dtype,n", [(capi.SQ_C128, 14)])
 def test_batch_adjoint_source_compiles(dtype, n):
     from snuqs_b200 import adjoint
