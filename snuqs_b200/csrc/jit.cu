@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <sstream>
@@ -359,6 +360,327 @@ std::string inner_call(const SweepOp &op, const char *R, const std::string &bits
   return s.str();
 }
 
+// Fused code for a run of consecutive diagonal ops of one phase (kSwDiag,
+// kSwPhase): instead of one complex multiply per amplitude per op, the run's
+// factors are multiplied together first and applied once.  Each op's factor
+// depends on its register bits V (plus per-thread bits: non-register targets,
+// conditions): ops with V = 0 fold into a scalar, ops with the same V into a
+// table of 2^|V| entries, and the tables combine into one table T over the
+// union U of their register bits, grown one table at a time (2^|U'| products
+// each); then every amplitude is multiplied by its T entry.  `coef(op)` is
+// the op's coefficient accessor; `na` amplitudes per thread.
+namespace {
+
+int bit_ext(int x, int mask) {  // bits of x at mask's positions, packed
+  int y = 0, k = 0;
+  for (int b = 0; b < 8; ++b)
+    if ((mask >> b) & 1) y |= ((x >> b) & 1) << k++;
+  return y;
+}
+
+int bit_dep(int y, int mask) {  // y's bits deposited at mask's positions
+  int x = 0, k = 0;
+  for (int b = 0; b < 8; ++b)
+    if ((mask >> b) & 1) x |= ((y >> k++) & 1) << b;
+  return x;
+}
+
+std::string cond_prefix(const SweepOp &op) {
+  if (!op.gmask && !op.lmask) return std::string();
+  std::ostringstream s;
+  s << "if (";
+  if (op.gmask) s << "(gbase & 0x" << std::hex << op.gmask << "ull) == 0x" << op.gval << "ull" << std::dec;
+  if (op.gmask && op.lmask) s << " && ";
+  if (op.lmask) s << "(jb & 0x" << std::hex << op.lmask << "u) == 0x" << op.lval << "u" << std::dec;
+  s << ") ";
+  return s.str();
+}
+
+std::string diag_bits_src(const SweepOp &op) {
+  std::ostringstream b;
+  b << "uint32_t b = 0;";
+  for (int t = 0; t < op.ndt; ++t) {
+    if (op.dsrc[t] == kSrcGlobal)
+      b << " b = (b << 1) | (uint32_t(gbase >> " << int(op.dpos[t]) << ") & 1u);";
+    else
+      b << " b = (b << 1) | ((jb >> " << int(op.dpos[t]) << ") & 1u);";
+  }
+  return b.str();
+}
+
+std::string nonreg_cond(const SweepOp &op) {
+  std::ostringstream c;
+  c << "true";
+  if (op.gmask) c << " && (gbase & 0x" << std::hex << op.gmask << "ull) == 0x" << op.gval << "ull" << std::dec;
+  if (op.lmask) c << " && (jb & 0x" << std::hex << op.lmask << "u) == 0x" << op.lval << "u" << std::dec;
+  return c.str();
+}
+
+}  // namespace
+
+// Diagonal runs are fused unless SQ_JIT_FUSE_DIAG=0.
+bool jit_fuse_diag() {
+  static const bool on = [] {
+    const char *e = std::getenv("SQ_JIT_FUSE_DIAG");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// An op a fused diagonal run may hold: a diagonal op without conditions, or
+// a conditional phase.
+bool fusable_diag(const SweepOp &op) {
+  return (op.kind == kSwDiag && !op.gmask && !op.lmask && !op.rmask) || op.kind == kSwPhase;
+}
+
+// Emission order of one phase's ops: single ops, and runs of diagonal ops
+// to fuse.  A diagonal op moves later past the non-diagonal ops it commutes
+// with (their targets miss its register bits: conditions are diagonal), so
+// the diagonal ops between such ops gather into one run; the order among
+// diagonal ops and among the others is kept.
+std::vector<std::vector<uint32_t>> phase_items(const SweepOp *ops, const SweepPhase &ph, bool two_state = false) {
+  std::vector<std::vector<uint32_t>> items;
+  std::vector<uint32_t> pending;
+  uint32_t pending_bits = 0;
+  auto flush = [&] {
+    if (pending.size() >= 2) {
+      items.push_back(pending);
+    } else {
+      for (uint32_t i : pending) items.push_back({i});
+    }
+    pending.clear();
+    pending_bits = 0;
+  };
+  for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
+    const SweepOp &op = ops[oi];
+    // Two-state sweeps: the inner products of diagonal generators join the
+    // runs too (they commute with every diagonal op).
+    if (jit_fuse_diag() && (fusable_diag(op) || (two_state && op.kind == kSwInnerDiag))) {
+      pending.push_back(oi);
+      pending_bits |= op.kind == kSwPhase ? op.rmask : op.vmask;
+      continue;
+    }
+    // An op moves ahead of the pending run when the run's diagonal ops (and
+    // the generators of its inner products) commute with it.
+    const bool commutes = (two_state || (op.kind != kSwInnerDiag && op.kind != kSwInnerDense)) &&
+                          !(op.vmask & pending_bits);
+    if (!commutes) flush();
+    items.push_back({oi});
+  }
+  flush();
+  return items;
+}
+
+std::string diag_run_src(const std::vector<const SweepOp *> &run, const char *R, int na,
+                         const std::function<std::string(const SweepOp &)> &coef,
+                         const std::vector<std::string> &states = {"A"}) {
+  std::ostringstream s;
+  s << "      { // " << run.size() << " diagonal ops, fused\n";
+  s << "        " << R << " s_r = 1, s_i = 0;\n";
+  // Factor tables by register mask, in first-use order.
+  std::vector<int> masks;
+  std::map<int, bool> started;
+  for (const SweepOp *op : run) {
+    const int V = op->kind == kSwPhase ? op->rmask : op->vmask;
+    const int nv = __builtin_popcount(uint32_t(V)), N = 1 << nv;
+    s << "        {\n";
+    if (op->kind == kSwDiag) {
+      s << "          uint32_t b = 0;";
+      for (int t = 0; t < op->ndt; ++t) {
+        if (op->dsrc[t] == kSrcGlobal)
+          s << " b = (b << 1) | (uint32_t(gbase >> " << int(op->dpos[t]) << ") & 1u);";
+        else
+          s << " b = (b << 1) | ((jb >> " << int(op->dpos[t]) << ") & 1u);";
+      }
+      s << "\n          const auto c = " << coef(*op) << ";\n";
+    } else {
+      s << "          const bool on = " << nonreg_cond(*op) << ";\n";
+      if (!(op->aux & kAuxPure)) s << "          const auto c = " << coef(*op) << ";\n";
+    }
+    const int yv = op->kind == kSwPhase ? bit_ext(op->rval, V) : -1;
+    auto factor = [&](int y, std::string &fr, std::string &fi) -> bool {  // false: factor is 1
+      if (op->kind == kSwDiag) {
+        std::ostringstream a, b;
+        a << "c[(b << " << nv << ") | " << y << "u].x";
+        b << "c[(b << " << nv << ") | " << y << "u].y";
+        fr = a.str();
+        fi = b.str();
+        return true;
+      }
+      if (y != yv) return false;
+      if (op->aux & kAuxPure) {
+        fr = std::string("(on ? ") + R + "(-1) : " + R + "(1))";
+        fi = std::string(R) + "(0)";
+      } else {
+        fr = std::string("(on ? ") + R + "(c[0].x) : " + R + "(1))";
+        fi = std::string("(on ? ") + R + "(c[0].y) : " + R + "(0))";
+      }
+      return true;
+    };
+    if (V == 0) {
+      std::string fr, fi;
+      if (factor(0, fr, fi)) s << "          jit_cmul_acc(s_r, s_i, " << R << "(" << fr << "), " << R << "(" << fi << "));\n";
+    } else if (!started[V]) {
+      started[V] = true;
+      masks.push_back(V);
+      for (int y = 0; y < N; ++y) {
+        std::string fr, fi;
+        if (!factor(y, fr, fi)) {
+          fr = std::string(R) + "(1)";
+          fi = std::string(R) + "(0)";
+        }
+        s << "          f" << V << "_r[" << y << "] = " << fr << "; f" << V << "_i[" << y << "] = " << fi << ";\n";
+      }
+    } else {
+      for (int y = 0; y < N; ++y) {
+        std::string fr, fi;
+        if (factor(y, fr, fi))
+          s << "          jit_cmul_acc(f" << V << "_r[" << y << "], f" << V << "_i[" << y << "], " << R << "(" << fr
+            << "), " << R << "(" << fi << "));\n";
+      }
+    }
+    s << "        }\n";
+  }
+  // The tables are declared before the op blocks that fill them.
+  std::ostringstream decl;
+  for (int V : masks) {
+    const int N = 1 << __builtin_popcount(uint32_t(V));
+    decl << "        " << R << " f" << V << "_r[" << N << "], f" << V << "_i[" << N << "];\n";
+  }
+  // T over the growing union U, starting from the scalar.
+  std::ostringstream t;
+  int U = 0;
+  t << "        " << R << " t0_r[1] = {s_r}, t0_i[1] = {s_i};\n";
+  int step = 0;
+  for (int V : masks) {
+    const int U2 = U | V, N2 = 1 << __builtin_popcount(uint32_t(U2));
+    t << "        " << R << " t" << step + 1 << "_r[" << N2 << "], t" << step + 1 << "_i[" << N2 << "];\n";
+    for (int x = 0; x < N2; ++x) {
+      const int full = bit_dep(x, U2);
+      const int xu = bit_ext(full, U), xv = bit_ext(full, V);
+      t << "        jit_cmul(t" << step << "_r[" << xu << "], t" << step << "_i[" << xu << "], f" << V << "_r[" << xv
+        << "], f" << V << "_i[" << xv << "], t" << step + 1 << "_r[" << x << "], t" << step + 1 << "_i[" << x << "]);\n";
+    }
+    U = U2;
+    ++step;
+  }
+  for (const std::string &st : states)
+    for (int ri = 0; ri < na; ++ri) {
+      const int xu = bit_ext(ri, U);
+      t << "        jit_cmul_acc(" << st << ".re[" << ri << "], " << st << ".im[" << ri << "], t" << step << "_r[" << xu
+        << "], t" << step << "_i[" << xu << "]);\n";
+    }
+  const std::string body = s.str();
+  const size_t cut = body.find('\n') + 1;  // after the opening line
+  std::ostringstream out;
+  out << body.substr(0, cut) << decl.str() << body.substr(cut) << t.str() << "      }\n";
+  return out.str();
+}
+
+// Code of one single-state phase's ops on the registers A (16 amplitudes):
+// fused diagonal runs, the other ops one by one.  coef(op): the op's
+// coefficient accessor.
+void one_state_ops_src(const SweepOp *ops, const SweepPhase &ph, const char *R, bool c64,
+                       const std::function<std::string(const SweepOp &)> &coef, std::ostream &s) {
+  for (const auto &item : phase_items(ops, ph)) {
+    if (item.size() >= 2) {
+      std::vector<const SweepOp *> run;
+      for (uint32_t oi : item) run.push_back(&ops[oi]);
+      s << diag_run_src(run, R, kRegAmps, coef);
+      continue;
+    }
+    const SweepOp &op = ops[item[0]];
+    std::string tmpl;
+    op_routine(op, c64, tmpl);
+    s << "      " << cond_prefix(op);
+    if (op.kind == kSwDiag)
+      s << "{ " << diag_bits_src(op) << " " << tmpl << "(A, " << coef(op) << ", b); }\n";
+    else
+      s << tmpl << "(A, " << coef(op) << ", " << int(op.rmask) << ", " << int(op.rval) << ");\n";
+  }
+}
+
+// Code of one two-state (reverse adjoint) phase's ops on F (phi) and G
+// (lambda), coefficients from the shared-memory copy `coef`.  A run of
+// diagonal ops and inner products of diagonal generators is emitted as: every
+// inner product first (the run's diagonal ops commute with the generators and
+// act on both states alike, so they leave <lambda|K|phi> unchanged), the
+// Pauli-Z ones from one shared set of products conj(lambda_r) phi_r; then
+// the run's diagonal ops, fused, on both states.  False when an op is not
+// covered (an inner product with conditions).
+bool two_state_ops_src(const SweepOp *ops, const SweepPhase &ph, const char *R, bool c64, int NT, std::ostream &s) {
+  auto cf = [](const SweepOp &o) { return "(coef + " + std::to_string(o.coef) + ")"; };
+  auto inner_plain = [&](const SweepOp &op) {
+    s << "      { double sr = 0.0, si = 0.0; " << inner_call(op, R, diag_bits_src(op)) << "jit_inner_acc<" << NT
+      << ", " << op.slot << ">(acc, sr, si); }\n";
+  };
+  auto single = [&](const SweepOp &op) {
+    std::string tmpl;
+    op_routine(op, c64, tmpl, kAdjAmps);
+    s << "      " << cond_prefix(op);
+    if (op.kind == kSwDiag)
+      s << "{ " << diag_bits_src(op) << " " << tmpl << "(F, " << cf(op) << ", b); " << tmpl << "(G, " << cf(op)
+        << ", b); }\n";
+    else
+      s << "{ " << tmpl << "(F, " << cf(op) << ", " << int(op.rmask) << ", " << int(op.rval) << "); " << tmpl
+        << "(G, " << cf(op) << ", " << int(op.rmask) << ", " << int(op.rval) << "); }\n";
+  };
+  for (const auto &item : phase_items(ops, ph, true)) {
+    for (uint32_t oi : item) {
+      const SweepOp &op = ops[oi];
+      if ((op.kind == kSwInnerDiag || op.kind == kSwInnerDense) &&
+          (op.gmask || op.lmask || op.rmask || op.slot >= uint32_t(kMaxInner)))
+        return false;
+    }
+    if (item.size() == 1) {
+      const SweepOp &op = ops[item[0]];
+      if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense)
+        inner_plain(op);
+      else
+        single(op);
+      continue;
+    }
+    std::vector<const SweepOp *> diag, pauli;
+    for (uint32_t oi : item) {
+      const SweepOp &op = ops[oi];
+      if (op.kind == kSwInnerDiag && (op.aux & kAuxPauli))
+        pauli.push_back(&op);
+      else if (op.kind == kSwInnerDiag)
+        inner_plain(op);
+      else
+        diag.push_back(&op);
+    }
+    if (!pauli.empty()) {
+      s << "      { // " << pauli.size() << " Pauli-Z inner products from shared products\n";
+      for (int ri = 0; ri < kAdjAmps; ++ri)
+        s << "        const double p" << ri << "r = fma(double(G.re[" << ri << "]), double(F.re[" << ri
+          << "]), double(G.im[" << ri << "]) * double(F.im[" << ri << "])), p" << ri << "i = fma(double(G.re["
+          << ri << "]), double(F.im[" << ri << "]), -double(G.im[" << ri << "]) * double(F.re[" << ri << "]));\n";
+      for (const SweepOp *op : pauli) {
+        const int V = op->vmask, Z = op->aux & 7, nv = __builtin_popcount(uint32_t(V));
+        std::ostringstream qr, qi;
+        for (int ri = 0; ri < kAdjAmps; ++ri) {
+          const bool neg = __builtin_popcount(uint32_t(bit_ext(ri, V) & Z)) & 1;
+          qr << (neg ? " - " : " + ") << "p" << ri << "r";
+          qi << (neg ? " - " : " + ") << "p" << ri << "i";
+        }
+        s << "        { double qr = 0.0" << qr.str() << ", qi = 0.0" << qi.str() << ";";
+        if (Z >> nv)
+          s << " " << diag_bits_src(*op) << " if (__popc(b & " << (Z >> nv) << "u) & 1) { qr = -qr; qi = -qi; }";
+        s << "\n          const auto a = " << cf(*op) << "[0];\n"
+          << "          jit_inner_acc<" << NT << ", " << op->slot << ">(acc, double(a.x) * qr - double(a.y) * qi, "
+          << "double(a.x) * qi + double(a.y) * qr); }\n";
+      }
+      s << "      }\n";
+    }
+    if (diag.size() >= 2)
+      s << diag_run_src(diag, R, kAdjAmps, cf, {"F", "G"});
+    else if (diag.size() == 1)
+      single(*diag[0]);
+  }
+  return true;
+}
+
 struct JitShape {
   bool smem_coef = false, dload = false, dstore = false;
   int stages = 0;     // > 0: bulk-copy pipeline with this many tiles in flight per CTA
@@ -505,39 +827,14 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi) {
       s << "      Ph::load(A, psi, gbase, jb);\n";
     else
       s << "      Ph::gather(A, tile, jb);\n";
-    for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
-      const SweepOp &op = ps.op[oi];
-      s << "      ";
-      const bool guard = op.gmask || op.lmask;
-      if (guard) {
-        s << "if (";
-        if (op.gmask)
-          s << "(gbase & 0x" << std::hex << op.gmask << "ull) == 0x" << op.gval << "ull" << std::dec;
-        if (op.gmask && op.lmask) s << " && ";
-        if (op.lmask) s << "(jb & 0x" << std::hex << op.lmask << "u) == 0x" << op.lval << "u" << std::dec;
-        s << ") ";
-      }
-      std::string tmpl;
-      op_routine(op, c64, tmpl);
-      std::ostringstream cexpr;
-      if (multi || lane_indexed(op))
-        cexpr << "coef + " << op.coef;
+    one_state_ops_src(ps.op.data(), ph, R, c64, [&](const SweepOp &o) {
+      std::ostringstream c;
+      if (multi || lane_indexed(o))
+        c << "(coef + " << o.coef << ")";
       else
-        cexpr << "ParamCoef<" << R << ", " << op.coef << ">{P.coef}";
-      if (op.kind == kSwDiag) {
-        s << "{ uint32_t b = 0;";
-        for (int t = 0; t < op.ndt; ++t) {
-          if (op.dsrc[t] == kSrcGlobal)
-            s << " b = (b << 1) | (uint32_t(gbase >> " << int(op.dpos[t]) << ") & 1u);";
-          else
-            s << " b = (b << 1) | ((jb >> " << int(op.dpos[t]) << ") & 1u);";
-        }
-        s << " " << tmpl << "(A, " << cexpr.str() << ", b); }\n";
-      } else {
-        s << tmpl << "(A, " << cexpr.str() << ", " << int(op.rmask) << ", " << int(op.rval)
-          << ");\n";
-      }
-    }
+        c << "ParamCoef<" << R << ", " << o.coef << ">{P.coef}";
+      return c.str();
+    }, s);
     if (p == last && js.dstore && remap) {
       s << "      using PhO = JitPhase<" << R << ", " << M << ", TileOut, " << int(ph.reg[0]) << ", "
         << int(ph.reg[1]) << ", " << int(ph.reg[2]) << ", " << int(ph.reg[3]);
@@ -575,17 +872,6 @@ std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb) {
   s << ">;\n";
   s << "  jit_adjoint_sweep<" << R << ", " << M
     << ", Tile>(psi, lam, P, partials, [&](C2 *ft, C2 *lt, const C2 *coef, uint64_t gbase, double2 *acc) {\n";
-  auto diag_bits = [&](const SweepOp &op) {
-    std::ostringstream b;
-    b << "uint32_t b = 0;";
-    for (int t = 0; t < op.ndt; ++t) {
-      if (op.dsrc[t] == kSrcGlobal)
-        b << " b = (b << 1) | (uint32_t(gbase >> " << int(op.dpos[t]) << ") & 1u);";
-      else
-        b << " b = (b << 1) | ((jb >> " << int(op.dpos[t]) << ") & 1u);";
-    }
-    return b.str();
-  };
   for (uint32_t p = 0; p < ps.h.nphases; ++p) {
     const SweepPhase &ph = ps.ph[p];
     s << "    {\n      using Ph = JitPhase2<" << R << ", " << M << ", Tile, " << int(ph.reg[0]) << ", "
@@ -594,40 +880,8 @@ std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb) {
     s << ">;\n";
     s << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << ", " << kAdjAmps
       << "> F, G;\n      Ph::gather(F, G, ft, lt, jb);\n";
-    for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
-      const SweepOp &op = ps.op[oi];
-      if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
-        // Inner products carry no conditions (as in the generic kernel).
-        if (op.gmask || op.lmask || op.rmask || op.slot >= uint32_t(kMaxInner)) return std::string();
-        s << "      { double sr = 0.0, si = 0.0; " << inner_call(op, R, diag_bits(op)) << "jit_inner_acc<" << NT
-          << ", " << op.slot << ">(acc, sr, si); }\n";
-        continue;
-      }
-      s << "      ";
-      if (op.gmask || op.lmask) {
-        s << "if (";
-        if (op.gmask)
-          s << "(gbase & 0x" << std::hex << op.gmask << "ull) == 0x" << op.gval << "ull" << std::dec;
-        if (op.gmask && op.lmask) s << " && ";
-        if (op.lmask) s << "(jb & 0x" << std::hex << op.lmask << "u) == 0x" << op.lval << "u" << std::dec;
-        s << ") ";
-      }
-      std::string tmpl;
-      op_routine(op, c64, tmpl, kAdjAmps);
-      // Coefficients from the shared-memory copy: read from the parameter
-      // block, the compiler keeps every coefficient of the sweep in registers
-      // across the tile loop (255 registers and spills for a QAOA sweep,
-      // 160-165 without spills from shared memory at 3 CTAs per SM).
-      std::ostringstream cexpr;
-      cexpr << "coef + " << op.coef;
-      if (op.kind == kSwDiag) {
-        s << "{ " << diag_bits(op) << " " << tmpl << "(F, " << cexpr.str() << ", b); " << tmpl << "(G, "
-          << cexpr.str() << ", b); }\n";
-      } else {
-        s << "{ " << tmpl << "(F, " << cexpr.str() << ", " << int(op.rmask) << ", " << int(op.rval) << "); "
-          << tmpl << "(G, " << cexpr.str() << ", " << int(op.rmask) << ", " << int(op.rval) << "); }\n";
-      }
-    }
+    // Inner products carry no conditions (as in the generic kernel).
+    if (!two_state_ops_src(ps.op.data(), ph, R, c64, NT, s)) return std::string();
     s << "      Ph::scatter(F, G, ft, lt, jb);\n      __syncthreads();\n    }\n";
   }
   s << "  });\n}\n";
@@ -640,29 +894,6 @@ std::string jit_adjoint_body(const PlannedSweep &ps, bool c64, int minb) {
 // packed plan, through shared memory).
 // ---------------------------------------------------------------------------
 namespace {
-
-std::string cond_prefix(const SweepOp &op) {
-  if (!op.gmask && !op.lmask) return std::string();
-  std::ostringstream s;
-  s << "if (";
-  if (op.gmask) s << "(gbase & 0x" << std::hex << op.gmask << "ull) == 0x" << op.gval << "ull" << std::dec;
-  if (op.gmask && op.lmask) s << " && ";
-  if (op.lmask) s << "(jb & 0x" << std::hex << op.lmask << "u) == 0x" << op.lval << "u" << std::dec;
-  s << ") ";
-  return s.str();
-}
-
-std::string diag_bits_src(const SweepOp &op) {
-  std::ostringstream b;
-  b << "uint32_t b = 0;";
-  for (int t = 0; t < op.ndt; ++t) {
-    if (op.dsrc[t] == kSrcGlobal)
-      b << " b = (b << 1) | (uint32_t(gbase >> " << int(op.dpos[t]) << ") & 1u);";
-    else
-      b << " b = (b << 1) | ((jb >> " << int(op.dpos[t]) << ") & 1u);";
-  }
-  return b.str();
-}
 
 std::string tile_type(const SweepHeader &h) {
   std::ostringstream s;
@@ -720,17 +951,10 @@ std::string jit_batch_adjoint_body(const unsigned char *plan, uint32_t nfwd, uin
         fns << ">;\n      if (threadIdx.x < " << NT4 << ") {\n"
             << "      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R
             << "> A;\n      Ph::gather(A, tile, jb);\n";
-        for (uint32_t oi = P.op_begin; oi < P.op_end; ++oi) {
-          const SweepOp &op = ops[oi];
-          if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) return std::string();
-          std::string tmpl;
-          op_routine(op, c64, tmpl, 16);
-          fns << "      " << cond_prefix(op);
-          if (op.kind == kSwDiag)
-            fns << "{ " << diag_bits_src(op) << " " << tmpl << "(A, coef + " << op.coef << ", b); }\n";
-          else
-            fns << tmpl << "(A, coef + " << op.coef << ", " << int(op.rmask) << ", " << int(op.rval) << ");\n";
-        }
+        for (uint32_t oi = P.op_begin; oi < P.op_end; ++oi)
+          if (ops[oi].kind == kSwInnerDiag || ops[oi].kind == kSwInnerDense) return std::string();
+        one_state_ops_src(ops, P, R, c64, [](const SweepOp &o) { return "(coef + " + std::to_string(o.coef) + ")"; },
+                          fns);
         fns << "      Ph::scatter(A, tile, jb);\n      }\n      __syncthreads(); }\n";
       } else {
         fns << "    { using Ph = JitPhase2<" << R << ", " << M << ", Tile, " << int(P.reg[0]) << ", "
@@ -738,25 +962,7 @@ std::string jit_batch_adjoint_body(const unsigned char *plan, uint32_t nfwd, uin
         for (int t : thread_positions(P, int(M), c64, false, kAdjRegBits)) fns << ", " << t;
         fns << ">;\n      const uint32_t jb = Ph::jb(threadIdx.x);\n      Amps<" << R << ", " << kAdjAmps
             << "> F, G;\n      Ph::gather(F, G, ft, lt, jb);\n";
-        for (uint32_t oi = P.op_begin; oi < P.op_end; ++oi) {
-          const SweepOp &op = ops[oi];
-          if (op.kind == kSwInnerDiag || op.kind == kSwInnerDense) {
-            if (op.gmask || op.lmask || op.rmask || op.slot >= uint32_t(kMaxInner)) return std::string();
-            fns << "      { double sr = 0.0, si = 0.0; " << inner_call(op, R, diag_bits_src(op)) << "jit_inner_acc<"
-                << NT << ", " << op.slot << ">(acc, sr, si); }\n";
-            continue;
-          }
-          std::string tmpl;
-          op_routine(op, c64, tmpl, kAdjAmps);
-          fns << "      " << cond_prefix(op);
-          if (op.kind == kSwDiag)
-            fns << "{ " << diag_bits_src(op) << " " << tmpl << "(F, coef + " << op.coef << ", b); " << tmpl
-                << "(G, coef + " << op.coef << ", b); }\n";
-          else
-            fns << "{ " << tmpl << "(F, coef + " << op.coef << ", " << int(op.rmask) << ", " << int(op.rval)
-                << "); " << tmpl << "(G, coef + " << op.coef << ", " << int(op.rmask) << ", " << int(op.rval)
-                << "); }\n";
-        }
+        if (!two_state_ops_src(ops, P, R, c64, NT, fns)) return std::string();
         fns << "      Ph::scatter(F, G, ft, lt, jb);\n      __syncthreads(); }\n";
       }
     }

@@ -29,6 +29,19 @@ struct ParamCoef {
   }
 };
 
+// Complex products of the fused diagonal runs: o = a b, and a *= b.
+template <typename Real>
+__device__ __forceinline__ void jit_cmul(Real ar, Real ai, Real br, Real bi, Real &o_r, Real &o_i) {
+  o_r = ar * br - ai * bi;
+  o_i = ar * bi + ai * br;
+}
+template <typename Real>
+__device__ __forceinline__ void jit_cmul_acc(Real &ar, Real &ai, Real br, Real bi) {
+  const Real r = ar * br - ai * bi;
+  ai = ar * bi + ai * br;
+  ar = r;
+}
+
 // Tile geometry of one sweep with its high tile bits as constants: tile
 // position L+i holds global index bit HI[i] (ascending); positions below L
 // are the L lowest global bits.  Global addresses then need no lookup table.

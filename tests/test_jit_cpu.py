@@ -149,7 +149,11 @@ def test_adjoint_inner_products_take_the_pauli_form():
     the reverse sweeps come from shared memory (no parameter-block reads)."""
     srcs = capi.jit_sources(20, _qaoa(20, 1, seed=2), capi.SQ_C128, adjoint=True)
     body = "".join(s.split("sq_jit_adjoint(")[1] for s in srcs if s)
-    assert "inner_dense_pauli<" in body and "inner_diag_pauli<" in body
+    assert "inner_dense_pauli<" in body
+    # ZZ generators: one at a time, or several from the shared products of a
+    # fused diagonal run.
+    assert "inner_diag_pauli<" in body or "Pauli-Z inner products from shared products" in body
+    assert "Pauli-Z inner products from shared products" in body and "diagonal ops, fused" in body
     assert "inner_dense<" not in body and "inner_diag<" not in body
     assert "ParamCoef<" not in body
     ops = [("Hadamard", (q,), ()) for q in range(20)]
