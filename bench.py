@@ -460,16 +460,40 @@ def _run_ours(args, rank, world, local):
             out["e2e"] = e2e(n, ops, args, amp)
         except Exception as e:  # report, do not lose the device-timed line
             out["e2e"] = {"value": None, "unit": "GB/s", "note": f"e2e failed: {e}"}
+        if dtype == capi.SQ_C128 and not args.no_configs and out["e2e"].get("value"):
+            try:
+                out["e2e"]["complex64"] = e2e(n, ops, args, 8, precision="complex64")
+            except Exception as e:
+                out["e2e"]["complex64"] = {"note": f"complex64 e2e failed: {e}"}
+    with_c64 = dtype == capi.SQ_C128 and not args.no_configs
     if world == 1 and rank == 0 and not args.no_adjoint:
+        ref = {}
         try:
-            out["adjoint"] = adjoint_metric(args.precision)
+            out["adjoint"] = adjoint_metric(args.precision, keep=ref)
         except Exception as e:
             out["adjoint"] = {"note": f"adjoint failed: {e}"}
+        if with_c64 and ref:
+            try:
+                got = {}
+                a64 = adjoint_metric("complex64", shift=False, keep=got)
+                a64 = {k: a64[k] for k in ("workload", "adjoint_ms", "forward_sweeps_ms", "reverse_sweeps_ms",
+                                           "reverse_sweep_frac", "roofline")}
+                a64["max_abs_gradient_error_vs_complex128"] = float(np.abs(got["gradient"] - ref["gradient"]).max())
+                a64["energy_error_vs_complex128"] = abs(got["energy"] - ref["energy"])
+                out["adjoint"]["complex64"] = a64
+            except Exception as e:
+                out["adjoint"]["complex64"] = {"note": f"complex64 adjoint failed: {e}"}
     if world == 1 and rank == 0 and not args.no_batch:
+        ref = {}
         try:
-            out["batch"] = batch_metric(args.precision)
+            out["batch"] = batch_metric(args.precision, keep=ref)
         except Exception as e:
             out["batch"] = {"note": f"batch failed: {e}"}
+        if with_c64 and ref:
+            try:
+                out["batch"]["complex64"] = batch_complex64_metric(ref["energies"])
+            except Exception as e:
+                out["batch"]["complex64"] = {"note": f"complex64 batch failed: {e}"}
         try:
             out["qaoa_batch"] = qaoa_batch_metric(args.precision)
         except Exception as e:
@@ -632,7 +656,7 @@ def qaoa_workload(n=26, p=8, seed=SEED):
     return ops, circuits.maxcut_hamiltonian(n, edges), theta
 
 
-def adjoint_metric(precision: str, shift: bool = True):
+def adjoint_metric(precision: str, shift: bool = True, keep: dict | None = None):
     """Adjoint gradient (one forward + one fused reverse pass) against the
     parameter-shift rule on the same engine, QAOA MaxCut 26 qubits p = 8:
     the full 1040-evaluation shift gradient is computed and compared
@@ -683,6 +707,8 @@ def adjoint_metric(precision: str, shift: bool = True):
         t_shift = time.perf_counter() - t0
         diff = float(np.abs(np.asarray(g) - np.asarray(g_shift)).max())
     ws.close()
+    if keep is not None:
+        keep["energy"], keep["gradient"] = e, np.array(g, copy=True)
     out = {"workload": f"qaoa_maxcut_{n}q_p{p}_{precision}", "params": 2 * p,
             "gate_occurrences": evals // 2, "energy": e,
             "adjoint_ms": round(t_adj * 1e3, 3), "adjoint_grads_per_s": round(1.0 / t_adj, 3),
@@ -720,6 +746,34 @@ def vqe_batch_circuits(ncirc: int = 4096, seed: int = SEED):
     sizes = [int(x) for x in rng.integers(8, 21, size=ncirc)]
     angles = [rng.uniform(0, 2 * np.pi, 12 * n) for n in sizes]
     return sizes, lambda i: (sizes[i], circuits.vqe_ansatz(sizes[i], angles[i]), terms[sizes[i]])
+
+
+def batch_complex64_metric(ref_energies, ncirc: int = 4096, seed: int = SEED):
+    """The VQE batch of batch_metric (same seed: same circuits and angles) on
+    complex64 states: kernel time (default configuration, median of 3) and
+    the energies' max-abs error against the complex128 batch."""
+    from snuqs_b200 import capi, circuits
+
+    rng = np.random.default_rng(seed)
+    b = capi.Batch(capi.SQ_C64)
+    hams = {n: b.add_hamiltonian(n, circuits.random_pauli_hamiltonian(n, 64, seed=seed + n))
+            for n in range(8, 21)}
+    sizes = rng.integers(8, 21, size=ncirc)
+    for n in sizes:
+        n = int(n)
+        b.add_circuit(n, circuits.vqe_ansatz(n, rng.uniform(0, 2 * np.pi, 12 * n)), hams[n])
+    b.run()
+    ks = []
+    for _ in range(3):
+        e = b.run()
+        ks.append(b.last_timing()[0])
+    groups = b.groups()
+    b.close()
+    err = np.abs(np.asarray(e) - np.asarray(ref_energies))
+    return {"workload": f"vqe_batch_{ncirc}x_8to20q_complex64", "kernel_ms": round(float(np.median(ks)), 3),
+            "structure_groups": groups[0], "circuits_in_groups": groups[1],
+            "max_abs_energy_error_vs_complex128": float(err.max()),
+            "max_rel_energy_error_vs_complex128": float((err / np.maximum(1.0, np.abs(ref_energies))).max())}
 
 
 def batch_metric_sharded(precision: str, rank: int, world: int, ncirc: int = 4096):
@@ -825,7 +879,7 @@ def qaoa_batch_metric(precision: str, sets: int = 512, n: int = 16, p: int = 8):
                       f"extrapolated from {done} evaluations"}
 
 
-def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED):
+def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED, keep: dict | None = None):
     """Batched VQE energies: ncirc hardware-efficient ansatz circuits with
     qubit counts uniform in 8..20 (6 layers of RY, RZ on every qubit and a CX
     ladder, angles uniform in [0, 2pi)), one 64-term random Pauli-sum
@@ -866,6 +920,8 @@ def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED):
     cfg = b.autotune(reps=1)
     t_tune = time.perf_counter() - t0
     k_tuned, energies = kernel_ms()
+    if keep is not None:
+        keep["energies"] = np.array(energies, copy=True)
     ctas = b.last_timing()[1]
     streamed, sweeps, alg = b.stats()
     groups, grouped = b.groups()
@@ -919,7 +975,7 @@ def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED):
                       "around the batch's kernels (median of 3)"}
 
 
-def e2e(n, ops, args, amp, shots: int = 1_000_000):
+def e2e(n, ops, args, amp, shots: int = 1_000_000, precision: str | None = None):
     """Same metric through the reference-facing `_C` drop-in, as a shot-based
     Braket task drives it (simulation.py: initialize_basis_z, one
     functionals.apply per gate, then retrieve_samples): each step applies the
@@ -933,7 +989,7 @@ def e2e(n, ops, args, amp, shots: int = 1_000_000):
     from snuqs_b200 import _C
 
     G = _C.operation.gate_operations
-    prec = args.precision
+    prec = precision or args.precision
     try:
         sv = _C.result_types.StateVector(_C.DeviceType.CUDA, n, prec)
     except Exception as e:

@@ -14,6 +14,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/snuqs_b200.h"
@@ -1269,9 +1270,32 @@ int adjoint_impl(sq_state *psi, sq_state *lam, const sq::AdjointPlan &ap, const 
   ropt.tile_bits = pick_adjoint_tile_bits(psi->dtype, n);
   ropt.reg_bits = sq::kAdjRegBits;
   ropt.max_dense_k = sq::kAdjRegBits;
+  // The reverse pass is planned (and its JIT kernels looked up or compiled)
+  // on a second host thread while this one plans and launches the forward
+  // pass, so its planning overlaps the forward sweeps on the device.
+  std::string rerr;
+  const bool jit = use_jit(psi);
+  std::thread rthread([&] {
+    try {
+      rplan = sq::plan_sweeps(ap.reverse, n, ropt);
+      if (jit) {
+        std::vector<const sq::PlannedSweep *> sweeps;
+        for (const auto &pl : rplan)
+          if (pl.is_sweep) sweeps.push_back(&pl.sweep);
+        sq::jit_prepare_adjoint(sweeps, sizeof(Real) == 4);
+      }
+    } catch (const std::exception &e) {
+      rerr = e.what();
+    }
+  });
+  struct Joiner {
+    std::thread &t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } joiner{rthread};
   try {
     fplan = sq::plan_sweeps(ap.forward, n, fopt);
-    rplan = sq::plan_sweeps(ap.reverse, n, ropt);
   } catch (const std::exception &e) {
     return fail(SQ_ERR_INVALID, "adjoint planner: %s", e.what());
   }
@@ -1282,6 +1306,8 @@ int adjoint_impl(sq_state *psi, sq_state *lam, const sq::AdjointPlan &ap, const 
       SQ_TRY(launch_gate<Real>(psi->data, n, as_dense(pl.gate), nullptr, st, di.sms));
     }
   }
+  rthread.join();
+  if (!rerr.empty()) return fail(SQ_ERR_INVALID, "adjoint planner: %s", rerr.c_str());
   // Device scratch for this call (stream-ordered).
   const uint32_t red_blocks = uint32_t(std::max<uint64_t>(
       1, std::min<uint64_t>(((uint64_t(1) << n) + sq::kReduceThreads - 1) / sq::kReduceThreads,
@@ -1298,12 +1324,6 @@ int adjoint_impl(sq_state *psi, sq_state *lam, const sq::AdjointPlan &ap, const 
       (reinterpret_cast<uintptr_t>(e_dev + 2) + 15) & ~uintptr_t(15));
   auto *partials = ipvals + nip;
   int status = SQ_OK;
-  if (use_jit(psi)) {
-    std::vector<const sq::PlannedSweep *> sweeps;
-    for (const auto &pl : rplan)
-      if (pl.is_sweep) sweeps.push_back(&pl.sweep);
-    sq::jit_prepare_adjoint(sweeps, sizeof(Real) == 4);
-  }
   auto run = [&]() -> int {
     SQ_CUDA(cudaMemsetAsync(ipvals, 0, nip * sizeof(double2), st));
     SQ_TRY(pauli_apply<Real>(psi, lam, paulis, w, nt, red, red_blocks, e_dev, st));

@@ -376,27 +376,52 @@ uint32_t op_budget(const PlanOptions &opt) {
   return opt.max_ops ? std::min<uint32_t>(opt.max_ops, kMaxOps) : uint32_t(kMaxOps);
 }
 
+// Per-op facts the tile selection reads many times (masks, coefficient
+// count, fusability), computed once per op of the planner's working copy
+// and looked up by address (every op pointer the planner holds points into
+// that copy).
+struct OpInfo {
+  uint64_t T, A, tm;  // non-diagonal, touched and target bits
+  uint32_t coef;
+  bool diag, fits, inner;
+};
+
+struct OpTable {
+  const HostOp *base = nullptr;
+  std::vector<OpInfo> v;
+  const OpInfo &operator()(const HostOp *p) const { return v[size_t(p - base)]; }
+  void set(const HostOp &op, const PlanOptions &opt) {
+    OpInfo &f = v[size_t(&op - base)];
+    f.T = op.nondiag_mask();
+    f.A = op.touched_mask();
+    f.tm = op.target_mask();
+    f.coef = SweepBuilder::coef_count(op);
+    f.diag = SweepBuilder::is_diag(op);
+    f.fits = fusable_size(op, opt);
+    f.inner = op.kind == kOpInner;
+  }
+};
+
 // Gates from rem[head..] that a sweep with tile bits S takes (same rules as
 // the collection below, without growing S).
 uint32_t absorbed(const std::vector<const HostOp *> &rem, size_t head, uint64_t S, uint32_t n,
-                  const PlanOptions &opt, size_t window) {
+                  const PlanOptions &opt, size_t window, const OpTable &tab) {
   uint32_t cnt = 0, ncoef = 0, ninner = 0;
   const uint32_t max_ops = op_budget(opt);
   uint64_t blockT = 0, blockA = 0;
   size_t skipped = 0;
   for (size_t i = head; i < rem.size(); ++i) {
-    const HostOp &op = *rem[i];
-    const uint64_t T = op.nondiag_mask(), A = op.touched_mask();
+    const OpInfo &f = tab(rem[i]);
+    const uint64_t T = f.T, A = f.A;
     const bool commutes = (T & blockA) == 0 && (A & blockT) == 0;
-    const bool diag = SweepBuilder::is_diag(op);
-    const uint32_t c = SweepBuilder::coef_count(op);
-    const bool fits = fusable_size(op, opt) && (diag || (op.target_mask() & ~S) == 0) &&
-                      cnt < max_ops && ncoef + c <= uint32_t(kMaxCoef) &&
-                      !(op.kind == kOpInner && ninner >= uint32_t(kMaxInner));
+    const bool diag = f.diag;
+    const uint32_t c = f.coef;
+    const bool fits = f.fits && (diag || (f.tm & ~S) == 0) && cnt < max_ops &&
+                      ncoef + c <= uint32_t(kMaxCoef) && !(f.inner && ninner >= uint32_t(kMaxInner));
     if (commutes && fits) {
       ++cnt;
       ncoef += c;
-      if (op.kind == kOpInner) ++ninner;
+      if (f.inner) ++ninner;
       if (cnt >= max_ops) break;
       continue;
     }
@@ -411,17 +436,17 @@ uint32_t absorbed(const std::vector<const HostOp *> &rem, size_t head, uint64_t 
 // the sweep absorbs: grown one bit, or one pair of a two-target gate's
 // bits, at a time by the best gain per added bit.
 uint64_t select_tile(const std::vector<const HostOp *> &rem, size_t head, uint32_t n, uint32_t m,
-                     uint64_t start, const PlanOptions &opt, size_t window) {
+                     uint64_t start, const PlanOptions &opt, size_t window, const OpTable &tab) {
   uint64_t S = start;
-  uint32_t cur = absorbed(rem, head, S, n, opt, window);
+  uint32_t cur = absorbed(rem, head, S, n, opt, window, tab);
   while (uint32_t(popc64(S)) < m) {
     // Candidate bits: targets of the next gates outside S.
     uint64_t cand = 0;
     std::vector<uint64_t> pairs;
     for (size_t i = head, seen = 0; i < rem.size() && seen < 2 * window; ++i, ++seen) {
-      const HostOp &op = *rem[i];
-      if (SweepBuilder::is_diag(op) || !fusable_size(op, opt)) continue;
-      const uint64_t out = op.target_mask() & ~S;
+      const OpInfo &f = tab(rem[i]);
+      if (f.diag || !f.fits) continue;
+      const uint64_t out = f.tm & ~S;
       cand |= out;
       if (popc64(out) == 2 && std::find(pairs.begin(), pairs.end(), out) == pairs.end() &&
           pairs.size() < 48)
@@ -433,17 +458,17 @@ uint64_t select_tile(const std::vector<const HostOp *> &rem, size_t head, uint32
     for (uint32_t b = 0; b < n; ++b) {
       if (!((cand >> b) & 1)) continue;
       const uint64_t add = uint64_t(1) << b;
-      const double g = double(absorbed(rem, head, S | add, n, opt, window)) - cur;
+      const double g = double(absorbed(rem, head, S | add, n, opt, window, tab)) - cur;
       if (g > best) best = g, best_add = add;
     }
     if (uint32_t(popc64(S)) + 2 <= m)
       for (uint64_t pr : pairs) {
-        const double g = (double(absorbed(rem, head, S | pr, n, opt, window)) - cur) / 2.0;
+        const double g = (double(absorbed(rem, head, S | pr, n, opt, window, tab)) - cur) / 2.0;
         if (g > best) best = g, best_add = pr;
       }
     if (!best_add) break;
     S |= best_add;
-    cur = absorbed(rem, head, S, n, opt, window);
+    cur = absorbed(rem, head, S, n, opt, window, tab);
   }
   return S;
 }
@@ -463,14 +488,17 @@ void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits, 
                      uint64_t low_out, std::vector<const HostOp *> &order,
                      std::vector<uint64_t> &phase_regs, std::vector<uint32_t> &phase_first) {
   const size_t N = ops.size();
-  std::vector<uint64_t> pred(N, 0);
+  std::vector<uint64_t> pred(N, 0), Tm(N), Am(N), tgt(N);
+  std::vector<char> dg(N);
   for (size_t j = 0; j < N; ++j) {
-    const uint64_t Tj = ops[j]->nondiag_mask(), Aj = ops[j]->touched_mask();
-    for (size_t i = 0; i < j; ++i) {
-      const uint64_t Ti = ops[i]->nondiag_mask(), Ai = ops[i]->touched_mask();
-      if ((Ti & Aj) || (Ai & Tj)) pred[j] |= uint64_t(1) << i;
-    }
+    Tm[j] = ops[j]->nondiag_mask();
+    Am[j] = ops[j]->touched_mask();
+    tgt[j] = ops[j]->target_mask();
+    dg[j] = SweepBuilder::is_diag(*ops[j]);
   }
+  for (size_t j = 0; j < N; ++j)
+    for (size_t i = 0; i < j; ++i)
+      if ((Tm[i] & Am[j]) || (Am[i] & Tm[j])) pred[j] |= uint64_t(1) << i;
   const uint64_t all = N == 64 ? ~uint64_t(0) : ((uint64_t(1) << N) - 1);
   uint64_t placed = 0;
   order.clear();
@@ -484,7 +512,7 @@ void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits, 
       for (size_t x = 0; x < N; ++x) {
         const uint64_t bit = uint64_t(1) << x;
         if ((placed & bit) || (pred[x] & ~placed)) continue;
-        const bool fits = SweepBuilder::is_diag(*ops[x]) || (ops[x]->target_mask() & ~R) == 0;
+        const bool fits = dg[x] || (tgt[x] & ~R) == 0;
         if (!fits) continue;
         placed |= bit;
         order.push_back(ops[x]);
@@ -498,14 +526,14 @@ void schedule_phases(const std::vector<const HostOp *> &ops, uint32_t reg_bits, 
       for (size_t x = 0; x < N; ++x) {
         const uint64_t bit = uint64_t(1) << x;
         if ((placed & bit) || (pred[x] & ~placed)) continue;
-        const uint64_t T = ops[x]->target_mask();
+        const uint64_t T = tgt[x];
         if (popc64(R | T) > int(reg_bits)) continue;
         const bool on_low = (T & (first_phase ? low : low_out)) != 0;
         const int key = (on_low == first_phase ? 16 : 0) + popc64(T & ~R);
         if (key < best_key) best_key = key, best = int(x);
       }
       if (best < 0) break;
-      R |= ops[size_t(best)]->target_mask();
+      R |= tgt[size_t(best)];
     }
     phase_regs.push_back(R);
   }
@@ -535,19 +563,20 @@ void relabel(HostOp &op, const std::vector<int> &perm) {
 // out[b]; empty: store in place) and the bits stored to the low bits.
 std::vector<int> choose_remap(const std::vector<const HostOp *> &after, uint64_t S,
                               const std::vector<int> &virt_at, uint32_t n, uint32_t m, uint32_t l,
-                              const PlanOptions &opt, size_t window, uint64_t &low_out) {
+                              const PlanOptions &opt, size_t window, uint64_t &low_out,
+                              const OpTable &tab) {
   const uint64_t low = (uint64_t(1) << l) - 1;
   S |= low;
   std::vector<std::pair<int, int>> swaps;  // (low slot, tile bit moved there)
   if (!after.empty()) {
-    const uint64_t wish = select_tile(after, 0, n, m, 0, opt, window);
+    const uint64_t wish = select_tile(after, 0, n, m, 0, opt, window, tab);
     uint64_t slots = low & ~wish;
     std::vector<std::pair<size_t, int>> cands;  // (first use, bit)
     for (uint32_t b = l; b < n; ++b) {
       if (!((wish >> b) & 1) || !((S >> b) & 1)) continue;
       size_t first = after.size();
       for (size_t i = 0; i < after.size() && i < window; ++i)
-        if ((after[i]->target_mask() >> b) & 1) {
+        if ((tab(after[i]).tm >> b) & 1) {
           first = i;
           break;
         }
@@ -642,6 +671,10 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
   const bool remap = opt.remap && select;
   std::vector<const HostOp *> rem;
   for (const auto &o : work) rem.push_back(&o);
+  OpTable tab;
+  tab.base = work.data();
+  tab.v.resize(work.size());
+  for (const auto &o : work) tab.set(o, opt);
   size_t head = 0;  // rem[head..] still to place
   while (head < rem.size()) {
     const HostOp &first = *rem[head];
@@ -666,8 +699,8 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
     if (select) {
       // Tile bits chosen up front; gates that fit them (or grow them while
       // there is room) are collected in circuit order, then scheduled.
-      uint64_t S = select_tile(rem, head, n, m, (uint64_t(1) << l) - 1, opt, kWindow);
-      if (absorbed(rem, head, S, n, opt, kWindow) == 0) S = ((uint64_t(1) << l) - 1) | first.target_mask();
+      uint64_t S = select_tile(rem, head, n, m, (uint64_t(1) << l) - 1, opt, kWindow, tab);
+      if (absorbed(rem, head, S, n, opt, kWindow, tab) == 0) S = ((uint64_t(1) << l) - 1) | first.target_mask();
       std::vector<const HostOp *> chosen;
       std::vector<size_t> chosen_idx, skipped_idx;
       uint64_t blockT = 0, blockAll = 0;
@@ -675,20 +708,20 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       size_t i = head;
       for (; i < rem.size(); ++i) {
         const HostOp &op = *rem[i];
-        const uint64_t T = op.nondiag_mask(), A = op.touched_mask();
+        const OpInfo &f = tab(&op);
+        const uint64_t T = f.T, A = f.A;
         const bool commutes = (T & blockAll) == 0 && (A & blockT) == 0;
-        const bool diag = SweepBuilder::is_diag(op);
-        const uint32_t c = SweepBuilder::coef_count(op);
-        const bool fits = fusable_size(op, opt) &&
-                          (diag || uint32_t(popc64(S | op.target_mask())) <= m) &&
+        const bool diag = f.diag;
+        const uint32_t c = f.coef;
+        const bool fits = f.fits && (diag || uint32_t(popc64(S | f.tm)) <= m) &&
                           chosen.size() < size_t(sb.max_ops) && ncoef + c <= uint32_t(kMaxCoef) &&
-                          !(op.kind == kOpInner && ninner >= uint32_t(kMaxInner));
+                          !(f.inner && ninner >= uint32_t(kMaxInner));
         if (commutes && fits) {
-          if (!diag) S |= op.target_mask();
+          if (!diag) S |= f.tm;
           chosen.push_back(&op);
           chosen_idx.push_back(i);
           ncoef += c;
-          if (op.kind == kOpInner) ++ninner;
+          if (f.inner) ++ninner;
           if (chosen.size() >= size_t(sb.max_ops)) {
             ++i;
             break;
@@ -711,7 +744,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
         for (size_t x : skipped_idx) after.push_back(rem[x]);
         for (size_t x = i; x < rem.size(); ++x) after.push_back(rem[x]);
         uint64_t lo = 0;
-        sb.outmap = choose_remap(after, S, virt_at, n, m, l, opt, kWindow, lo);
+        sb.outmap = choose_remap(after, S, virt_at, n, m, l, opt, kWindow, lo, tab);
         if (!sb.outmap.empty()) {
           low_out = lo;
           for (uint32_t b = 0; b < n; ++b)  // every bit the remap moves is a tile bit
@@ -751,7 +784,10 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       next.insert(next.end(), rem.begin() + i, rem.end());
       if (!sb.outmap.empty()) {
         // Ops after the sweep see its stored bit order.
-        for (const HostOp *op : next) relabel(const_cast<HostOp &>(*op), sb.outmap);
+        for (const HostOp *op : next) {
+          relabel(const_cast<HostOp &>(*op), sb.outmap);
+          tab.set(*op, opt);
+        }
         std::vector<int> va(n);
         for (uint32_t b = 0; b < n; ++b) va[size_t(sb.outmap[b])] = virt_at[b];
         virt_at.swap(va);
