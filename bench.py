@@ -68,6 +68,9 @@ def parse():
     p.add_argument("--adjoint-only", action="store_true",
                    help="only the QAOA-26 adjoint gradient, without the parameter-shift comparison "
                         "(a short command for profiling the adjoint kernels)")
+    p.add_argument("--batch-only", action="store_true",
+                   help="only the VQE energy batch, default configuration, no autotuning or oracle "
+                        "check (a short command for profiling the batch kernels)")
     p.add_argument("--kernel-tour", action="store_true",
                    help="run each kernel family once on a small case (for ncu captures) "
                         "instead of the benchmark line")
@@ -352,6 +355,9 @@ def main():
         return
     if args.adjoint_only:
         print(json.dumps(adjoint_metric(args.precision, shift=False)))
+        return
+    if args.batch_only:
+        print(json.dumps(batch_metric(args.precision, tune=False)))
         return
     if args.op_cost:
         op_cost(args)
@@ -879,7 +885,8 @@ def qaoa_batch_metric(precision: str, sets: int = 512, n: int = 16, p: int = 8):
                       f"extrapolated from {done} evaluations"}
 
 
-def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED, keep: dict | None = None):
+def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED, keep: dict | None = None,
+                 tune: bool = True):
     """Batched VQE energies: ncirc hardware-efficient ansatz circuits with
     qubit counts uniform in 8..20 (6 layers of RY, RZ on every qubit and a CX
     ladder, angles uniform in [0, 2pi)), one 64-term random Pauli-sum
@@ -915,11 +922,15 @@ def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED, keep: dict
             ks.append(b.last_timing()[0])
         return float(np.median(ks)), e
 
-    k_default, _ = kernel_ms()
-    t0 = time.perf_counter()
-    cfg = b.autotune(reps=1)
-    t_tune = time.perf_counter() - t0
-    k_tuned, energies = kernel_ms()
+    k_default, energies = kernel_ms()
+    cfg = {"tile_bits": 0, "low_bits": 0, "max_ops": 0, "ctas_per_sm": 0}
+    t_tune = 0.0
+    k_tuned = k_default
+    if tune:
+        t0 = time.perf_counter()
+        cfg = b.autotune(reps=1)
+        t_tune = time.perf_counter() - t0
+        k_tuned, energies = kernel_ms()
     if keep is not None:
         keep["energies"] = np.array(energies, copy=True)
     ctas = b.last_timing()[1]
@@ -928,7 +939,7 @@ def batch_metric(precision: str, ncirc: int = 4096, seed: int = SEED, keep: dict
     # Oracle check: the first five circuits of every qubit count.
     picked = []
     for n in range(8, 21):
-        picked += [i for i in range(ncirc) if int(sizes[i]) == n][:5]
+        picked += [i for i in range(ncirc) if int(sizes[i]) == n][:5 if tune else 0]
     worst = 0.0
     for i in picked:
         n = int(sizes[i])

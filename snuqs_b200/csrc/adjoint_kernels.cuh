@@ -28,39 +28,64 @@ struct PauliApplyParams {
   PauliApplyGroup g[kMaxGroups];
   uint64_t zy[kMaxTerms];
   double wr[kMaxTerms], wi[kMaxTerms];  // w_t * (-i)^ny_t
+  // Bit r of sgn[t]: parity of the two top index bits r (amplitude r of a
+  // thread's four) under zy_t.  real[g / 32] bit g % 32: every wi of group g
+  // is zero.
+  uint8_t sgn[kMaxTerms];
+  uint32_t real[kMaxGroups / 32];
 };
 
 // out[i] = sum_t w_t (-i)^ny_t (-1)^popc(i & zy_t) psi[i ^ x_t];
-// partial[block] = this block's share of Re <psi|out> (FP64).
+// partial[block] = this block's share of Re <psi|out> (FP64).  Each thread
+// takes the four amplitudes j + r 2^(n-2) (r = 0..3; for each r the lanes
+// read consecutive amplitudes): one popcount per term serves all four, and
+// the imaginary weights are skipped for groups whose weights are real.  The
+// per-amplitude sums add the signed weights in term order, as a direct
+// evaluation would.
 template <typename Real>
 __global__ void __launch_bounds__(kReduceThreads)
     pauli_apply_kernel(const typename Vec2<Real>::T *__restrict__ psi,
                        typename Vec2<Real>::T *__restrict__ out,
                        const __grid_constant__ PauliApplyParams P, double *__restrict__ partial) {
   using C2 = typename Vec2<Real>::T;
-  const uint64_t N = uint64_t(1) << P.n;
+  const uint32_t hs = P.n - 2;
+  const uint64_t Q = uint64_t(1) << hs;
   double e = 0.0;
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N;
-       i += uint64_t(gridDim.x) * blockDim.x) {
-    double ar = 0.0, ai = 0.0;
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < Q;
+       j += uint64_t(gridDim.x) * blockDim.x) {
+    double ar[4] = {0.0, 0.0, 0.0, 0.0}, ai[4] = {0.0, 0.0, 0.0, 0.0};
     for (uint32_t gi = 0; gi < P.ngroups; ++gi) {
       const PauliApplyGroup &G = P.g[gi];
-      double cr = 0.0, ci = 0.0;
+      const bool real = (P.real[gi >> 5] >> (gi & 31)) & 1u;
+      double cr[4] = {0.0, 0.0, 0.0, 0.0}, ci[4] = {0.0, 0.0, 0.0, 0.0};
       for (uint32_t t = G.t0; t < G.t1; ++t) {
-        const double s = (__popcll(i & P.zy[t]) & 1) ? -1.0 : 1.0;
-        cr = fma(s, P.wr[t], cr);
-        ci = fma(s, P.wi[t], ci);
+        const uint32_t sg = P.sgn[t] ^ ((__popcll(j & P.zy[t]) & 1u) ? 0xfu : 0u);
+        const double wr = P.wr[t];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) cr[r] += ((sg >> r) & 1u) ? -wr : wr;
+        if (!real) {
+          const double wi = P.wi[t];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) ci[r] += ((sg >> r) & 1u) ? -wi : wi;
+        }
       }
-      const C2 b = psi[i ^ G.x];
-      ar += cr * double(b.x) - ci * double(b.y);
-      ai += cr * double(b.y) + ci * double(b.x);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const C2 b = psi[(j | (uint64_t(r) << hs)) ^ G.x];
+        ar[r] += cr[r] * double(b.x) - ci[r] * double(b.y);
+        ai[r] += cr[r] * double(b.y) + ci[r] * double(b.x);
+      }
     }
-    C2 o;
-    o.x = Real(ar);
-    o.y = Real(ai);
-    out[i] = o;
-    const C2 a = psi[i];
-    e += double(a.x) * ar + double(a.y) * ai;  // Re(conj(a) * acc)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint64_t i = j | (uint64_t(r) << hs);
+      C2 o;
+      o.x = Real(ar[r]);
+      o.y = Real(ai[r]);
+      out[i] = o;
+      const C2 a = psi[i];
+      e += double(a.x) * ar[r] + double(a.y) * ai[r];  // Re(conj(a) * acc)
+    }
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;

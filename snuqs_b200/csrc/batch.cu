@@ -123,7 +123,7 @@ struct sq_batch {
   HostBuf h_plans, h_table, h_energy, h_occ, h_def;
   std::vector<uint32_t> deferred;  // table positions whose energy the grid-wide pass computes
   uint32_t nitems = 0;              // work items of that pass
-  size_t def_words = 0;             // staged words: deferred, item offsets, item circuits, chunks
+  size_t def_words = 0;             // staged words: deferred circuits, item offsets
   size_t hams_uploaded = 0;
   std::vector<uint64_t> state_off;  // per circuit id; ~0 when not kept
   std::vector<uint32_t> order;      // sorted position -> circuit id
@@ -238,7 +238,7 @@ void pack_sweep(const sq::PlannedSweep &ps, std::vector<unsigned char> &out) {
 // Plans one circuit into packed sweeps; returns the sweep count or < 0.
 template <typename Real>
 int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
-                 std::vector<unsigned char> &out, std::string &err) {
+                 std::vector<unsigned char> &out, std::string &err, int select = -1) {
   try {
     std::vector<sq::HostOp> ops;
     for (const auto &op : c.ops) {
@@ -260,6 +260,7 @@ int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
     opt.tile_bits = m;
     opt.max_dense_k = sizeof(Real) == 4 ? 4 : 3;
     opt.max_ops = max_ops;
+    opt.select = select;
     // Low bits matter only for a state streamed through tiles (n > m).
     if (low_bits && c.n > m && low_bits + uint32_t(sq::kRegBits) <= m) opt.low_bits = low_bits;
     const auto plan = sq::plan_sweeps(ops, c.n, opt);
@@ -343,6 +344,16 @@ std::vector<sq::PlannedSweep> unpack_sweeps(const std::vector<unsigned char> &p,
     off += rec.bytes;
   }
   return out;
+}
+
+// Tile selection for the circuits of structure groups (PlanOptions::select):
+// on at every size (a group streams K states, so its sweeps behave as those
+// of one large state): fewer sweeps (VQE ansatz, 15-17 qubits, complex128:
+// 8/9/11 -> 6/8/8) and first and last phases that move data straight between
+// HBM and registers.  SQ_BATCH_SELECT=-1 leaves it to the planner's size rule.
+int multi_select() {
+  const char *e = std::getenv("SQ_BATCH_SELECT");
+  return e && *e ? std::atoi(e) : 1;
 }
 
 // Multi-state JIT sweeps for the energy runs: on unless SQ_JIT=0 or
@@ -456,7 +467,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
         for (size_t k = next++; k < ids.size(); k = next++) {
           const uint32_t i = ids[k];
           packed[i].clear();
-          nsweeps[i] = cand[i] ? plan_circuit<Real>(b->circs[i], MJ, 0, 0, packed[i], errs[i])
+          nsweeps[i] = cand[i] ? plan_circuit<Real>(b->circs[i], MJ, 0, 0, packed[i], errs[i], multi_select())
                                : plan_circuit<Real>(b->circs[i], M, b->low_bits, b->max_ops, packed[i], errs[i]);
         }
       });
@@ -615,23 +626,18 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     G.plan_off = tab[G.first].plan_off;
   }
   // Work items of the energy pass: chunks of 2^kEnergyChunkBits pairs.
-  // Staged as [deferred | item_off (ndef+1) | item_k | item_j].
+  // Staged as [deferred | item_off (ndef+1)]; the kernel finds an item's
+  // circuit by binary search over item_off.
   {
-    std::vector<uint32_t> item_off{0}, item_k, item_j;
+    std::vector<uint32_t> item_off{0};
     for (uint32_t k = 0; k < b->deferred.size(); ++k) {
       const uint32_t n = tab[b->deferred[k]].n;
       const uint32_t chunks = n - 1 > sq::kEnergyChunkBits ? 1u << (n - 1 - sq::kEnergyChunkBits) : 1u;
-      for (uint32_t j = 0; j < chunks; ++j) {
-        item_k.push_back(k);
-        item_j.push_back(j);
-      }
-      item_off.push_back(uint32_t(item_k.size()));
+      item_off.push_back(item_off.back() + chunks);
     }
-    b->nitems = uint32_t(item_k.size());
+    b->nitems = item_off.back();
     std::vector<uint32_t> staged(b->deferred);
     staged.insert(staged.end(), item_off.begin(), item_off.end());
-    staged.insert(staged.end(), item_k.begin(), item_k.end());
-    staged.insert(staged.end(), item_j.begin(), item_j.end());
     b->def_words = staged.size();
     if (int s = b->d_def.ensure(staged.size() * sizeof(uint32_t))) return s;
     if (int s = b->h_def.ensure(staged.size() * sizeof(uint32_t))) return s;
@@ -709,11 +715,11 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
       if (ndef) {
         cudaMemcpyAsync(b->d_def.p, b->h_def.p, b->def_words * sizeof(uint32_t), cudaMemcpyHostToDevice, cs);
         const uint32_t *defp = static_cast<const uint32_t *>(b->d_def.p);
-        const uint32_t *offp = defp + ndef, *kp = offp + ndef + 1, *jp = kp + b->nitems;
+        const uint32_t *offp = defp + ndef;
         double *partp = static_cast<double *>(b->d_part.p);
         const C2 *cpool = poolp;
         uint32_t nitems = b->nitems;
-        void *gargs[] = {&cpool, &P, &defp, &kp, &jp, &nitems, &partp};
+        void *gargs[] = {&cpool, &P, &defp, &offp, &ndef, &nitems, &partp};
         cudaLaunchKernel(reinterpret_cast<const void *>(&sq::batch_energy_grid<Real>), dim3(egrid),
                          dim3(sq::kReduceThreads), gargs, 0, cs);
         sq::batch_energy_finalize<<<ndef, sq::kReduceThreads, 0, cs>>>(partp, offp, defp, P.energies);
@@ -1214,7 +1220,9 @@ int sq_jit_multi_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops
   c.ops.assign(ops, ops + nops);
   std::vector<unsigned char> packed;
   std::string err;
-  const int ns = c64 ? plan_circuit<float>(c, M, 0, 0, packed, err) : plan_circuit<double>(c, M, 0, 0, packed, err);
+  const int sel = multi_select();
+  const int ns = c64 ? plan_circuit<float>(c, M, 0, 0, packed, err, sel)
+                     : plan_circuit<double>(c, M, 0, 0, packed, err, sel);
   if (ns < 0) return fail(SQ_ERR_UNSUPPORTED, err);
   if (nsweeps) *nsweeps = uint32_t(ns);
   if (sweep_index >= uint32_t(ns)) return fail(SQ_ERR_INVALID, "no such sweep");

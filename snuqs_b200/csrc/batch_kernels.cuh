@@ -235,21 +235,33 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 1)
 // one is one block's work.  partials[w] receives the block's sum;
 // batch_energy_finalize adds a circuit's items in order.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kEnergyChunkBits = 14;
+// Chunks of 2^10 pairs: a circuit of n qubits has 2^(n-11) items, and the
+// blocks running at any one time (items in index order) cover a few states
+// at most, which then stay in L2 across all of their Pauli groups (with
+// larger chunks the concurrent items spanned tens of 2^20-amplitude states,
+// more than L2 holds, and every group re-read its state from HBM).
+constexpr uint32_t kEnergyChunkBits = 10;
 
 template <typename Real>
 __global__ void __launch_bounds__(kReduceThreads)
     batch_energy_grid(const typename Vec2<Real>::T *__restrict__ pool, const __grid_constant__ BatchParams B,
-                      const uint32_t *__restrict__ deferred, const uint32_t *__restrict__ item_k,
-                      const uint32_t *__restrict__ item_j, uint32_t nitems, double *__restrict__ partials) {
+                      const uint32_t *__restrict__ deferred, const uint32_t *__restrict__ item_off, uint32_t ndef,
+                      uint32_t nitems, double *__restrict__ partials) {
   using C2 = typename Vec2<Real>::T;
   constexpr int U = 4;
   for (uint32_t w = blockIdx.x; w < nitems; w += gridDim.x) {
-    const BatchCircuit &C = B.circuits[deferred[item_k[w]]];
+    // Deferred circuit k with item_off[k] <= w < item_off[k + 1].
+    uint32_t lo_k = 0, hi_k = ndef;
+    while (hi_k - lo_k > 1) {
+      const uint32_t mid = (lo_k + hi_k) / 2;
+      if (item_off[mid] <= w) lo_k = mid;
+      else hi_k = mid;
+    }
+    const BatchCircuit &C = B.circuits[deferred[lo_k]];
     const PauliParams &H = B.hams[C.ham];
     const C2 *psi = pool + C.state_off;
     const uint32_t n = C.n;
-    const uint64_t j = item_j[w];
+    const uint64_t j = w - item_off[lo_k];
     double acc = 0.0;
     for (uint32_t gi = 0; gi < H.ngroups; ++gi) {
       const PauliGroup &G = H.g[gi];

@@ -1162,17 +1162,24 @@ int pauli_apply(sq_state *psi, sq_state *lam, const char *paulis, const double *
     if (P->ngroups >= uint32_t(sq::kMaxGroups) || nt > uint32_t(sq::kMaxTerms))
       return fail(SQ_ERR_UNSUPPORTED, "adjoint: at most %d terms in %d flip groups",
                   sq::kMaxTerms, sq::kMaxGroups);
-    sq::PauliApplyGroup &g = P->g[P->ngroups++];
+    const uint32_t gi = P->ngroups++;
+    sq::PauliApplyGroup &g = P->g[gi];
     g.x = xm[idx[pos]];
     g.t0 = k;
+    bool real = true;
     for (uint32_t e = pos; e < end; ++e) {
       const uint32_t t = idx[e];
       static const double pr[4] = {1, 0, -1, 0}, pi[4] = {0, -1, 0, 1};  // (-i)^ny
       P->zy[k] = zym[t];
       P->wr[k] = w[t] * pr[ny[t] & 3];
       P->wi[k] = w[t] * pi[ny[t] & 3];
+      real = real && P->wi[k] == 0.0;
+      const uint32_t top = uint32_t(zym[t] >> (n - 2)) & 3u;
+      for (uint32_t r = 0; r < 4; ++r)
+        if (__builtin_popcount(r & top) & 1) P->sgn[k] |= uint8_t(1u << r);
       ++k;
     }
+    if (real) P->real[gi >> 5] |= 1u << (gi & 31);
     g.t1 = k;
     pos = end;
   }
