@@ -152,6 +152,13 @@ struct sq_batch {
   // and the table positions [0, n_interp) that batch_kernel runs.
   std::vector<MultiGroup> groups;
   uint32_t n_interp = 0;
+  // Angle changes (sq_batch_set_angles) bump values_version only: the next
+  // energy run re-emits each circuit's plan from its sweep recipes with the
+  // new coefficients (no planning) when the ops keep their signature.
+  uint64_t values_version = 0, planned_values = 0;
+  std::vector<std::vector<sq::SweepRecipe>> recipes;    // per circuit id
+  std::vector<std::pair<uint64_t, uint64_t>> sigs;      // per circuit id
+  std::vector<uint64_t> plan_at, plan_size;             // packed plan in h_plans, per circuit id
 };
 
 namespace {
@@ -236,26 +243,43 @@ void pack_sweep(const sq::PlannedSweep &ps, std::vector<unsigned char> &out) {
 }
 
 // Plans one circuit into packed sweeps; returns the sweep count or < 0.
+// A circuit's gates as planner ops (identities dropped).  False with `err`.
+bool circuit_host_ops(const Circ &c, std::vector<sq::HostOp> &ops, std::string &err) {
+  ops.clear();
+  for (const auto &op : c.ops) {
+    std::vector<cplx> mat;
+    if (op.gate < 0) {
+      const size_t d = size_t(1) << op.k;
+      mat.resize(d * d);
+      std::memcpy(mat.data(), op.matrix, d * d * sizeof(cplx));
+    } else if (sq::gate_matrix(op.gate, op.angles, op.nangles, mat) < 0) {
+      err = "batch: bad gate or angle count";
+      return false;
+    }
+    std::vector<int> tb;
+    for (uint32_t j = 0; j < op.k; ++j) tb.push_back(int(c.n - 1 - op.qubits[j]));
+    sq::HostOp h;
+    if (sq::analyse_op(mat, tb, 0, 0, h)) ops.push_back(h);
+  }
+  return true;
+}
+
+std::pair<uint64_t, uint64_t> signature_hash(const std::vector<sq::HostOp> &ops) {
+  return sq::op_signature_hash(ops);
+}
+
+// Plans one circuit of an energy run into packed sweeps.  recipes / sig (when
+// given): the sweeps' recipes and the ops' signature hash, for re-emitting the
+// plan when only angles change.
 template <typename Real>
 int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
-                 std::vector<unsigned char> &out, std::string &err, int select = -1) {
+                 std::vector<unsigned char> &out, std::string &err, int select = -1,
+                 std::vector<sq::SweepRecipe> *recipes = nullptr, std::pair<uint64_t, uint64_t> *sig = nullptr) {
   try {
     std::vector<sq::HostOp> ops;
-    for (const auto &op : c.ops) {
-      std::vector<cplx> mat;
-      if (op.gate < 0) {
-        const size_t d = size_t(1) << op.k;
-        mat.resize(d * d);
-        std::memcpy(mat.data(), op.matrix, d * d * sizeof(cplx));
-      } else if (sq::gate_matrix(op.gate, op.angles, op.nangles, mat) < 0) {
-        err = "batch: bad gate or angle count";
-        return -1;
-      }
-      std::vector<int> tb;
-      for (uint32_t j = 0; j < op.k; ++j) tb.push_back(int(c.n - 1 - op.qubits[j]));
-      sq::HostOp h;
-      if (sq::analyse_op(mat, tb, 0, 0, h)) ops.push_back(h);
-    }
+    if (!circuit_host_ops(c, ops, err)) return -1;
+    if (sig) *sig = signature_hash(ops);
+    if (recipes) recipes->clear();
     sq::PlanOptions opt;
     opt.tile_bits = m;
     opt.max_dense_k = sizeof(Real) == 4 ? 4 : 3;
@@ -271,6 +295,7 @@ int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
         return -1;
       }
       pack_sweep<Real>(pl.sweep, out);
+      if (recipes) recipes->push_back(pl.sweep.recipe);
       ++sweeps;
     }
     return sweeps;
@@ -429,6 +454,59 @@ int batch_shape(uint32_t m, const void *&fn, int &threads, size_t &smem, int &pe
   return SQ_OK;
 }
 
+// Re-emits every circuit's packed plan (in the pinned staging buffer) for
+// its current angles from the sweep recipes of the last planning.  False
+// when a circuit's ops changed signature or a rebuilt sweep changed form (the
+// caller then plans every circuit anew).
+template <typename Real>
+bool refresh_values(sq_batch *b) {
+  const size_t nc = b->circs.size();
+  if (b->recipes.size() != nc || b->sigs.size() != nc || b->plan_at.size() != nc || !b->h_plans.p) return false;
+  unsigned char *hp = static_cast<unsigned char *>(b->h_plans.p);
+  std::atomic<size_t> next{0};
+  std::atomic<bool> ok{true};
+  auto work = [&] {
+    std::vector<sq::HostOp> ops;
+    std::vector<unsigned char> packed, old;
+    std::string err;
+    for (size_t i = next++; i < nc && ok; i = next++) {
+      const Circ &c = b->circs[i];
+      if (!circuit_host_ops(c, ops, err) || signature_hash(ops) != b->sigs[i]) {
+        ok = false;
+        break;
+      }
+      old.assign(hp + b->plan_at[i], hp + b->plan_at[i] + b->plan_size[i]);
+      packed.clear();
+      size_t off = 0;
+      bool good = true;
+      for (const sq::SweepRecipe &r : b->recipes[i]) {
+        if (off + sizeof(sq::PackedSweep) > old.size()) {
+          good = false;
+          break;
+        }
+        const auto &rec = *reinterpret_cast<const sq::PackedSweep *>(old.data() + off);
+        sq::PlannedSweep ps;
+        if (!sq::rebuild_sweep(r, ops, c.n, rec.h.m, rec.h.l, ps)) {
+          good = false;
+          break;
+        }
+        pack_sweep<Real>(ps, packed);
+        off += rec.bytes;
+      }
+      if (!good || packed.size() != old.size() || !same_structure(old, packed, coef_ranges<Real>(old))) {
+        ok = false;
+        break;
+      }
+      std::memcpy(hp + b->plan_at[i], packed.data(), packed.size());
+    }
+  };
+  const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nth; ++t) pool.emplace_back(work);
+  for (auto &th : pool) th.join();
+  return ok;
+}
+
 template <typename Real>
 int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   using C2 = typename sq::Vec2<Real>::T;
@@ -439,10 +517,16 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   int threads = 0, per_sm = 0;
   size_t smem = 0;
   if (int s = batch_shape<Real>(M, fn, threads, smem, per_sm)) return s;
-  const bool replan = b->planned_version != b->version || b->planned_m != M ||
-                      b->planned_l != b->low_bits || b->planned_ops != b->max_ops;
+  bool replan = b->planned_version != b->version || b->planned_m != M || b->planned_l != b->low_bits ||
+                b->planned_ops != b->max_ops;
+  // Only angles changed: new coefficients into the same plans, else plan anew.
+  if (!replan && b->planned_values != b->values_version) {
+    if (refresh_values<Real>(b)) b->planned_values = b->values_version;
+    else replan = true;
+  }
   size_t plan_bytes = b->planned_bytes;
   if (replan) {
+  b->planned_values = b->values_version;
   b->deferred.clear();
   int sms = 0;
   SQB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
@@ -467,12 +551,16 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
         for (size_t k = next++; k < ids.size(); k = next++) {
           const uint32_t i = ids[k];
           packed[i].clear();
-          nsweeps[i] = cand[i] ? plan_circuit<Real>(b->circs[i], MJ, 0, 0, packed[i], errs[i], multi_select())
-                               : plan_circuit<Real>(b->circs[i], M, b->low_bits, b->max_ops, packed[i], errs[i]);
+          nsweeps[i] = cand[i] ? plan_circuit<Real>(b->circs[i], MJ, 0, 0, packed[i], errs[i], multi_select(),
+                                                    &b->recipes[i], &b->sigs[i])
+                               : plan_circuit<Real>(b->circs[i], M, b->low_bits, b->max_ops, packed[i], errs[i], -1,
+                                                    &b->recipes[i], &b->sigs[i]);
         }
       });
     for (auto &th : pool) th.join();
   };
+  b->recipes.assign(nc, {});
+  b->sigs.assign(nc, {0, 0});
   {
     std::vector<uint32_t> all(nc);
     for (size_t i = 0; i < nc; ++i) all[i] = uint32_t(i);
@@ -603,10 +691,14 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   auto *tab = static_cast<sq::BatchCircuit *>(b->h_table.p);
   unsigned char *hp = static_cast<unsigned char *>(b->h_plans.p);
   size_t off = 0;
+  b->plan_at.assign(nc, 0);
+  b->plan_size.assign(nc, 0);
   for (size_t pos = 0; pos < nc; ++pos) {
     const uint32_t id = b->order[pos];
     const Circ &c = b->circs[id];
     std::memcpy(hp + off, packed[id].data(), packed[id].size());
+    b->plan_at[id] = off;
+    b->plan_size[id] = packed[id].size();
     sq::BatchCircuit &t = tab[pos];
     t.n = c.n;
     t.nsweeps = uint32_t(nsweeps[id]);
@@ -1099,7 +1191,7 @@ int sq_batch_set_angles(sq_batch *b, uint32_t circuit, const double *angles, uin
       op.angles[j] = angles[k++];
     }
   if (k != count) return fail(SQ_ERR_INVALID, "batch: angle count mismatch");
-  b->version++;
+  b->values_version++;
   return SQ_OK;
 }
 

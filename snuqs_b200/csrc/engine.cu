@@ -108,7 +108,45 @@ struct sq_state {
   uint32_t *errword = nullptr;
   void *rscratch = nullptr;  // result kernels' scratch (results.cu)
   size_t rscratch_bytes = 0;
+  // The last plans, reused for the same gate sequence with other values (a
+  // circuit run again with other angles): sq::rebuild_plan re-emits them
+  // from their recipes without planning.  Keyed by the ops' signature hash
+  // and the plan options.
+  struct PlanMemo {
+    std::pair<uint64_t, uint64_t> sig{0, 0};
+    uint64_t opts = ~uint64_t(0);
+    std::vector<sq::PlannedLaunch> plan;
+  };
+  PlanMemo flush_memo, fwd_memo, rev_memo;
 };
+
+// The plan options a memo entry depends on, packed into one word.
+static uint64_t plan_opts_key(const sq::PlanOptions &o) {
+  return uint64_t(o.tile_bits) | (uint64_t(o.low_bits) << 8) | (uint64_t(o.max_dense_k) << 16) |
+         (uint64_t(o.reg_bits) << 24) | (uint64_t(o.max_ops) << 32) | (uint64_t(o.reorder) << 48) |
+         (uint64_t(o.remap) << 49) | (uint64_t(uint8_t(o.select)) << 50);
+}
+
+// Plans `ops`, or re-emits the memo's plan when the ops have its signature
+// and options (and every sweep of it has a recipe); the memo then holds the
+// new plan.  Throws what plan_sweeps throws.
+static std::vector<sq::PlannedLaunch> plan_memo(sq_state::PlanMemo &memo, const std::vector<sq::HostOp> &ops,
+                                                uint32_t n, const sq::PlanOptions &opt) {
+  const auto sig = sq::op_signature_hash(ops);
+  const uint64_t key = plan_opts_key(opt);
+  if (memo.opts == key && memo.sig == sig) {
+    std::vector<sq::PlannedLaunch> plan = memo.plan;
+    if (sq::rebuild_plan(plan, ops, n)) {
+      memo.plan = plan;
+      return plan;
+    }
+  }
+  std::vector<sq::PlannedLaunch> plan = sq::plan_sweeps(ops, n, opt);
+  memo.sig = sig;
+  memo.opts = key;
+  memo.plan = plan;
+  return plan;
+}
 
 // JIT-specialised sweeps pay a one-off NVRTC compile per distinct sweep
 // structure; below this size the generic kernel's sweeps are too short for
@@ -479,7 +517,7 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
       opt.low_bits = sq::auto_low_bits(c64, n, opt.tile_bits);
     // Remapping sweeps exist only as JIT-specialised kernels.
     opt.remap = s->remap && use_jit(s);
-    plan = sq::plan_sweeps(ops, n, opt);
+    plan = plan_memo(s->flush_memo, ops, n, opt);
   } catch (const std::exception &e) {
     return fail(SQ_ERR_INVALID, "planner: %s", e.what());
   }
@@ -498,7 +536,7 @@ static int flush_impl(sq_state *s, cudaStream_t st) {
     if (!ready) {
       try {
         opt.remap = false;
-        plan = sq::plan_sweeps(ops, n, opt);
+        plan = plan_memo(s->flush_memo, ops, n, opt);
       } catch (const std::exception &e) {
         return fail(SQ_ERR_INVALID, "planner: %s", e.what());
       }
@@ -1284,7 +1322,7 @@ int adjoint_impl(sq_state *psi, sq_state *lam, const sq::AdjointPlan &ap, const 
   const bool jit = use_jit(psi);
   std::thread rthread([&] {
     try {
-      rplan = sq::plan_sweeps(ap.reverse, n, ropt);
+      rplan = plan_memo(psi->rev_memo, ap.reverse, n, ropt);
       if (jit) {
         std::vector<const sq::PlannedSweep *> sweeps;
         for (const auto &pl : rplan)
@@ -1302,7 +1340,7 @@ int adjoint_impl(sq_state *psi, sq_state *lam, const sq::AdjointPlan &ap, const 
     }
   } joiner{rthread};
   try {
-    fplan = sq::plan_sweeps(ap.forward, n, fopt);
+    fplan = plan_memo(psi->fwd_memo, ap.forward, n, fopt);
   } catch (const std::exception &e) {
     return fail(SQ_ERR_INVALID, "adjoint planner: %s", e.what());
   }

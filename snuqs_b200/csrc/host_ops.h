@@ -3,6 +3,7 @@
 #include <complex>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "sq_plan.h"
@@ -48,6 +49,19 @@ struct HostOp {
 bool analyse_op(const std::vector<cplx> &m, const std::vector<int> &tbits, uint64_t cmask,
                 uint64_t cval, HostOp &out);
 
+// How a planned sweep was formed, so that the same gate sequence with other
+// values (other angles) is re-emitted without planning (rebuild_plan): the
+// tile bits, every phase's register bits and first op, and the position of
+// each of the sweep's ops in the planner's input.  Empty `src`: not
+// rebuildable (a sweep of a remapping plan).
+struct SweepRecipe {
+  uint64_t S = 0;
+  std::vector<uint64_t> phase_regs;
+  std::vector<uint32_t> phase_first;
+  std::vector<uint32_t> src;
+  uint32_t reg_bits = 0, max_dense_k = 0;
+};
+
 // A planned launch: a fused sweep, or one unfused gate.
 struct PlannedSweep {
   SweepHeader h;
@@ -57,12 +71,14 @@ struct PlannedSweep {
   uint32_t ngates = 0;  // queued ops it carries
   // Adjoint sweeps: global inner-product slot of each local slot 0, 1, ...
   std::vector<uint32_t> inner_global;
+  SweepRecipe recipe;
 };
 
 struct PlannedLaunch {
   bool is_sweep = true;
   PlannedSweep sweep;
   HostOp gate;  // unfused gate (dense, any k; cmask/cval are its controls)
+  uint32_t gate_src = 0;  // its position in the planner's input
 };
 
 struct PlanOptions {
@@ -106,5 +122,24 @@ inline uint32_t auto_low_bits(bool c64, uint32_t n, uint32_t m) {
 // Packs ops (in circuit order) into fused sweeps for an n-qubit state.
 std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t n,
                                        const PlanOptions &opt);
+
+// The op structure a plan depends on: per op its kind, targets, controls and
+// inner-product slot, not its values.  Two op lists with equal signatures
+// can share one plan's recipes.
+std::vector<uint64_t> op_signature(const std::vector<HostOp> &ops);
+// Two independent 64-bit FNV-1a hashes of op_signature(ops).
+std::pair<uint64_t, uint64_t> op_signature_hash(const std::vector<HostOp> &ops);
+
+// Re-emits `plan` (made by plan_sweeps for ops of the same signature) for
+// `ops`: every sweep rebuilt from its recipe with the new values.  False,
+// leaving `plan` unusable, when a sweep has no recipe or when a rebuilt
+// sweep's header, phases or ops differ from the old ones (a value that changes
+// an op's form, e.g. an angle that makes a dense gate a permutation); the
+// caller then plans anew.
+bool rebuild_plan(std::vector<PlannedLaunch> &plan, const std::vector<HostOp> &ops, uint32_t n);
+// One sweep of such a plan from its recipe (m, l: its tile and low bits);
+// false when the recipe is empty or names an op past `ops`.
+bool rebuild_sweep(const SweepRecipe &r, const std::vector<HostOp> &ops, uint32_t n, uint32_t m, uint32_t l,
+                   PlannedSweep &out);
 
 }  // namespace sq

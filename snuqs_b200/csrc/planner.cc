@@ -86,8 +86,6 @@ struct SweepBuilder {
 // Position of global bit b within the ascending bit list of mask.
 int rank_in(uint64_t mask, int b) { return popc64(mask & ((uint64_t(1) << b) - 1)); }
 
-// Picks the cheapest sweep-op kind for a dense k-qubit matrix in canonical
-// order and appends its coefficients.
 // Pauli form of an inner-product op's K (canonical local order): K = alpha P
 // with P_(r, r^x) = (-1)^popc(r & z) times K's row-0 entry in column x and
 // every other entry zero, each to within 1e-14 |alpha| (rotation generators
@@ -113,6 +111,8 @@ bool pauli_form(const cplx *K, int d, bool diag, uint32_t &x, uint32_t &z) {
   return true;
 }
 
+// Picks the cheapest sweep-op kind for a dense k-qubit matrix in canonical
+// order and appends its coefficients.
 void encode_dense(SweepOp &so, const std::vector<cplx> &cm, int k, std::vector<cplx> &coef) {
   const int d = 1 << k;
   auto M = [&](int r, int c) { return cm[size_t(r) * d + c]; };
@@ -675,6 +675,19 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
   tab.base = work.data();
   tab.v.resize(work.size());
   for (const auto &o : work) tab.set(o, opt);
+  // Recipe of a finished sweep (none when the plan remaps: its later ops are
+  // relabelled copies).
+  auto recipe = [&](const SweepBuilder &sb) {
+    SweepRecipe r;
+    if (remap) return r;
+    r.S = sb.S;
+    r.phase_regs = sb.phase_regs;
+    r.phase_first = sb.phase_first;
+    r.reg_bits = sb.reg_bits;
+    r.max_dense_k = sb.max_dense_k;
+    for (const HostOp *op : sb.ops) r.src.push_back(uint32_t(op - work.data()));
+    return r;
+  };
   size_t head = 0;  // rem[head..] still to place
   while (head < rem.size()) {
     const HostOp &first = *rem[head];
@@ -688,6 +701,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       PlannedLaunch pl;
       pl.is_sweep = false;
       pl.gate = first;
+      pl.gate_src = uint32_t(&first - work.data());
       out.push_back(std::move(pl));
       ++head;
       continue;
@@ -775,6 +789,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
       PlannedLaunch pl;
       pl.is_sweep = true;
       pl.sweep = sb.finish();
+      pl.sweep.recipe = recipe(sb);
       out.push_back(std::move(pl));
       std::vector<size_t> again(skipped_idx);
       again.insert(again.end(), back_idx.begin(), back_idx.end());
@@ -817,6 +832,7 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
     PlannedLaunch pl;
     pl.is_sweep = true;
     pl.sweep = sb.finish();
+    pl.sweep.recipe = recipe(sb);
     out.push_back(std::move(pl));
     // Remaining = skipped (in order) + everything after i.
     std::vector<const HostOp *> next(skipped.begin(), skipped.end());
@@ -856,6 +872,73 @@ std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t 
     }
   }
   return out;
+}
+
+std::vector<uint64_t> op_signature(const std::vector<HostOp> &ops) {
+  std::vector<uint64_t> sig;
+  sig.reserve(ops.size() * 4);
+  for (const HostOp &op : ops) {
+    sig.push_back(uint64_t(op.kind) | (uint64_t(op.inner_diag) << 8) | (uint64_t(op.tbits.size()) << 16) |
+                  (uint64_t(op.slot) << 32));
+    uint64_t t = 0;
+    for (size_t j = 0; j < op.tbits.size(); ++j) t = (t << 7) | uint64_t(op.tbits[j] & 127);
+    sig.push_back(t);
+    sig.push_back(op.cmask);
+    sig.push_back(op.cval);
+  }
+  return sig;
+}
+
+std::pair<uint64_t, uint64_t> op_signature_hash(const std::vector<HostOp> &ops) {
+  const std::vector<uint64_t> sig = op_signature(ops);
+  uint64_t a = 1469598103934665603ull, b = 0x9ae16a3b2f90404full;
+  for (uint64_t w : sig)
+    for (int k = 0; k < 8; ++k) {
+      const uint8_t x = uint8_t(w >> (8 * k));
+      a = (a ^ x) * 1099511628211ull;
+      b = (b ^ x) * 0x100000001b3ull + 0x9e3779b97f4a7c15ull;
+    }
+  return {a, b ^ sig.size()};
+}
+
+bool rebuild_sweep(const SweepRecipe &r, const std::vector<HostOp> &ops, uint32_t n, uint32_t m, uint32_t l,
+                   PlannedSweep &out) {
+  if (r.src.empty()) return false;
+  SweepBuilder sb(n, m, l);
+  sb.S = r.S;
+  sb.phase_regs = r.phase_regs;
+  sb.phase_first = r.phase_first;
+  sb.reg_bits = r.reg_bits;
+  sb.max_dense_k = r.max_dense_k;
+  for (uint32_t i : r.src) {
+    if (i >= ops.size()) return false;
+    sb.ops.push_back(&ops[i]);
+    sb.ncoef += SweepBuilder::coef_count(ops[i]);
+    if (ops[i].kind == kOpInner) ++sb.ninner;
+  }
+  out = sb.finish();
+  out.recipe = r;
+  return true;
+}
+
+bool rebuild_plan(std::vector<PlannedLaunch> &plan, const std::vector<HostOp> &ops, uint32_t n) {
+  for (PlannedLaunch &pl : plan) {
+    if (!pl.is_sweep) {
+      if (pl.gate_src >= ops.size()) return false;
+      pl.gate = ops[pl.gate_src];
+      continue;
+    }
+    PlannedSweep &old = pl.sweep;
+    PlannedSweep ns;
+    if (!rebuild_sweep(old.recipe, ops, n, old.h.m, old.h.l, ns)) return false;
+    if (std::memcmp(&ns.h, &old.h, sizeof(SweepHeader)) != 0 || ns.ph.size() != old.ph.size() ||
+        ns.op.size() != old.op.size() || ns.inner_global != old.inner_global ||
+        (!ns.ph.empty() && std::memcmp(ns.ph.data(), old.ph.data(), ns.ph.size() * sizeof(SweepPhase)) != 0) ||
+        (!ns.op.empty() && std::memcmp(ns.op.data(), old.op.data(), ns.op.size() * sizeof(SweepOp)) != 0))
+      return false;
+    old.coef.swap(ns.coef);
+  }
+  return true;
 }
 
 }  // namespace sq

@@ -44,6 +44,36 @@ def run(state, n, gates, tile_bits=12, reorder=True, low_bits=0):
     return psi, r, unf.value
 
 
+def run_rebuilt(state, n, gates_a, gates_b, tile_bits=12, reorder=True, low_bits=0):
+    """Plans gates_a, re-emits the plan for gates_b (the same gates with other
+    matrices) by rebuild_plan, emulates it; returns (state, sweeps, rebuilt)
+    with rebuilt False when the plan was made anew instead."""
+    psi = np.array(state, dtype=np.complex128)
+    k, qoff, qs, nc, coff, cs, cv, moff, ma, mb = [], [], [], [], [], [], [], [], [], []
+    mo = 0
+    for (m, q, c, v), (m2, q2, c2, v2) in zip(gates_a, gates_b):
+        assert tuple(q) == tuple(q2) and tuple(c) == tuple(c2) and tuple(v) == tuple(v2)
+        k.append(len(q)); qoff.append(len(qs)); qs.extend(q)
+        nc.append(len(c)); coff.append(len(cs)); cs.extend(c); cv.extend(v)
+        moff.append(mo)
+        ma.append(np.asarray(m, dtype=np.complex128).ravel())
+        mb.append(np.asarray(m2, dtype=np.complex128).ravel())
+        mo += ma[-1].size
+    arr = lambda x, t: np.ascontiguousarray(np.array(x if x else [0], dtype=t))
+    K, QO, QS, NC, CO, CS, CV = (arr(x, np.int32) for x in (k, qoff, qs, nc, coff, cs, cv))
+    MO = arr(moff, np.int64)
+    MA = np.ascontiguousarray(np.concatenate(ma))
+    MB = np.ascontiguousarray(np.concatenate(mb))
+    rebuilt = ctypes.c_int(0)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    r = lib().emu_rebuild(P(psi), n, len(gates_a), P(K), P(QO), P(QS), P(NC), P(CO), P(CS), P(CV),
+                          P(MO), P(MA), P(MB), tile_bits, _reorder_code(reorder), low_bits,
+                          ctypes.byref(rebuilt))
+    if r < 0:
+        raise RuntimeError("emulator failed")
+    return psi, r, bool(rebuilt.value)
+
+
 def _reorder_code(reorder):
     return {"select": 2, "noselect": 3, "remap": 4}.get(reorder, int(bool(reorder)))
 

@@ -252,49 +252,94 @@ extern "C" {
 // controls at controls[coff[i]..] with values cvals[coff[i]..], and its
 // 4^k matrix at mats[moff[i]..] (complex128).  Returns the number of fused
 // sweeps (>= 0) or -1 on error.
+}  // extern "C"
+
+namespace {
+
+std::vector<HostOp> host_ops(int n, int nops, const int *k, const int *qoff, const int *qubits, const int *nc,
+                             const int *coff, const int *controls, const int *cvals, const long *moff,
+                             const double *mats) {
+  std::vector<HostOp> ops;
+  for (int i = 0; i < nops; ++i) {
+    std::vector<int> tb;
+    for (int j = 0; j < k[i]; ++j) tb.push_back(n - 1 - qubits[qoff[i] + j]);
+    uint64_t cm = 0, cv = 0;
+    for (int j = 0; j < nc[i]; ++j) {
+      const uint64_t bit = uint64_t(1) << (n - 1 - controls[coff[i] + j]);
+      cm |= bit;
+      if (cvals[coff[i] + j]) cv |= bit;
+    }
+    const size_t d = size_t(1) << k[i];
+    std::vector<cplx> mm(d * d);
+    std::memcpy(mm.data(), mats + 2 * moff[i], d * d * sizeof(cplx));
+    HostOp h;
+    if (analyse_op(mm, tb, cm, cv, h)) ops.push_back(h);
+  }
+  return ops;
+}
+
+PlanOptions emu_options(int tile_bits, int reorder, int low_bits) {
+  PlanOptions opt;
+  opt.tile_bits = uint32_t(tile_bits);
+  opt.reorder = reorder != 0;
+  // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection,
+  // 4 on + selection + qubit remapping
+  opt.select = (reorder == 2 || reorder == 4) ? 1 : reorder == 3 ? 0 : -1;
+  opt.remap = reorder == 4;
+  opt.low_bits = uint32_t(low_bits);
+  return opt;
+}
+
+int emulate_plan(double *state, int n, const std::vector<PlannedLaunch> &plan, int *unfused_out) {
+  int sweeps = 0, unfused = 0;
+  cplx *psi = reinterpret_cast<cplx *>(state);
+  for (const auto &pl : plan) {
+    if (pl.is_sweep) {
+      emulate_sweep(psi, pl.sweep);
+      ++sweeps;
+    } else {
+      emulate_gate(psi, uint32_t(n), pl.gate);
+      ++unfused;
+    }
+  }
+  if (unfused_out) *unfused_out = unfused;
+  return sweeps;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Plans the gates with the matrices mats_a, then re-emits that plan with
+// mats_b (same gates, other values) by rebuild_plan and emulates it on
+// `state`.  *rebuilt = 1 when the rebuild took (equal op signatures and
+// equal sweep structure), else 0 and the gates with mats_b were planned
+// anew.  Returns the number of sweeps or -1.
+int emu_rebuild(double *state, int n, int nops, const int *k, const int *qoff, const int *qubits, const int *nc,
+                const int *coff, const int *controls, const int *cvals, const long *moff, const double *mats_a,
+                const double *mats_b, int tile_bits, int reorder, int low_bits, int *rebuilt) {
+  try {
+    const auto a = host_ops(n, nops, k, qoff, qubits, nc, coff, controls, cvals, moff, mats_a);
+    const auto b = host_ops(n, nops, k, qoff, qubits, nc, coff, controls, cvals, moff, mats_b);
+    const PlanOptions opt = emu_options(tile_bits, reorder, low_bits);
+    auto plan = plan_sweeps(a, uint32_t(n), opt);
+    *rebuilt = op_signature(a) == op_signature(b) && rebuild_plan(plan, b, uint32_t(n)) ? 1 : 0;
+    if (!*rebuilt) plan = plan_sweeps(b, uint32_t(n), opt);
+    return emulate_plan(state, n, plan, nullptr);
+  } catch (const std::exception &) {
+    return -1;
+  }
+}
+
 int emu_run(double *state, int n, int nops, const int *k, const int *qoff, const int *qubits,
             const int *nc, const int *coff, const int *controls, const int *cvals,
             const long *moff, const double *mats, int tile_bits, int reorder,
             int low_bits, int *unfused_out) {
   try {
-    std::vector<HostOp> ops;
-    for (int i = 0; i < nops; ++i) {
-      std::vector<int> tb;
-      for (int j = 0; j < k[i]; ++j) tb.push_back(n - 1 - qubits[qoff[i] + j]);
-      uint64_t cm = 0, cv = 0;
-      for (int j = 0; j < nc[i]; ++j) {
-        const uint64_t bit = uint64_t(1) << (n - 1 - controls[coff[i] + j]);
-        cm |= bit;
-        if (cvals[coff[i] + j]) cv |= bit;
-      }
-      const size_t d = size_t(1) << k[i];
-      std::vector<cplx> mm(d * d);
-      std::memcpy(mm.data(), mats + 2 * moff[i], d * d * sizeof(cplx));
-      HostOp h;
-      if (analyse_op(mm, tb, cm, cv, h)) ops.push_back(h);
-    }
-    PlanOptions opt;
-    opt.tile_bits = uint32_t(tile_bits);
-    opt.reorder = reorder != 0;
-    // reorder: 0 off, 1 on (tile selection automatic), 2 on + selection, 3 on, no selection,
-    // 4 on + selection + qubit remapping
-    opt.select = (reorder == 2 || reorder == 4) ? 1 : reorder == 3 ? 0 : -1;
-    opt.remap = reorder == 4;
-    opt.low_bits = uint32_t(low_bits);
+    const auto ops = host_ops(n, nops, k, qoff, qubits, nc, coff, controls, cvals, moff, mats);
+    const PlanOptions opt = emu_options(tile_bits, reorder, low_bits);
     auto plan = plan_sweeps(ops, uint32_t(n), opt);
-    int sweeps = 0, unfused = 0;
-    cplx *psi = reinterpret_cast<cplx *>(state);
-    for (const auto &pl : plan) {
-      if (pl.is_sweep) {
-        emulate_sweep(psi, pl.sweep);
-        ++sweeps;
-      } else {
-        emulate_gate(psi, uint32_t(n), pl.gate);
-        ++unfused;
-      }
-    }
-    if (unfused_out) *unfused_out = unfused;
-    return sweeps;
+    return emulate_plan(state, n, plan, unfused_out);
   } catch (const std::exception &) {
     return -1;
   }

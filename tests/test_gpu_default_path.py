@@ -211,3 +211,24 @@ def test_remapping_sweeps_against_reference(low_bits):
             st.close()
             assert max_abs_diff(psi, ref) <= TOL128, (low_bits, remap)
         assert launches[1] <= launches[0] + 1
+
+
+def test_same_circuit_with_new_angles_on_one_state():
+    """A state runs one gate sequence with three sets of angles (its plan is
+    re-emitted from the sweep recipes after the first), each against the
+    reference; then a different sequence (planned anew)."""
+    n = 22
+    rng = np.random.default_rng(5)
+    st = capi.State(n)
+    for k in range(3):
+        ops = circuits.vqe_ansatz(n, rng.uniform(0, 2 * np.pi, 12 * n))
+        st.init_basis(0)
+        st.apply_ops(ops)
+        st.flush()
+        assert max_abs_diff(st.to_host(), reference(ops, n)) <= TOL128, k
+    ops = circuits.random_mix(n, 200, seed=3)
+    st.init_basis(0)
+    st.apply_ops(ops)
+    st.flush()
+    assert max_abs_diff(st.to_host(), reference(ops, n)) <= TOL128
+    st.close()

@@ -129,3 +129,47 @@ def test_remapping_saves_sweeps_on_the_benchmark_mix():
     plain = emulator.plan_stats(30, g, tile_bits=11, reorder="select", low_bits=3)["sweeps"]
     remap = emulator.plan_stats(30, g, tile_bits=11, reorder="remap", low_bits=3)["sweeps"]
     assert remap < plain
+
+
+def _param_circuit(n, angles):
+    """Rotations (RotX/RotY/RotZ/PhaseShift/ZZ/XX/U), fixed CX/CZ/H and a
+    controlled rotation, angles from `angles` in order."""
+    it = iter(angles)
+    ops = []
+    for l in range(3):
+        for q in range(n):
+            ops.append(("RotY", (q,), (next(it),)))
+            ops.append(("RotZ", (q,), (next(it),)))
+        for q in range(0, n - 1, 2):
+            ops.append(("ZZ", (q, q + 1), (next(it),)))
+        for q in range(n - 1):
+            ops.append(("CX", (q, q + 1), ()))
+        ops.append(("XX", (0, n - 1), (next(it),)))
+        ops.append(("PhaseShift", (n // 2,), (next(it),)))
+        ops.append(("U", (1,), (next(it), next(it), next(it))))
+        ops.append(("CPhaseShift", (2, n - 2), (next(it),)))
+        ops.append(("Hadamard", (3,), ()))
+    return ops
+
+
+@pytest.mark.parametrize("n,tb,reorder", [(13, 9, "select"), (14, 10, True), (12, 8, "noselect"), (16, 11, "select")])
+def test_rebuilt_plans_match_oracle(n, tb, reorder):
+    """A plan made for one set of angles, re-emitted for another by
+    rebuild_plan (same gates, no planning), gives the oracle's state for the
+    new angles; an angle that turns a gate into the identity (dropped by the
+    op analysis) changes the op signature and the plan is made anew."""
+    rng = np.random.default_rng(n)
+    na = len([a for op in _param_circuit(n, iter(lambda: 0.5, None)) for a in op[2]])
+    a, b = rng.uniform(0.1, 3.0, na), rng.uniform(0.1, 3.0, na)
+    ops_a, ops_b = _param_circuit(n, a), _param_circuit(n, b)
+    ref = oracle.run_ops(ops_b, n)
+    psi, sweeps, rebuilt = emulator.run_rebuilt(oracle.basis_state(n), n, gates_of(ops_a), gates_of(ops_b),
+                                                tb, reorder)
+    assert rebuilt and sweeps > 1
+    assert np.abs(psi - ref).max() <= 1e-12
+    c = b.copy()
+    c[1] = 0.0  # RotZ(0) is the identity: dropped, so the ops differ
+    ops_c = _param_circuit(n, c)
+    psi, _, rebuilt = emulator.run_rebuilt(oracle.basis_state(n), n, gates_of(ops_a), gates_of(ops_c), tb, reorder)
+    assert not rebuilt
+    assert np.abs(psi - oracle.run_ops(ops_c, n)).max() <= 1e-12
