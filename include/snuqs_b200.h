@@ -377,7 +377,9 @@ int sq_batch_last_timing(const sq_batch *b, double *kernel_ms, uint32_t *ctas);
 /* Plan statistics of the last sq_batch_run: circuits streamed through HBM
  * (more qubits than the tile), their fused sweeps, and their algorithmic HBM
  * bytes (per streamed circuit (2 x sweeps + 1) x 2^n x amplitude bytes: every
- * sweep reads and writes the state, the energy pass reads it once). */
+ * sweep reads and writes the state, the energy pass reads it once; one pass
+ * less for a circuit of a structure group whose first sweep starts from
+ * |0...0> without reading). */
 int sq_batch_stats(const sq_batch *b, uint64_t *streamed, uint64_t *sweeps, uint64_t *hbm_bytes);
 /* Structure groups of the last sq_batch_run: streamed circuits whose plans
  * differ only in their angles (the same circuit with other parameters) run
@@ -387,11 +389,13 @@ int sq_batch_stats(const sq_batch *b, uint64_t *streamed, uint64_t *sweeps, uint
 int sq_batch_groups(const sq_batch *b, uint32_t *groups, uint32_t *circuits);
 /* Test hook: CUDA source of the multi-state JIT kernel (sq_jit_msweep) of
  * sweep `sweep_index` of a circuit as a batch energy run plans it with the
- * default tile size (num_qubits above it).  Writes at most cap bytes
- * (NUL-terminated), the full length to *len and the number of sweeps to
- * *nsweeps.  Needs no GPU. */
+ * default tile size (num_qubits above it); from_zero = 1: the form that
+ * starts every state from |0...0> instead of reading it (*len = 0 when the
+ * sweep has none).  Writes at most cap bytes (NUL-terminated), the full
+ * length to *len and the number of sweeps to *nsweeps.  Needs no GPU. */
 int sq_jit_multi_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
-                        uint32_t sweep_index, char *buf, uint64_t cap, uint64_t *len, uint32_t *nsweeps);
+                        uint32_t sweep_index, int from_zero, char *buf, uint64_t cap, uint64_t *len,
+                        uint32_t *nsweeps);
 
 #ifdef __cplusplus
 }

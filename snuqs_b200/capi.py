@@ -106,7 +106,7 @@ SIGNATURES = {
     "sq_batch_last_timing": (_I, [_P, _PD, _PU32]),
     "sq_batch_stats": (_I, [_P, _PU64, _PU64, _PU64]),
     "sq_batch_groups": (_I, [_P, _PU32, _PU32]),
-    "sq_jit_multi_source": (_I, [_U32, _I, _P, _U32, _U32, ctypes.c_char_p, _U64, _PU64, _PU32]),
+    "sq_jit_multi_source": (_I, [_U32, _I, _P, _U32, _U32, _I, ctypes.c_char_p, _U64, _PU64, _PU32]),
 }
 
 
@@ -136,13 +136,17 @@ def jit_info():
 
 
 def jit_sources(n: int, ops, dtype: int = SQ_C128, limit: int | None = None, adjoint: bool = False,
-                multi: bool = False):
+                multi: bool = False, from_zero: bool = False):
     """CUDA sources of the JIT kernels of the fused sweeps of a circuit (with
     adjoint=True: of the reverse sweeps of its adjoint-gradient plan; with
-    multi=True: the multi-state kernels of its batch energy plan; "" for a
-    sweep the generic kernel runs)."""
-    fn = (lib().sq_jit_adjoint_source if adjoint else
-          lib().sq_jit_multi_source if multi else lib().sq_jit_source)
+    multi=True: the multi-state kernels of its batch energy plan, from_zero:
+    their form that starts from |0...0>; "" for a sweep the generic kernel
+    runs)."""
+    if multi:
+        raw = lib().sq_jit_multi_source
+        fn = lambda *a: raw(*a[:5], int(from_zero), *a[5:])
+    else:
+        fn = lib().sq_jit_adjoint_source if adjoint else lib().sq_jit_source
     arr, keep = circuit_ops(ops)
     ln, ns = _U64(0), _U32(0)
     check(fn(n, dtype, ctypes.cast(arr, _P), len(ops), 0, None, 0, ctypes.byref(ln), ctypes.byref(ns)))

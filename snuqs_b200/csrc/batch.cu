@@ -108,6 +108,9 @@ struct MultiGroup {
   uint32_t n = 0, count = 0, first = 0;
   uint64_t pool_off = 0, plan_off = 0, rec_bytes = 0;
   std::vector<MultiSweep> sweeps;
+  // The first sweep starts every state from |0...0> itself (no init pass,
+  // no first read).
+  bool zero_first = false;
 };
 
 }  // namespace
@@ -594,10 +597,21 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
       gcoef.emplace_back();
       gsweeps.push_back(unpack_sweeps(packed[ids[0]], gcoef.back()));
     }
-    std::vector<const sq::PlannedSweep *> todo;
-    for (const auto &g : gsweeps)
-      for (const auto &ps : g) todo.push_back(&ps);
-    sq::jit_prepare_multi(todo, sizeof(Real) == 4);
+    // The first sweep of a group in its from-|0...0> form where it has one.
+    std::vector<const sq::PlannedSweep *> todo, zero;
+    std::vector<char> zero_ok(gsweeps.size(), 0);
+    for (size_t g = 0; g < gsweeps.size(); ++g)
+      for (size_t k = 0; k < gsweeps[g].size(); ++k) {
+        const sq::PlannedSweep &ps = gsweeps[g][k];
+        if (k == 0 && !sq::jit_body(ps, sizeof(Real) == 4, sq::jit_minb(sizeof(Real) == 4, ps.h.m), true, true)
+                           .empty()) {
+          zero_ok[g] = 1;
+          zero.push_back(&ps);
+        } else {
+          todo.push_back(&ps);
+        }
+      }
+    sq::jit_prepare_multi(todo, sizeof(Real) == 4, zero);
     for (size_t g = 0; g < members.size(); ++g) {
       MultiGroup G;
       G.n = b->circs[members[g][0]].n;
@@ -608,7 +622,11 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
         const sq::PlannedSweep &ps = gsweeps[g][k];
         MultiSweep w;
         std::string err;
-        w.fn = sq::jit_msweep_kernel(ps, sizeof(Real) == 4, err);
+        if (k == 0 && zero_ok[g]) {
+          w.fn = sq::jit_msweep_kernel(ps, sizeof(Real) == 4, err, true);
+          G.zero_first = w.fn != nullptr;
+        }
+        if (!w.fn) w.fn = sq::jit_msweep_kernel(ps, sizeof(Real) == 4, err);
         w.smem = sq::jit_msweep_smem(ps, sizeof(Real) == 4);
         w.ncoef = ps.h.ncoef;
         w.coef_at = gcoef[g][k];
@@ -641,7 +659,9 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
     if (b->circs[i].n > M || group_of[i] >= 0) {
       b->stat_streamed++;
       b->stat_sweeps += uint64_t(nsweeps[i]);
-      b->stat_bytes += (2 * uint64_t(nsweeps[i]) + 1) * (uint64_t(1) << b->circs[i].n) * sizeof(C2);
+      // A group whose first sweep starts from |0...0> does not read the state there.
+      const bool zf = group_of[i] >= 0 && b->groups[size_t(group_of[i])].zero_first;
+      b->stat_bytes += (2 * uint64_t(nsweeps[i]) + 1 - (zf ? 1 : 0)) * (uint64_t(1) << b->circs[i].n) * sizeof(C2);
     }
   // Table order: the circuits batch_kernel runs, largest first (its dynamic
   // work queue), then each structure group's circuits together.
@@ -791,7 +811,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
         C2 *gpsi = poolp + G.pool_off;
         const uint64_t total = uint64_t(G.count) << G.n;
         const uint32_t ig = uint32_t(std::min<uint64_t>((total + 255) / 256, uint64_t(sms) * 8));
-        sq::batch_group_init<Real><<<ig, 256, 0, cs>>>(gpsi, total, G.n);
+        if (!G.zero_first) sq::batch_group_init<Real><<<ig, 256, 0, cs>>>(gpsi, total, G.n);
         for (const MultiSweep &w : G.sweeps) {
           sq::MultiParams Q;
           Q.coefs = static_cast<const unsigned char *>(b->d_plans.p) + G.plan_off + w.coef_at;
@@ -1301,7 +1321,8 @@ int sq_jit_batch_adjoint_source(uint32_t num_qubits, int dtype, const sq_circuit
 }
 
 int sq_jit_multi_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops, uint32_t nops,
-                        uint32_t sweep_index, char *buf, uint64_t cap, uint64_t *len, uint32_t *nsweeps) {
+                        uint32_t sweep_index, int from_zero, char *buf, uint64_t cap, uint64_t *len,
+                        uint32_t *nsweeps) {
   if ((nops && !ops) || !len) return fail(SQ_ERR_INVALID, "null pointer");
   if (dtype != SQ_C128 && dtype != SQ_C64) return fail(SQ_ERR_INVALID, "bad dtype");
   const bool c64 = dtype == SQ_C64;
@@ -1321,8 +1342,9 @@ int sq_jit_multi_source(uint32_t num_qubits, int dtype, const sq_circuit_op *ops
   std::vector<uint64_t> coef_at;
   const auto sweeps = unpack_sweeps(packed, coef_at);
   const sq::PlannedSweep &ps = sweeps[sweep_index];
-  const std::string body = sq::jit_body(ps, c64, sq::jit_minb(c64, ps.h.m), true);
-  const std::string src = body.empty() ? std::string() : sq::jit_source(ps, c64, sq::jit_minb(c64, ps.h.m), true);
+  const std::string body = sq::jit_body(ps, c64, sq::jit_minb(c64, ps.h.m), true, from_zero != 0);
+  const std::string src =
+      body.empty() ? std::string() : sq::jit_source(ps, c64, sq::jit_minb(c64, ps.h.m), true, from_zero != 0);
   *len = src.size();
   if (buf && cap) {
     const size_t n = std::min<size_t>(cap - 1, src.size());

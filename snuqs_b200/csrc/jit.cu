@@ -755,11 +755,16 @@ JitShape jit_shape(const PlannedSweep &ps, bool c64, bool multi = false) {
 // form sq_jit_msweep (one launch over K states sharing the sweep's
 // structure, coefficients per state); empty when the sweep remaps qubits
 // (not covered by that form).
-std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi) {
+std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi, bool from_zero) {
   const char *R = c64 ? "float" : "double";
   const int M = int(ps.h.m);
   const JitShape js = jit_shape(ps, c64, multi);
   if (multi && (ps.h.flags & kRemap)) return std::string();
+  // From |0...0>: the first phase must take its registers from HBM (which it
+  // then does not read).
+  if (from_zero && (!multi || !(js.early || js.dload))) return std::string();
+  std::ostringstream nm;
+  nm << "0x" << std::hex << ((uint64_t(1) << ps.h.n) - 1) << "ull";
   std::ostringstream s;
   if (multi)
     s << "extern \"C\" __global__ void __launch_bounds__(" << (1 << (M - kRegBits)) << ", " << minb
@@ -799,8 +804,12 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi) {
     else
       s << "  jit_sweep_early<" << R << ", " << M << ", Tile, " << tf(js.smem_coef) << ", " << tf(js.dstore)
         << ", TileOut>(psi, P, ";
-    s << "[&](Amps<" << R << "> &A, uint64_t gb) { Ph0::load(A, psi, gb, Ph0::jb(threadIdx.x)); }, "
-      << "[&](const Amps<" << R << "> &A0, C2 *tile, const C2 *coef, uint64_t gbase) {\n";
+    if (from_zero)
+      s << "[&](Amps<" << R << "> &A, uint64_t gb) { Ph0::zero_state(A, gb, Ph0::jb(threadIdx.x), " << nm.str()
+        << "); }, ";
+    else
+      s << "[&](Amps<" << R << "> &A, uint64_t gb) { Ph0::load(A, psi, gb, Ph0::jb(threadIdx.x)); }, ";
+    s << "[&](const Amps<" << R << "> &A0, C2 *tile, const C2 *coef, uint64_t gbase) {\n";
   } else if (multi)
     s << "  jit_msweep<" << R << ", " << M << ", Tile, " << tf(js.dload) << ", " << tf(js.dstore)
       << ">(psi, Q, [&](C2 *tile, const C2 *coef, uint64_t gbase) {\n";
@@ -823,6 +832,8 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi) {
       s << "      Ph::gather_lin(A, stage, jb);\n      ctl.release();\n";
     else if (p == 0 && js.early)
       s << "      A = A0;\n";
+    else if (from_hbm && from_zero)
+      s << "      Ph::zero_state(A, gbase, jb, " << nm.str() << ");\n";
     else if (from_hbm)
       s << "      Ph::load(A, psi, gbase, jb);\n";
     else
@@ -850,8 +861,8 @@ std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi) {
   return s.str();
 }
 
-std::string jit_source(const PlannedSweep &ps, bool c64, int minb, bool multi) {
-  return prelude() + jit_body(ps, c64, minb, multi);
+std::string jit_source(const PlannedSweep &ps, bool c64, int minb, bool multi, bool from_zero) {
+  return prelude() + jit_body(ps, c64, minb, multi, from_zero);
 }
 
 // Source of the JIT kernel of one reverse (two-state) adjoint sweep; empty
@@ -1100,12 +1111,12 @@ Entry &sweep_entry(const PlannedSweep &ps, bool c64) {
   return *e;
 }
 
-Entry *msweep_entry(const PlannedSweep &ps, bool c64) {
-  const PlanKey k = plan_key(ps, c64, 2);
+Entry *msweep_entry(const PlannedSweep &ps, bool c64, bool from_zero) {
+  const PlanKey k = plan_key(ps, c64, from_zero ? 3 : 2);
   bool found = false;
   Entry *e = plan_lookup(k, &found);
   if (found) return e;
-  const std::string body = jit_body(ps, c64, jit_minb(c64, ps.h.m), true);
+  const std::string body = jit_body(ps, c64, jit_minb(c64, ps.h.m), true, from_zero);
   e = body.empty() ? nullptr : &get_entry(body, "sq_jit_msweep");
   plan_store(k, e);
   return e;
@@ -1180,8 +1191,8 @@ const void *jit_sweep_kernel(const PlannedSweep &ps, bool c64, std::string &err)
   return reinterpret_cast<const void *>(e.kernel);
 }
 
-const void *jit_msweep_kernel(const PlannedSweep &ps, bool c64, std::string &err) {
-  Entry *e = msweep_entry(ps, c64);
+const void *jit_msweep_kernel(const PlannedSweep &ps, bool c64, std::string &err, bool from_zero) {
+  Entry *e = msweep_entry(ps, c64, from_zero);
   if (!e) {
     err = "sweep not covered by the multi-state JIT form";
     return nullptr;
@@ -1198,15 +1209,31 @@ size_t jit_msweep_smem(const PlannedSweep &ps, bool c64) {
   return jit_smem_bytes(int(ps.h.m), c64 ? 8 : 16, js.dload || js.early, (ps.h.ncoef + 1) & ~1u);
 }
 
-void jit_prepare_multi(const std::vector<const PlannedSweep *> &sweeps, bool c64) {
-  if (!jit_available() || sweeps.empty()) return;
+void jit_prepare_multi(const std::vector<const PlannedSweep *> &sweeps, bool c64,
+                       const std::vector<const PlannedSweep *> &from_zero) {
+  if (!jit_available() || (sweeps.empty() && from_zero.empty())) return;
   std::vector<const PlannedSweep *> todo;
-  for (const auto *ps : sweeps) {
-    bool found = false;
-    plan_lookup(plan_key(*ps, c64, 2), &found);
-    if (!found) todo.push_back(ps);
-  }
-  prepare_parallel(todo, [&](const PlannedSweep &ps) { msweep_entry(ps, c64); });
+  std::vector<char> zero;
+  for (int z = 0; z < 2; ++z)
+    for (const auto *ps : z ? from_zero : sweeps) {
+      bool found = false;
+      plan_lookup(plan_key(*ps, c64, z ? 3 : 2), &found);
+      if (!found) {
+        todo.push_back(ps);
+        zero.push_back(char(z));
+      }
+    }
+  // Index of each task's variant: the tasks are distinct pointers per variant.
+  std::vector<std::pair<const PlannedSweep *, bool>> tasks;
+  for (size_t i = 0; i < todo.size(); ++i) tasks.emplace_back(todo[i], zero[i] != 0);
+  std::atomic<size_t> next{0};
+  const unsigned nth = std::max(1u, std::min<unsigned>(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < std::min<size_t>(nth, tasks.size()); ++t)
+    pool.emplace_back([&] {
+      for (size_t i = next++; i < tasks.size(); i = next++) msweep_entry(*tasks[i].first, c64, tasks[i].second);
+    });
+  for (auto &th : pool) th.join();
 }
 
 void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64) {

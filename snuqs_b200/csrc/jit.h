@@ -12,9 +12,12 @@ bool jit_available();
 void jit_note_launch(bool jit);
 // CUDA source of the kernel specialised for `ps` (`minb` CTAs per SM);
 // multi: its multi-state form (jit_msweep_kernel).
-std::string jit_source(const PlannedSweep &ps, bool c64, int minb, bool multi = false);
+// from_zero (multi-state only): the first phase starts from |0...0> in every
+// state instead of reading it (empty source when the sweep's first phase does
+// not load from HBM).
+std::string jit_source(const PlannedSweep &ps, bool c64, int minb, bool multi = false, bool from_zero = false);
 // The part of that source that depends on `ps` (the cache key).
-std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi = false);
+std::string jit_body(const PlannedSweep &ps, bool c64, int minb, bool multi = false, bool from_zero = false);
 // Dynamic shared memory the JIT kernel of `ps` needs.
 size_t jit_smem(const PlannedSweep &ps, bool c64);
 // CTAs per SM the kernels of (precision, tile bits) are built for.
@@ -42,9 +45,10 @@ std::string jit_batch_source(const std::string &body);
 // Multi-state sweeps (sq_jit_msweep: one launch applies the sweep to K states
 // that share its structure, sq::MultiParams): the kernel (or nullptr with
 // `err`), its dynamic shared memory, and a parallel pre-compile.
-const void *jit_msweep_kernel(const PlannedSweep &ps, bool c64, std::string &err);
+const void *jit_msweep_kernel(const PlannedSweep &ps, bool c64, std::string &err, bool from_zero = false);
 size_t jit_msweep_smem(const PlannedSweep &ps, bool c64);
-void jit_prepare_multi(const std::vector<const PlannedSweep *> &sweeps, bool c64);
+void jit_prepare_multi(const std::vector<const PlannedSweep *> &sweeps, bool c64,
+                       const std::vector<const PlannedSweep *> &from_zero = {});
 // Compiles the kernels of several sweeps in parallel (fills the cache).
 void jit_prepare(const std::vector<const PlannedSweep *> &sweeps, bool c64);
 

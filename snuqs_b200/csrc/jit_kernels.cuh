@@ -175,6 +175,17 @@ struct JitPhase {
       A.im[ri] = v.y;
     }
   }
+  // The first phase of a state that starts as |0...0>: amplitude 1 where the
+  // global index has no bit of nmask set (state index bits), else 0; nothing
+  // is read (multi-state sweeps: the first sweep of a structure group).
+  __device__ __forceinline__ static void zero_state(Amps<Real> &A, uint64_t gbase, uint32_t jbv, uint64_t nmask) {
+    const uint64_t base = gbase | Tile::off(jbv);
+#pragma unroll
+    for (int ri = 0; ri < kRegAmps; ++ri) {
+      A.re[ri] = Real(((base | goff(ri)) & nmask) == 0 ? 1 : 0);
+      A.im[ri] = Real(0);
+    }
+  }
   // Straight from registers to HBM (the mirror case for a last phase).
   __device__ __forceinline__ static void store(const Amps<Real> &A, C2 *psi, uint64_t gbase, uint32_t jbv) {
     C2 *p = psi + (gbase | Tile::off(jbv));

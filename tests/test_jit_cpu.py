@@ -218,3 +218,7 @@ def test_multi_state_sources_compile(dtype, n):
     assert not any("ParamCoef<" in s.split("sq_jit_msweep")[1] for s in srcs)
     for s in srcs[:2]:
         capi.jit_compile(s)
+    # The first sweep in the form that starts every state from |0...0>.
+    z = capi.jit_sources(n, ops, dtype, multi=True, from_zero=True, limit=1)[0]
+    assert "zero_state(" in z and "Ph0::load(" not in z.split("sq_jit_msweep")[1]
+    capi.jit_compile(z)
