@@ -87,3 +87,22 @@ def test_adjoint_rejects_bad_input():
         # parameter index 3 but only 1 parameter: rejected by the C ABI
         adjoint.adjoint_gradient(ws, [("RotX", (0,), (0.1,), (3,))], [0.0] * 4, [(1.0, "ZIIIII")], 1)
     ws.close()
+
+
+def test_repeated_gradients_on_one_workspace_reuse_plans():
+    """Gradients of one circuit at three parameter sets on the same workspace
+    (the forward and reverse plans are re-emitted from their recipes after the
+    first), each against the parameter-shift rule; 20 qubits, JIT sweeps."""
+    n, p = 20, 2
+    ops, terms = qaoa(n, p, seed=4)
+    ws = adjoint.Workspace(n)
+    ref = capi.State(n, capi.SQ_C128)
+    rng = np.random.default_rng(4)
+    for _ in range(3):
+        theta = rng.uniform(0, np.pi, 2 * p)
+        e, g = adjoint.adjoint_gradient(ws, ops, theta, terms, 2 * p)
+        gs = adjoint.parameter_shift_gradient(ref, ops, theta, terms, 2 * p)
+        assert abs(e - adjoint.energy(ref, ops, theta, terms)) <= 1e-10
+        assert np.abs(g - gs).max() <= 1e-10 * max(1.0, np.abs(gs).max())
+    ref.close()
+    ws.close()
