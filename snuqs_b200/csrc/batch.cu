@@ -14,8 +14,10 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/snuqs_b200.h"
@@ -246,6 +248,36 @@ void pack_sweep(const sq::PlannedSweep &ps, std::vector<unsigned char> &out) {
 }
 
 // Plans one circuit into packed sweeps; returns the sweep count or < 0.
+// Plans shared between the circuits of one structure within one planning
+// pass (many parameter sets of one ansatz): the first circuit of a structure
+// (op signature, qubits, plan options) is planned, the others re-emit its
+// plan with their own values (sq::rebuild_plan), and fall back to planning
+// when that fails.
+struct PlanShare {
+  using Key = std::tuple<uint64_t, uint64_t, uint64_t, uint32_t>;
+  std::mutex mu;
+  std::map<Key, std::shared_ptr<const std::vector<sq::PlannedLaunch>>> plans;
+
+  std::vector<sq::PlannedLaunch> plan(const std::vector<sq::HostOp> &ops, uint32_t n, const sq::PlanOptions &opt) {
+    const auto sig = sq::op_signature_hash(ops);
+    const Key key{sig.first, sig.second, sq::plan_options_key(opt), n};
+    std::shared_ptr<const std::vector<sq::PlannedLaunch>> have;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = plans.find(key);
+      if (it != plans.end()) have = it->second;
+    }
+    if (have) {
+      std::vector<sq::PlannedLaunch> p = *have;
+      if (sq::rebuild_plan(p, ops, n)) return p;
+    }
+    std::vector<sq::PlannedLaunch> p = sq::plan_sweeps(ops, n, opt);
+    std::lock_guard<std::mutex> lk(mu);
+    plans.emplace(key, std::make_shared<const std::vector<sq::PlannedLaunch>>(p));
+    return p;
+  }
+};
+
 // A circuit's gates as planner ops (identities dropped).  False with `err`.
 bool circuit_host_ops(const Circ &c, std::vector<sq::HostOp> &ops, std::string &err) {
   ops.clear();
@@ -277,7 +309,8 @@ std::pair<uint64_t, uint64_t> signature_hash(const std::vector<sq::HostOp> &ops)
 template <typename Real>
 int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
                  std::vector<unsigned char> &out, std::string &err, int select = -1,
-                 std::vector<sq::SweepRecipe> *recipes = nullptr, std::pair<uint64_t, uint64_t> *sig = nullptr) {
+                 std::vector<sq::SweepRecipe> *recipes = nullptr, std::pair<uint64_t, uint64_t> *sig = nullptr,
+                 PlanShare *share = nullptr) {
   try {
     std::vector<sq::HostOp> ops;
     if (!circuit_host_ops(c, ops, err)) return -1;
@@ -290,7 +323,7 @@ int plan_circuit(const Circ &c, uint32_t m, uint32_t low_bits, uint32_t max_ops,
     opt.select = select;
     // Low bits matter only for a state streamed through tiles (n > m).
     if (low_bits && c.n > m && low_bits + uint32_t(sq::kRegBits) <= m) opt.low_bits = low_bits;
-    const auto plan = sq::plan_sweeps(ops, c.n, opt);
+    const auto plan = share ? share->plan(ops, c.n, opt) : sq::plan_sweeps(ops, c.n, opt);
     int sweeps = 0;
     for (const auto &pl : plan) {
       if (!pl.is_sweep) {
@@ -546,6 +579,7 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
   std::vector<std::string> errs(nc);
   std::atomic<size_t> next{0};
   const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  PlanShare share;
   auto plan_all = [&](const std::vector<uint32_t> &ids) {
     next = 0;
     std::vector<std::thread> pool;
@@ -555,9 +589,9 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
           const uint32_t i = ids[k];
           packed[i].clear();
           nsweeps[i] = cand[i] ? plan_circuit<Real>(b->circs[i], MJ, 0, 0, packed[i], errs[i], multi_select(),
-                                                    &b->recipes[i], &b->sigs[i])
+                                                    &b->recipes[i], &b->sigs[i], &share)
                                : plan_circuit<Real>(b->circs[i], M, b->low_bits, b->max_ops, packed[i], errs[i], -1,
-                                                    &b->recipes[i], &b->sigs[i]);
+                                                    &b->recipes[i], &b->sigs[i], &share);
         }
       });
     for (auto &th : pool) th.join();
@@ -868,7 +902,8 @@ int run_impl(sq_batch *b, double *energies, cudaStream_t st) {
 // sweeps (adjoint_plan.cc), packed back to back.  Returns false with `err`.
 template <typename Real>
 bool plan_gradient_circuit(const Circ &c, uint32_t m, std::vector<unsigned char> &out, uint32_t &nfwd,
-                           uint32_t &nrev, std::vector<std::pair<int32_t, double>> &occ, std::string &err) {
+                           uint32_t &nrev, std::vector<std::pair<int32_t, double>> &occ, std::string &err,
+                           PlanShare *share = nullptr) {
   try {
     sq::AdjointPlan ap;
     sq::build_adjoint(c.ops.data(), uint32_t(c.ops.size()), c.n, ap);
@@ -879,8 +914,8 @@ bool plan_gradient_circuit(const Circ &c, uint32_t m, std::vector<unsigned char>
     ropt.tile_bits = m;
     ropt.reg_bits = sq::kAdjRegBits;
     ropt.max_dense_k = sq::kAdjRegBits;
-    const auto fplan = sq::plan_sweeps(ap.forward, c.n, fopt);
-    const auto rplan = sq::plan_sweeps(ap.reverse, c.n, ropt);
+    const auto fplan = share ? share->plan(ap.forward, c.n, fopt) : sq::plan_sweeps(ap.forward, c.n, fopt);
+    const auto rplan = share ? share->plan(ap.reverse, c.n, ropt) : sq::plan_sweeps(ap.reverse, c.n, ropt);
     nfwd = nrev = 0;
     for (const auto &pl : fplan) {
       if (!pl.is_sweep) {
@@ -947,11 +982,12 @@ int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *
   std::vector<char> ok(nc, 0);
   std::atomic<size_t> next{0};
   const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  PlanShare share;
   std::vector<std::thread> workers;
   for (unsigned t = 0; t < nth; ++t)
     workers.emplace_back([&]() {
       for (size_t i = next++; i < nc; i = next++)
-        ok[i] = plan_gradient_circuit<Real>(b->circs[i], M, packed[i], nfwd[i], nrev[i], occs[i], errs[i]);
+        ok[i] = plan_gradient_circuit<Real>(b->circs[i], M, packed[i], nfwd[i], nrev[i], occs[i], errs[i], &share);
     });
   for (auto &th : workers) th.join();
   for (size_t i = 0; i < nc; ++i) {

@@ -120,20 +120,13 @@ struct sq_state {
   PlanMemo flush_memo, fwd_memo, rev_memo;
 };
 
-// The plan options a memo entry depends on, packed into one word.
-static uint64_t plan_opts_key(const sq::PlanOptions &o) {
-  return uint64_t(o.tile_bits) | (uint64_t(o.low_bits) << 8) | (uint64_t(o.max_dense_k) << 16) |
-         (uint64_t(o.reg_bits) << 24) | (uint64_t(o.max_ops) << 32) | (uint64_t(o.reorder) << 48) |
-         (uint64_t(o.remap) << 49) | (uint64_t(uint8_t(o.select)) << 50);
-}
-
 // Plans `ops`, or re-emits the memo's plan when the ops have its signature
 // and options (and every sweep of it has a recipe); the memo then holds the
 // new plan.  Throws what plan_sweeps throws.
 static std::vector<sq::PlannedLaunch> plan_memo(sq_state::PlanMemo &memo, const std::vector<sq::HostOp> &ops,
                                                 uint32_t n, const sq::PlanOptions &opt) {
   const auto sig = sq::op_signature_hash(ops);
-  const uint64_t key = plan_opts_key(opt);
+  const uint64_t key = sq::plan_options_key(opt);
   if (memo.opts == key && memo.sig == sig) {
     std::vector<sq::PlannedLaunch> plan = memo.plan;
     if (sq::rebuild_plan(plan, ops, n)) {

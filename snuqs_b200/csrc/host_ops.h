@@ -119,6 +119,13 @@ inline uint32_t auto_low_bits(bool c64, uint32_t n, uint32_t m) {
   return lb && lb + uint32_t(kRegBits) <= m ? lb : 0u;
 }
 
+// The plan options a plan depends on, packed into one word (a cache key).
+inline uint64_t plan_options_key(const PlanOptions &o) {
+  return uint64_t(o.tile_bits) | (uint64_t(o.low_bits) << 8) | (uint64_t(o.max_dense_k) << 16) |
+         (uint64_t(o.reg_bits) << 24) | (uint64_t(o.max_ops) << 32) | (uint64_t(o.reorder) << 48) |
+         (uint64_t(o.remap) << 49) | (uint64_t(uint8_t(o.select)) << 50);
+}
+
 // Packs ops (in circuit order) into fused sweeps for an n-qubit state.
 std::vector<PlannedLaunch> plan_sweeps(const std::vector<HostOp> &ops, uint32_t n,
                                        const PlanOptions &opt);
