@@ -1001,9 +1001,27 @@ int run_gradient_impl(sq_batch *b, uint32_t n_params, double *energies, double *
   // circuit) and stream their states get a JIT-specialised kernel.
   const void *jit_fn = nullptr;
   if (uniform_plans<Real>(b, packed, nfwd, nrev, occs, M)) {
-    std::string err;
-    jit_fn = sq::jit_batch_adjoint_kernel(packed[0].data(), nfwd[0], nrev[0], b->circs[0].n, M,
-                                          sizeof(Real) == 4, err);
+    // Looked up by plan structure: a repeated gradient run of the same
+    // circuit skips generating (and hashing) the kernel's source.
+    static std::mutex memo_mu;
+    static std::map<std::tuple<uint64_t, uint64_t, uint64_t>, const void *> memo;
+    const auto sk = structure_key(packed[0], coef_ranges<Real>(packed[0]), b->circs[0].n);
+    const std::tuple<uint64_t, uint64_t, uint64_t> key{
+        sk.first, sk.second, (uint64_t(nfwd[0]) << 32) | (uint64_t(nrev[0]) << 8) | (M << 1) | (sizeof(Real) == 4)};
+    {
+      std::lock_guard<std::mutex> lk(memo_mu);
+      auto it = memo.find(key);
+      if (it != memo.end()) jit_fn = it->second;
+    }
+    if (!jit_fn) {
+      std::string err;
+      jit_fn = sq::jit_batch_adjoint_kernel(packed[0].data(), nfwd[0], nrev[0], b->circs[0].n, M,
+                                            sizeof(Real) == 4, err);
+      if (jit_fn) {
+        std::lock_guard<std::mutex> lk(memo_mu);
+        memo[key] = jit_fn;
+      }
+    }
   }
   // Largest work first.
   b->order.resize(nc);
