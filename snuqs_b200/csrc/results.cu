@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <complex>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -46,25 +47,31 @@ __device__ __forceinline__ double prob(const C2 *__restrict__ psi, uint64_t i, u
   return __dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im));
 }
 
-// Sum of one leaf in the fixed tree: a thread sums its 16 amplitudes
-// pairwise, then threads t and t^1, t^2, ... combine (commutative adds give
-// both partners the same value), then warps pairwise through shared memory.
+// Sum of one leaf in the fixed tree (pairwise sums over consecutive
+// amplitudes, level by level).  Warp w covers the 512 amplitudes from
+// 512 w; lane l reads amplitude 32 k + l for k = 0..15 (coalesced), the five
+// lowest levels of each group of 32 are lane pairs l, l^1, l^2, ... (shuffles;
+// a commutative add gives both partners the same value), the next four are
+// the groups k in registers, then the warps pairwise through shared memory.
 template <typename C2>
 __global__ void __launch_bounds__(kLeafThreads) leaf_sum_kernel(const C2 *__restrict__ psi, uint64_t N,
                                                                 double *__restrict__ leaves) {
   __shared__ double ws[kLeafThreads / 32];
-  const uint64_t base = uint64_t(blockIdx.x) * kLeafAmps + uint64_t(threadIdx.x) * kPerThread;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t base = uint64_t(blockIdx.x) * kLeafAmps + uint64_t(threadIdx.x >> 5) * (32 * kPerThread) + lane;
   double v[kPerThread];
 #pragma unroll
-  for (uint32_t j = 0; j < kPerThread; ++j) v[j] = prob(psi, base + j, N);
+  for (uint32_t k = 0; k < kPerThread; ++k) v[k] = prob(psi, base + 32 * k, N);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+    for (uint32_t k = 0; k < kPerThread; ++k) v[k] = __dadd_rn(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
 #pragma unroll
   for (uint32_t w = kPerThread / 2; w >= 1; w >>= 1)
 #pragma unroll
     for (uint32_t j = 0; j < w; ++j) v[j] = __dadd_rn(v[2 * j], v[2 * j + 1]);
-  double s = v[0];
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  const double s = v[0];
+  if (lane == 0) ws[threadIdx.x >> 5] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
     double w[kLeafThreads / 32];
@@ -114,31 +121,45 @@ __global__ void shot_descend_kernel(const double *__restrict__ tree, uint32_t de
   atomicAdd(&count[k], 1u);
 }
 
-// Exclusive scan of the per-leaf counts (one block; leaves <= 2^22).
+// Exclusive scan of the per-leaf counts (one block; leaves <= 2^22): 1024
+// counts per step, read coalesced, scanned with warp shuffles.
 __global__ void __launch_bounds__(1024) count_scan_kernel(const uint32_t *__restrict__ count, uint32_t nleaves,
                                                           uint32_t *__restrict__ offset,
                                                           uint32_t *__restrict__ cursor) {
-  __shared__ uint32_t part[1024];
-  const uint32_t per = (nleaves + 1023) / 1024;
-  const uint32_t b = threadIdx.x * per, e = min(nleaves, b + per);
-  uint32_t sum = 0;
-  for (uint32_t i = b; i < e; ++i) sum += count[i];
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t run = 0;
-    for (int i = 0; i < 1024; ++i) {
-      const uint32_t c = part[i];
-      part[i] = run;
-      run += c;
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t total;
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  uint32_t base = 0;
+  for (uint32_t t0 = 0; t0 < nleaves; t0 += 1024) {
+    const uint32_t i = t0 + threadIdx.x;
+    const uint32_t v = i < nleaves ? count[i] : 0u;
+    uint32_t x = v;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= uint32_t(o)) x += y;
     }
-  }
-  __syncthreads();
-  uint32_t run = part[threadIdx.x];
-  for (uint32_t i = b; i < e; ++i) {
-    offset[i] = run;
-    cursor[i] = run;
-    run += count[i];
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      const uint32_t sw = wsum[lane];
+      uint32_t y = sw;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t z = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= uint32_t(o)) y += z;
+      }
+      wsum[lane] = y - sw;  // exclusive over warps
+      if (lane == 31) total = y;
+    }
+    __syncthreads();
+    const uint32_t excl = base + wsum[w] + x - v;
+    if (i < nleaves) {
+      offset[i] = excl;
+      cursor[i] = excl;
+    }
+    base += total;
+    __syncthreads();
   }
 }
 
@@ -329,9 +350,12 @@ size_t sample_scratch_bytes(uint32_t n, uint64_t shots) {
          2 * align256(shots * sizeof(uint32_t)) + align256(shots * sizeof(double));
 }
 
+// u_ready (optional): an event the shot phase waits for before reading the
+// uniforms (they may still be in flight on another stream while the
+// probability tree is built).
 template <typename C2>
 int sample_impl(const C2 *psi, uint32_t n, const double *u, uint64_t shots, uint64_t *out, void *scr,
-                cudaStream_t st) {
+                cudaStream_t st, cudaEvent_t u_ready = nullptr, const std::function<int()> &before_shots = {}) {
   const uint64_t N = uint64_t(1) << n;
   const uint32_t depth = n > uint32_t(kLeafBits) ? n - kLeafBits : 0;
   const uint64_t nleaves = uint64_t(1) << depth;
@@ -358,6 +382,11 @@ int sample_impl(const C2 *psi, uint32_t n, const double *u, uint64_t shots, uint
   if (depth) upper_tree_kernel<<<1, 1024, 0, st>>>(tree, depth);
   RQ_CUDA(cudaGetLastError());
   RQ_CUDA(cudaMemsetAsync(count, 0, nleaves * sizeof(uint32_t), st));
+  if (before_shots) {
+    const int rc = before_shots();
+    if (rc != SQ_OK) return rc;
+  }
+  if (u_ready) RQ_CUDA(cudaStreamWaitEvent(st, u_ready, 0));
   const unsigned sb = unsigned((shots + 255) / 256);
   shot_descend_kernel<<<sb, 256, 0, st>>>(tree, depth, u, shots, leaf, resid, count);
   RQ_CUDA(cudaGetLastError());
@@ -367,10 +396,11 @@ int sample_impl(const C2 *psi, uint32_t n, const double *u, uint64_t shots, uint
   RQ_CUDA(cudaGetLastError());
   const size_t smem = (2 * size_t(kLeafAmps) - 1) * sizeof(double);
   RQ_CUDA(cudaFuncSetAttribute(leaf_sample_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  int sms = 0, dev = 0;
+  int sms = 0, dev = 0, per_sm = 0;
   RQ_CUDA(cudaGetDevice(&dev));
   RQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const unsigned grid = unsigned(std::min<uint64_t>(nleaves, uint64_t(sms) * 2));
+  RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_sample_kernel<C2>, kLeafThreads, smem));
+  const unsigned grid = unsigned(std::min<uint64_t>(nleaves, uint64_t(sms) * uint64_t(std::max(per_sm, 1))));
   leaf_sample_kernel<C2><<<grid, kLeafThreads, smem, st>>>(psi, N, uint32_t(nleaves), count, offset, order,
                                                            resid, out);
   RQ_CUDA(cudaGetLastError());
@@ -414,11 +444,39 @@ int sq_sample_host(sq_state *s, const double *uniforms, uint64_t shots, uint64_t
   char *p = static_cast<char *>(scr);
   double *du = reinterpret_cast<double *>(p);
   uint64_t *dout = reinterpret_cast<uint64_t *>(p + b_u);
-  RQ_CUDA(cudaMemcpyAsync(du, uniforms, shots * sizeof(double), cudaMemcpyHostToDevice, st));
+  // The uniforms go up on a second stream while the probability tree is
+  // built (the host blocks in a copy from pageable memory, so the tree
+  // kernels are queued first); the shot phase waits for them.
+  cudaStream_t cs = nullptr;
+  cudaEvent_t prior = nullptr, ready = nullptr;
+  struct Release {
+    cudaStream_t &cs;
+    cudaEvent_t &a, &b;
+    ~Release() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+      if (cs) cudaStreamDestroy(cs);
+    }
+  } release{cs, prior, ready};
+  RQ_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  RQ_CUDA(cudaEventCreateWithFlags(&prior, cudaEventDisableTiming));
+  RQ_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  RQ_CUDA(cudaEventRecord(prior, st));  // earlier work on the state's stream
+  auto upload = [&]() -> int {
+    RQ_CUDA(cudaStreamWaitEvent(cs, prior, 0));
+    RQ_CUDA(cudaMemcpyAsync(du, uniforms, shots * sizeof(double), cudaMemcpyHostToDevice, cs));
+    RQ_CUDA(cudaEventRecord(ready, cs));
+    return SQ_OK;
+  };
   rc = sq_state_dtype(s) == SQ_C64
-           ? sample_impl(static_cast<const float2 *>(sq_state_data(s)), n, du, shots, dout, p + b_u + b_o, st)
-           : sample_impl(static_cast<const double2 *>(sq_state_data(s)), n, du, shots, dout, p + b_u + b_o, st);
-  if (rc != SQ_OK) return rc;
+           ? sample_impl(static_cast<const float2 *>(sq_state_data(s)), n, du, shots, dout, p + b_u + b_o, st,
+                         ready, upload)
+           : sample_impl(static_cast<const double2 *>(sq_state_data(s)), n, du, shots, dout, p + b_u + b_o, st,
+                         ready, upload);
+  if (rc != SQ_OK) {
+    cudaStreamSynchronize(cs);
+    return rc;
+  }
   RQ_CUDA(cudaMemcpyAsync(out, dout, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   RQ_CUDA(cudaStreamSynchronize(st));
   return SQ_OK;
