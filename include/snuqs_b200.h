@@ -220,9 +220,10 @@ int sq_variance_pauli(sq_state *s, const char *paulis, const double *weights,
  * shots <= 2^31 per call; num_qubits <= 34. */
 int sq_sample(sq_state *s, const double *uniforms_device, uint64_t shots,
               uint64_t *out_device, void *stream);
-/* sq_sample with HOST buffers (staged through the state's device scratch):
- * the uniforms go to the device, only the shot indices come back.
- * Synchronous. */
+/* sq_sample with HOST buffers (staged through the state's device scratch
+ * and a pinned host buffer of 8 x shots bytes that the state keeps until it
+ * is destroyed): the uniforms go to the device while the probability tree is
+ * built, only the shot indices come back.  Synchronous. */
 int sq_sample_host(sq_state *s, const double *uniforms, uint64_t shots,
                    uint64_t *out, void *stream);
 /* Amplitudes psi[indices[i]] as complex128 (interleaved doubles) into

@@ -108,6 +108,8 @@ struct sq_state {
   uint32_t *errword = nullptr;
   void *rscratch = nullptr;  // result kernels' scratch (results.cu)
   size_t rscratch_bytes = 0;
+  void *hscratch = nullptr;  // pinned host staging of results with host buffers
+  size_t hscratch_bytes = 0;
   // The last plans, reused for the same gate sequence with other values (a
   // circuit run again with other angles): sq::rebuild_plan re-emits them
   // from their recipes without planning.  Keyed by the ops' signature hash
@@ -583,6 +585,18 @@ int sq_detail_state_scratch(sq_state *s, size_t bytes, void **out) {
   return SQ_OK;
 }
 
+int sq_detail_state_host_scratch(sq_state *s, size_t bytes, void **out) {
+  if (s->hscratch_bytes < bytes) {
+    if (s->hscratch) SQ_CUDA(cudaFreeHost(s->hscratch));
+    s->hscratch = nullptr;
+    s->hscratch_bytes = 0;
+    SQ_CUDA(cudaHostAlloc(&s->hscratch, bytes, cudaHostAllocDefault));
+    s->hscratch_bytes = bytes;
+  }
+  *out = s->hscratch;
+  return SQ_OK;
+}
+
 static int ensure_scratch(sq_state *s, uint32_t len) {
   if (s->scratch_len >= len) return SQ_OK;
   if (s->scratch) SQ_CUDA(cudaFree(s->scratch));
@@ -757,6 +771,7 @@ int sq_state_destroy(sq_state *s) {
   if (s->scratch) SQ_CUDA(cudaFree(s->scratch));
   if (s->errword) SQ_CUDA(cudaFree(s->errword));
   if (s->rscratch) SQ_CUDA(cudaFree(s->rscratch));
+  if (s->hscratch) SQ_CUDA(cudaFreeHost(s->hscratch));
   for (auto &ev : s->sweep_events) {
     cudaEventDestroy(ev.first);
     cudaEventDestroy(ev.second);

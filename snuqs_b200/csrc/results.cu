@@ -444,9 +444,12 @@ int sq_sample_host(sq_state *s, const double *uniforms, uint64_t shots, uint64_t
   char *p = static_cast<char *>(scr);
   double *du = reinterpret_cast<double *>(p);
   uint64_t *dout = reinterpret_cast<uint64_t *>(p + b_u);
-  // The uniforms go up on a second stream while the probability tree is
-  // built (the host blocks in a copy from pageable memory, so the tree
-  // kernels are queued first); the shot phase waits for them.
+  // Pinned staging (the state's, reused): the uniforms are copied into it
+  // and go up on a second stream while the probability tree is built; the
+  // shot phase waits for them; the indices come back through it.
+  void *hs = nullptr;
+  rc = sq_detail_state_host_scratch(s, std::max(shots * sizeof(double), shots * sizeof(uint64_t)), &hs);
+  if (rc != SQ_OK) return rc;
   cudaStream_t cs = nullptr;
   cudaEvent_t prior = nullptr, ready = nullptr;
   struct Release {
@@ -463,8 +466,9 @@ int sq_sample_host(sq_state *s, const double *uniforms, uint64_t shots, uint64_t
   RQ_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
   RQ_CUDA(cudaEventRecord(prior, st));  // earlier work on the state's stream
   auto upload = [&]() -> int {
+    std::memcpy(hs, uniforms, shots * sizeof(double));  // while the tree kernels run
     RQ_CUDA(cudaStreamWaitEvent(cs, prior, 0));
-    RQ_CUDA(cudaMemcpyAsync(du, uniforms, shots * sizeof(double), cudaMemcpyHostToDevice, cs));
+    RQ_CUDA(cudaMemcpyAsync(du, hs, shots * sizeof(double), cudaMemcpyHostToDevice, cs));
     RQ_CUDA(cudaEventRecord(ready, cs));
     return SQ_OK;
   };
@@ -477,8 +481,9 @@ int sq_sample_host(sq_state *s, const double *uniforms, uint64_t shots, uint64_t
     cudaStreamSynchronize(cs);
     return rc;
   }
-  RQ_CUDA(cudaMemcpyAsync(out, dout, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  RQ_CUDA(cudaMemcpyAsync(hs, dout, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   RQ_CUDA(cudaStreamSynchronize(st));
+  std::memcpy(out, hs, shots * sizeof(uint64_t));
   return SQ_OK;
 }
 
